@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Benchmark of the MISA-MD EAM hot path on B200: atom-steps/s.
+
+A "step" is one velocity-Verlet timestep of the whole lattice (rho/df pass, force
+pass with the integration fused, interstitial passes), state resident in HBM.
+
+Default workload (the scale configuration): BCC Fe 128^3 unit cells
+(4,194,304 sites), 0.5% of sites vacated (seed 7), 200 interstitial atoms at random
+octahedral sites (seed 7), 300 K, dt = 1 fs, plain FP64, synthetic analytic
+potential tabulated at 5000 knots.  `--config mixed` runs the 200^3-cell mixed
+precision configuration instead.
+
+Multi-GPU: every rank advances its own independent replica (the path does not
+shard; no collective on the data path): value = all ranks' atom-steps / max time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib.util
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+A0, MASS, RC, SKIN, DT = 2.855, 55.845, 5.6, 0.7, 1.0
+
+# algorithmic figures per atom-step (device-resident SoA, stored force):
+#   rho pass   reads x (24) + type (4), writes df (8)                        = 36 B
+#   force pass reads x, type, df, v, f_old (84), writes x, v, f (72)         = 156 B
+#   flops: 58 pairs x (20 rho + 50 force) + 30 per atom                      = 4090
+BYTES_RHO, BYTES_FORCE = 36, 156
+FLOP_RHO, FLOP_FORCE = 58 * 20, 58 * 50 + 30
+
+WORKLOADS = {
+    "scale": dict(name="fe_bcc_128c_vac0.5pct_itl200_300K_fp64", cells=(128, 128, 128), temperature=300.0,
+                  vacancy=0.005, n_itl=200, seed=7, precision="fp64"),
+    "mixed": dict(name="fe_bcc_200c_vac0.5pct_itl763_900K_mixed", cells=(200, 200, 200), temperature=900.0,
+                  vacancy=0.005, n_itl=763, seed=7, precision="mixed"),
+    "small": dict(name="fe_bcc_20c_600K_fp64", cells=(20, 20, 20), temperature=600.0, vacancy=0.0, n_itl=0,
+                  seed=42, precision="fp64"),
+}
+
+
+def _package():
+    if "misa_b200" in sys.modules:
+        return sys.modules["misa_b200"]
+    pkg_dir = ROOT / "misa-md-hip_b200"
+    spec = importlib.util.spec_from_file_location("misa_b200", pkg_dir / "__init__.py",
+                                                  submodule_search_locations=[str(pkg_dir)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["misa_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def build_state(mb, wl: dict, cells=None):
+    cells = cells or wl["cells"]
+    box = mb.lattice.bcc_box(cells, A0)
+    mb.lattice.add_vacancies(box, wl["vacancy"], wl["seed"])
+    scale = (cells[0] * cells[1] * cells[2]) / float(np.prod(wl["cells"]))
+    n_itl = int(round(wl["n_itl"] * scale))
+    itl = mb.lattice.octahedral_interstitials(n_itl, cells, A0, wl["seed"])
+    # interstitials never sit on a vacated site's octahedral neighbour twice: distinct sites suffice
+    mb.lattice.maxwell_boltzmann(box, itl, wl["temperature"], MASS, wl["seed"] + 1000)
+    return box, itl
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def ncu_traffic(kernel: str) -> float | None:
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        return float(json.loads(p.read_text())[kernel]["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows: list[list[str]] = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return self
+
+        def pump():
+            for line in self.proc.stdout:
+                self.rows.append([c.strip() for c in line.split(",")])
+
+        self.thread = threading.Thread(target=pump, daemon=True)
+        self.thread.start()
+        return self
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 4 + k and r[4 + k].lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, value: float) -> float:
+    if pg is None:
+        return value
+    import torch
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def cpu_oracle_rate(mb, wl: dict, cells, steps: int, threads: int | None = None):
+    """Atom-steps/s of the CPU oracle (the reference algorithm restated) on a sample lattice."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle as orc
+    if threads:
+        orc.set_threads(threads)
+    box, itl = build_state(mb, wl, cells)
+    ghost = mb.lattice.ghost_for_reach(A0, RC + SKIN)
+    dom = orc.make_domain(cells, ghost)
+    even, odd = orc.stencil(dom, A0, RC + SKIN)
+    ext = mb.lattice.box_to_ext(box, cells, ghost, A0).view(orc.ATOM)
+    io = itl.view(orc.ATOM).copy()
+    pot = orc.Pot.from_tables(mb.potential.fe_analytic())
+    mp = orc.md_params(A0, MASS, DT, RC)
+    n_atoms = int((box["type"] >= 0).sum()) + io.shape[0]
+    orc.compute_forces(pot, dom, ext, io, even, odd, mp)  # forces at the start (untimed)
+    t0 = time.perf_counter()
+    orc.md_run(pot, dom, ext, io, even, odd, mp, steps, record=False)  # one force evaluation per step
+    dt = time.perf_counter() - t0
+    return n_atoms, dt, orc.num_threads()
+
+
+def run_reference(args, mb, wl, world, rank) -> None:
+    if rank != 0:
+        return
+    cells = tuple(min(c, 48) for c in wl["cells"])
+    n_threads = os.cpu_count() or 1
+    # warm-up steps (untimed) then K timed steps, each one MD step of the sample lattice
+    if args.warmup:
+        cpu_oracle_rate(mb, wl, cells, 1, n_threads)
+    n_atoms, dt, thr = cpu_oracle_rate(mb, wl, cells, args.steps, n_threads)
+    step_time = dt / args.steps
+    value = n_atoms / step_time
+    sample = f"{cells[0]}x{cells[1]}x{cells[2]} cells of the same workload ({n_atoms} atoms), 1 step per timed step"
+    line = {
+        "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_time * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": wl["name"], "sample_cells": list(cells)},
+        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": thr, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, mb, wl, world, rank, local, pg) -> None:
+    mb.check(mb.lib().mb_env_init(local))
+    precision = mb.MB_PREC_FP64 if wl["precision"] == "fp64" else mb.MB_PREC_MIXED
+    box, itl = build_state(mb, wl)
+    n_atoms = int((box["type"] >= 0).sum()) + itl.shape[0]
+    sim = mb.Sim(wl["cells"], mb.potential.fe_analytic(), lattice_const=A0, mass=MASS, dt=DT, cutoff=RC,
+                 stencil_skin=SKIN, precision=precision, max_interstitials=max(1, itl.shape[0]))
+    sim.upload(box, itl)
+    info = sim.info()
+    sim.run(max(args.warmup, 3))  # W >= 3 untimed warm-up steps (graph capture happens here)
+
+    clocks = ClockSampler(local).start()
+    barrier(pg)
+    ms = sim.time_steps(args.steps)
+    barrier(pg)
+    clk = clocks.stop()
+    ms = reduce_max(pg, ms)
+    total_atom_steps = n_atoms * args.steps * world
+    value = total_atom_steps / (ms * 1e-3)
+
+    # per-kernel device time (CUDA events on the sim's stream, outside the timed region)
+    rho_ms, force_ms = sim.kernel_times()
+    peaks = measured_peaks()
+    f64 = C.c_double()
+    f32 = C.c_double()
+    mb.check(mb.lib().mb_measure_fma_peaks(C.byref(f64), C.byref(f32)))
+    force_bytes = BYTES_FORCE * n_atoms
+    achieved = force_bytes / (force_ms * 1e-3) / 1e9
+    traffic = ncu_traffic("force")
+    roofline = {
+        "kernel": "k_force64 (force + velocity-Verlet)" if precision == mb.MB_PREC_FP64 else "force (mixed)",
+        "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+        "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+        "traffic": traffic, "algorithmic_bytes_per_launch": force_bytes, "launch_ms": force_ms,
+        "fp64": {"achieved_tflops": FLOP_FORCE * n_atoms / (force_ms * 1e-3) / 1e12,
+                 "peak_tflops": f64.value, "frac": FLOP_FORCE * n_atoms / (force_ms * 1e-3) / 1e12 / f64.value,
+                 "peak_source": "measured FMA-chain probe (mb_measure_fma_peaks)"},
+        "rho_kernel": {"launch_ms": rho_ms, "achieved_gbs": BYTES_RHO * n_atoms / (rho_ms * 1e-3) / 1e9,
+                       "achieved_tflops": FLOP_RHO * n_atoms / (rho_ms * 1e-3) / 1e12},
+        "fp32_peak_tflops": f32.value,
+    }
+
+    # end to end through the public host-buffer entry point: every step uploads the
+    # lattice records from pinned host memory and reads the updated records back
+    e2e = None
+    if precision == mb.MB_PREC_FP64:
+        n_box = box.shape[0]
+        p = C.c_void_p()
+        alloc = C.c_int()
+        mb.check(mb.lib().mb_create_atoms_mem(C.byref(p), 104, n_box, 1, 1, C.byref(alloc)))
+        host = np.ctypeslib.as_array((C.c_uint8 * (104 * n_box)).from_address(p.value)).view(mb.ATOM_DTYPE)
+        b2, i2 = sim.download()
+        host[:] = b2
+        k_e2e = max(3, min(args.steps, 20))
+        sim.step_host(host, i2)  # warm-up
+        barrier(pg)
+        t0 = time.perf_counter()
+        for _ in range(k_e2e):
+            sim.step_host(host, i2)
+        e2e_s = time.perf_counter() - t0
+        barrier(pg)
+        e2e_s = reduce_max(pg, e2e_s)
+        rel = C.c_int()
+        mb.check(mb.lib().mb_release_atoms_mem(p, C.byref(rel)))
+        e2e = {"value": n_atoms * k_e2e * world / e2e_s, "unit": "atom-steps/s",
+               "h2d_bytes_per_step": 104 * (n_box + i2.shape[0]), "d2h_bytes_per_step": 104 * (n_box + i2.shape[0]),
+               "steps": k_e2e, "api": "mb_sim_step_host (pinned host AoS records in, updated records out)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cells = tuple(min(c, 32) for c in wl["cells"])
+        na, dt, thr = cpu_oracle_rate(mb, wl, cells, 3, os.cpu_count())
+        cpu = {"value": na * 3 / dt, "unit": "atom-steps/s", "cores": thr, "kind": "port",
+               "sample": f"{cells[0]}x{cells[1]}x{cells[2]} cells of the same workload ({na} atoms), 3 steps"}
+    sim.close()
+    launches_per_step = 5 if itl.shape[0] else 2
+    if rank == 0:
+        line = {
+            "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == mb.MB_PREC_FP64 else "f32+f64",
+            "data": "synthetic (seeded lattice, analytic tabulated potential)",
+            "config": {"workload": wl["name"], "cells": list(wl["cells"]), "atoms_per_gpu": n_atoms,
+                       "stencil": info["n_stencil"], "replicas": world,
+                       "l2": f"state {info['device_bytes'] / 1e6:.0f} MB per GPU > 126 MB L2 (no flush needed)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(WORKLOADS), default="scale")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local, pg = dist_setup()
+    mb = _package()
+    wl = WORKLOADS[args.config]
+    try:
+        if args.impl == "reference":
+            run_reference(args, mb, wl, world, rank)
+        else:
+            run_ours(args, mb, wl, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,193 @@
+/*
+ * misa_b200 — B200-native EAM hot path for MISA-MD, C ABI.
+ *
+ * Three layers, all plain C types (no torch, no C++ in the signatures):
+ *   1. Drop-in hooks: the plugin interface of misa-md-hip, with the reference's
+ *      argument meaning and synchronous semantics, on the host's own ghost-extended
+ *      AoS lattice array.
+ *   2. Device-resident molecular dynamics: one lattice (plus interstitials) kept in
+ *      HBM, ghost wrap done on the device, velocity-Verlet fused into the force
+ *      pass, FP64 or mixed precision.
+ *   3. Ensembles and serving: many independent lattices advanced together.
+ *
+ * Every entry point returns MB_OK (0) or a positive MB_ERR_* code; the message of
+ * the last failure on the calling thread is in mb_last_error().  Nothing aborts.
+ */
+#ifndef MISA_B200_H
+#define MISA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MB_OK 0
+#define MB_ERR_ARG 1         /* bad argument or size */
+#define MB_ERR_CUDA 2        /* CUDA runtime failure (message has the CUDA error) */
+#define MB_ERR_STATE 3       /* call order: e.g. a pass before mb_pot_init */
+#define MB_ERR_NOMEM 4       /* device allocation refused / over budget */
+#define MB_ERR_TIMEOUT 5     /* a bounded device wait gave up */
+#define MB_ERR_UNSUPPORTED 6 /* valid request this build does not implement */
+
+#define MB_PREC_FP64 0  /* plain FP64: the drop-in path */
+#define MB_PREC_MIXED 1 /* FP32 pair/spline work, compensated FP32 sums, FP64 state */
+
+const char *mb_last_error(void);
+const char *mb_version(void);
+
+/* ------------------------------------------------------------------ types */
+
+/* One lattice site, byte-compatible with misa-md-hip's _cuAtomElement
+ * (src/kernel_types.h:40-48), itself a copy of MISA-MD's AtomElement: 104 bytes.
+ * type < 0 marks a vacancy / invalid site. */
+typedef struct mb_atom_element {
+  int64_t id;
+  int32_t type;
+  int32_t pad_;
+  double x[3];
+  double v[3];
+  double f[3];
+  double rho;
+  double df;
+} mb_atom_element;
+
+/* Lattice geometry, field-for-field the reference's _hipDeviceDomain
+ * (src/kernel_types.h:51-64).  Sizes along x are in the doubled BCC index
+ * (two sites per unit cell).  ghost = local_low - ghost_low, ext = box + 2 ghost,
+ * box_index_start = global index of the first box site. */
+typedef struct mb_device_domain {
+  int32_t ghost_size_x, ghost_size_y, ghost_size_z;
+  int32_t box_size_x, box_size_y, box_size_z;
+  int32_t ext_size_x, ext_size_y, ext_size_z;
+  int32_t pad_;
+  int64_t box_index_start_x, box_index_start_y, box_index_start_z;
+} mb_device_domain;
+
+/* Tabulated EAM potential.  Knots are uniformly spaced from 0: r_k = k*dr,
+ * rho_k = k*drho.  f: n_types rows of nr electron-density values f_t(r);
+ * F: n_types rows of nrho embedding energies F_t(rho); phi: n_types*(n_types+1)/2
+ * rows of nr pair energies phi_ab(r) (not r*phi), packed upper triangle
+ * (0,0),(0,1),..,(0,n-1),(1,1),...  Beyond the last rho knot F continues
+ * linearly with its end slope; pairs at r >= cutoff do not interact. */
+typedef struct mb_eam_tables {
+  int32_t n_types; /* 1..3 (the reference uploads types {0,1,2}) */
+  int32_t nr;
+  int32_t nrho;
+  int32_t pad_;
+  double dr;
+  double drho;
+  double cutoff;
+  const double *f;
+  const double *F;
+  const double *phi;
+} mb_eam_tables;
+
+/* ------------------------------------------------- 1. drop-in plugin hooks */
+
+/* hip_env_init (src/hip_arch_acc_imp.cpp:28-40): select the device. */
+int mb_env_init(int device);
+/* hip_env_clean (src/hip_arch_acc_imp.cpp:42-45): frees every device buffer the
+ * hooks own (the reference leaks them). */
+int mb_env_clean(void);
+/* hip_domain_init (src/hip_arch_acc_imp.cpp:47-99), taking the converted domain
+ * instead of comm::BccDomain.  ghost_size_x and box_size_x must be even. */
+int mb_domain_init(const mb_device_domain *domain);
+/* hip_nei_offset_init (src/hip_arch_acc_imp.cpp:101-144): the even / odd x-parity
+ * neighbour stencils as linear offsets into the ghost-extended array (what
+ * NeighbourIndex::nei_even_offsets / nei_odd_offsets hold). */
+int mb_nei_offset_init(const int64_t *nei_even, size_t n_even, const int64_t *nei_odd, size_t n_odd);
+/* hip_pot_init (src/hip_arch_acc_imp.cpp:146-150): build and upload the spline tables. */
+int mb_pot_init(const mb_eam_tables *tables);
+/* hip_eam_rho_calc (src/hip_arch_acc_imp.cpp:163-181): for every box site with
+ * type >= 0, rho = sum over the stencil of f_{t_j}(r) for r < cutoff, then
+ * df = F'(rho) (fused, full-neighbour build).  atoms is the host's
+ * ghost-extended AoS array (ghosts already filled); rho and df are written back. */
+int mb_eam_rho_calc(mb_atom_element *atoms, double cutoff_radius);
+/* hip_eam_df_calc (src/hip_arch_acc_imp.cpp:183-205): a no-op in the full-neighbour
+ * build, exactly like the reference (df is produced by the rho pass). */
+int mb_eam_df_calc(mb_atom_element *atoms, double cutoff_radius);
+/* hip_eam_force_calc (src/hip_arch_acc_imp.cpp:207-225): f = sum del * fpair over
+ * the stencil, overwriting f of every box site with type >= 0 (needs df of the
+ * ghost sites filled by the host). */
+int mb_eam_force_calc(mb_atom_element *atoms, double cutoff_radius);
+/* The calDf kernel of the half-neighbour build (src/kernels/hip_kernels.hip.cpp:21-40):
+ * df = F'(rho) for every box site with type >= 0. */
+int mb_eam_df_from_rho(mb_atom_element *atoms);
+/* hip_create_atoms_mem (src/mem.cpp:14-23): page-locked host allocation of
+ * size_x*size_y*size_z elements; *allocated = 1 when this library allocated. */
+int mb_create_atoms_mem(void **atoms, size_t data_type_size, int64_t size_x, int64_t size_y, int64_t size_z,
+                        int *allocated);
+/* hip_release_atoms_mem (src/mem.cpp:25-32). */
+int mb_release_atoms_mem(void *atoms, int *released);
+/* hip_cli_options / hip_cli_options_parse (src/cli.cpp:16-27): the -b/--batches
+ * value.  Accepted and reported; state is device-resident, so it changes no result. */
+int mb_cli_set_batches(unsigned int batches);
+unsigned int mb_cli_batches(void);
+
+/* Neighbour stencils in the reference's linear form for an ext array of
+ * ext_x x ext_y: every BCC site whose ideal offset is shorter than reach (the role
+ * MISA-MD's NeighbourIndex plays for hip_nei_offset_init).  Ordered dz, dy, dx
+ * ascending; *n receives the length of each. */
+int mb_stencil_linear(double lattice_const, double reach, int ext_x, int ext_y, int64_t *even, int64_t *odd, int cap,
+                      int *n);
+/* The 7 spline coefficients per knot the device tables are built from
+ * (y, s, c2, c3, s/dx, 2 c2/dx, 3 c3/dx), for checking the table build on the host. */
+int mb_spline_coeffs(const double *y, int n, double dx, double *coef7);
+
+/* Timing of the last hook call: device milliseconds of its kernels and of its
+ * host<->device copies (CUDA events). */
+int mb_hook_last_timing(float *kernel_ms, float *copy_ms);
+
+/* Throughput of dependent-free FMA chains on the CUDA cores of the current device
+ * (TFLOP/s, FMA = 2 flops): the FP64 and FP32 roofline denominators. */
+int mb_measure_fma_peaks(double *fp64_tflops, double *fp32_tflops);
+
+/* ---------------------------------------- 2. device-resident simulation */
+
+typedef struct mb_sim mb_sim;
+
+typedef struct mb_sim_config {
+  int32_t cells_x, cells_y, cells_z; /* unit cells; box = (2*cells_x, cells_y, cells_z) sites */
+  int32_t precision;                 /* MB_PREC_FP64 or MB_PREC_MIXED */
+  double lattice_const;              /* A */
+  double mass;                       /* amu */
+  double dt;                         /* fs */
+  double cutoff;                     /* A */
+  double stencil_skin;               /* A: stencil = sites with ideal distance < cutoff + skin */
+  int32_t max_interstitials;
+  int32_t pad_;
+} mb_sim_config;
+
+/* Per-site records in "box order": index ((z*box_y)+y)*box_x + x with x doubled. */
+int mb_sim_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **out);
+int mb_sim_destroy(mb_sim *sim);
+/* Load positions, velocities and types (box order) plus an interstitial list.
+ * Forces are (re)computed on the next run. */
+int mb_sim_upload(mb_sim *sim, const mb_atom_element *box_atoms, const mb_atom_element *itl, int32_t n_itl);
+/* Synchronised state at the current step: x, v, f, rho, df of every site. */
+int mb_sim_download(mb_sim *sim, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t *n_itl);
+/* Advance nsteps velocity-Verlet steps on the device (asynchronous on the sim's
+ * stream).  energy_every > 0 records (pe, ke) every that many steps. */
+int mb_sim_run(mb_sim *sim, int32_t nsteps, int32_t energy_every);
+int mb_sim_sync(mb_sim *sim);
+/* Energies recorded by the last run: n pairs (step, pe, ke) in eV. */
+int mb_sim_energies(mb_sim *sim, double *out_step_pe_ke, int32_t cap, int32_t *n);
+/* Device time of nsteps (CUDA events around the sim's stream), after one
+ * untimed priming pass if needed. */
+int mb_sim_time_steps(mb_sim *sim, int32_t nsteps, float *ms);
+/* One full step through host buffers: upload box_atoms (x, v, f, type),
+ * one velocity-Verlet step on the device, write x, v, f, rho, df back.  The
+ * e2e form of the hot path: host<->device copies are part of every call. */
+int mb_sim_step_host(mb_sim *sim, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t n_itl);
+/* Mean kernel milliseconds of the rho and force launches of the last timed run. */
+int mb_sim_kernel_times(mb_sim *sim, float *rho_ms, float *force_ms);
+int mb_sim_info(mb_sim *sim, int64_t *n_sites, int64_t *n_stencil, int64_t *device_bytes);
+/* CUDA graph capture of the steady-state step (on by default). */
+int mb_sim_set_graphs(mb_sim *sim, int enable);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

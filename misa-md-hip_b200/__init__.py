@@ -1,0 +1,156 @@
+"""misa_b200: B200-native EAM hot path of MISA-MD (host-side Python mirror).
+
+The compute path is the CUDA library ``libmisa_b200.so`` (csrc/, built for
+sm_100a); this package only binds its C ABI (include/misa_b200.h) with ctypes and
+sets up lattices.  Importing it does not need a GPU; every compute call does, and
+raises if the library or the device is missing (there is no CPU fallback).
+
+Two ways in:
+  * ``Hooks`` — the misa-md-hip plugin interface (rho / df / force passes on the
+    host's ghost-extended AoS lattice), for a MISA-MD-style host loop;
+  * ``Sim``   — device-resident molecular dynamics of one lattice.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi, lattice, potential
+from ._abi import ATOM_DTYPE, MB_PREC_FP64, MB_PREC_MIXED, MbError, check, lib, ptr
+
+__all__ = ["ATOM_DTYPE", "MB_PREC_FP64", "MB_PREC_MIXED", "MbError", "Hooks", "Sim", "lattice", "potential",
+           "lib", "build"]
+
+
+def build(force: bool = False, verbose: bool = False):
+    from . import builder
+    return builder.build(force=force, verbose=verbose)
+
+
+class Hooks:
+    """The drop-in plugin interface (misa-md-hip src/hip_arch_acc_imp.cpp:28-225)."""
+
+    def __init__(self, device: int = 0):
+        check(lib().mb_env_init(device))
+
+    def domain_init(self, dom: _abi.MbDeviceDomain) -> None:
+        check(lib().mb_domain_init(C.byref(dom)))
+
+    def nei_offset_init(self, even: np.ndarray, odd: np.ndarray) -> None:
+        even = np.ascontiguousarray(even, dtype=np.int64)
+        odd = np.ascontiguousarray(odd, dtype=np.int64)
+        check(lib().mb_nei_offset_init(_abi.i64ptr(even), even.size, _abi.i64ptr(odd), odd.size))
+
+    def pot_init(self, tables: potential.EamTables) -> None:
+        t = tables.as_c()
+        check(lib().mb_pot_init(C.byref(t)))
+
+    def rho_calc(self, atoms: np.ndarray, cutoff: float) -> None:
+        assert atoms.dtype == ATOM_DTYPE
+        check(lib().mb_eam_rho_calc(ptr(atoms), cutoff))
+
+    def df_calc(self, atoms: np.ndarray, cutoff: float) -> None:
+        check(lib().mb_eam_df_calc(ptr(atoms), cutoff))
+
+    def df_from_rho(self, atoms: np.ndarray) -> None:
+        check(lib().mb_eam_df_from_rho(ptr(atoms)))
+
+    def force_calc(self, atoms: np.ndarray, cutoff: float) -> None:
+        assert atoms.dtype == ATOM_DTYPE
+        check(lib().mb_eam_force_calc(ptr(atoms), cutoff))
+
+    def last_timing(self) -> tuple[float, float]:
+        k, c = C.c_float(), C.c_float()
+        check(lib().mb_hook_last_timing(C.byref(k), C.byref(c)))
+        return k.value, c.value
+
+    @staticmethod
+    def clean() -> None:
+        check(lib().mb_env_clean())
+
+
+class Sim:
+    """Device-resident MD of one periodic BCC lattice (+ interstitials)."""
+
+    def __init__(self, cells, tables: potential.EamTables, lattice_const: float = 2.855, mass: float = 55.845,
+                 dt: float = 1.0, cutoff: float | None = None, stencil_skin: float = 0.7,
+                 precision: int = MB_PREC_FP64, max_interstitials: int = 0):
+        self.cells = tuple(int(c) for c in cells)
+        self.lattice_const = lattice_const
+        self.mass = mass
+        self.dt = dt
+        cfg = _abi.MbSimConfig(self.cells[0], self.cells[1], self.cells[2], precision, lattice_const, mass, dt,
+                               tables.cutoff if cutoff is None else cutoff, stencil_skin, max_interstitials, 0)
+        t = tables.as_c()
+        h = C.c_void_p()
+        check(lib().mb_sim_create(C.byref(cfg), C.byref(t), C.byref(h)))
+        self._h = h
+        self.n_box = 2 * self.cells[0] * self.cells[1] * self.cells[2]
+        self.n_itl = 0
+        self.max_interstitials = max_interstitials
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().mb_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, box: np.ndarray, itl: np.ndarray | None = None) -> None:
+        assert box.dtype == ATOM_DTYPE and box.shape[0] == self.n_box
+        n = 0 if itl is None else int(itl.shape[0])
+        itl_p = ptr(np.ascontiguousarray(itl)) if n else None
+        check(lib().mb_sim_upload(self._h, ptr(np.ascontiguousarray(box)), itl_p, n))
+        self.n_itl = n
+
+    def download(self) -> tuple[np.ndarray, np.ndarray]:
+        box = np.zeros(self.n_box, dtype=ATOM_DTYPE)
+        itl = np.zeros(max(1, self.max_interstitials), dtype=ATOM_DTYPE)
+        n = C.c_int32(0)
+        check(lib().mb_sim_download(self._h, ptr(box), ptr(itl), C.byref(n)))
+        return box, itl[:n.value].copy()
+
+    def run(self, nsteps: int, energy_every: int = 0) -> None:
+        check(lib().mb_sim_run(self._h, nsteps, energy_every))
+        check(lib().mb_sim_sync(self._h))
+
+    def energies(self) -> np.ndarray:
+        n = C.c_int32(0)
+        check(lib().mb_sim_energies(self._h, None, 0, C.byref(n)))
+        out = np.zeros((max(1, n.value), 3))
+        check(lib().mb_sim_energies(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), n.value, C.byref(n)))
+        return out[:n.value]
+
+    def time_steps(self, nsteps: int) -> float:
+        ms = C.c_float()
+        check(lib().mb_sim_time_steps(self._h, nsteps, C.byref(ms)))
+        return ms.value
+
+    def kernel_times(self) -> tuple[float, float]:
+        a, b = C.c_float(), C.c_float()
+        check(lib().mb_sim_kernel_times(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def step_host(self, box: np.ndarray, itl: np.ndarray | None = None) -> None:
+        """One full step through host buffers (box / itl updated in place)."""
+        n = 0 if itl is None else int(itl.shape[0])
+        check(lib().mb_sim_step_host(self._h, ptr(box), ptr(itl) if n else None, n))
+
+    def info(self) -> dict:
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().mb_sim_info(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"n_sites": a.value, "n_stencil": b.value, "device_bytes": c.value}
+
+    def set_graphs(self, enable: bool) -> None:
+        check(lib().mb_sim_set_graphs(self._h, int(enable)))

@@ -1,0 +1,172 @@
+// Shared declarations of the misa_b200 library (host + device).
+//
+// Device layout ("sublattice-split SoA"): the reference indexes a BCC lattice
+// with x doubled, so neighbouring memory cells alternate between the two
+// simple-cubic sublattices and every warp mixes two stencils
+// (src/kernels/kernel_itl.hpp:82,86).  Here each sublattice s in {0,1} is its own
+// ghost-extended (ecx, ey, ez) array, x fastest, so a warp always walks one
+// stencil and every neighbour fetch is a contiguous 32-site row.  The site at
+// doubled ext index ex lives in sublattice ex & 1, column ex >> 1.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/misa_b200.h"
+
+#define MB_MAX_STENCIL 320       // per parity; the reference's full stencil is about 228
+#define MB_FTM2V 9.64853321233e-3 // (eV/A)/amu -> A/fs^2
+#define MB_MVV2E (1.0 / MB_FTM2V) // amu A^2/fs^2 -> eV
+#define MB_VACANT_POS 1.0e30      // position given to vacant sites: every r^2 test rejects them
+#define MB_FLAG_ITL 0x40          // site code bit: an interstitial is within reach
+
+namespace mb {
+
+// Read-only 32-byte load through the non-coherent path (two 16-byte halves).
+__device__ __forceinline__ double4 ldg4(const double4 *p) {
+  const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+  const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define MB_CUDA(call)                                                                                          \
+  do {                                                                                                         \
+    cudaError_t e_ = (call);                                                                                   \
+    if (e_ != cudaSuccess) return ::mb::cuda_fail(e_, #call);                                                  \
+  } while (0)
+
+#define MB_TRY(call)                                                                                           \
+  do {                                                                                                         \
+    int rc_ = (call);                                                                                          \
+    if (rc_ != MB_OK) return rc_;                                                                              \
+  } while (0)
+
+// ------------------------------------------------------------ potential
+// Per-knot cubic pieces.  value(p) = ((c3 p + c2) p + s) p + y on [m, m+1];
+// d/dx value = (d2 p + d1) p + d0 with d = (s, 2 c2, 3 c3) / dx.
+struct DevPot {
+  int n_types, nr, nrho;
+  double rdr, rdrho, rho_max, cutoff;
+  const double4 *f_val;   // [nt][nr]   {y, s, c2, c3}
+  const double4 *f_der;   // [nt][nr]   {d0, d1, d2, 0}
+  const double4 *F_val;   // [nt][nrho]
+  const double4 *F_der;   // [nt][nrho]
+  const double4 *phi_val; // [np][nr]
+  const double4 *phi_der; // [np][nr]
+  const double2 *force1;  // single type: [nr][3] {f d0, phi d0}, {f d1, phi d1}, {f d2, phi d2}
+  // single precision copies for the mixed path
+  const float4 *f_val32;  // [nt][nr]
+  const float4 *force132; // single type: [nr][2] {f d0, f d1, f d2, phi d0}, {phi d1, phi d2, 0, 0}
+};
+
+struct PotHost;
+int pot_build(const mb_eam_tables *t, PotHost **out);
+void pot_free(PotHost *p);
+const DevPot &pot_dev(const PotHost *p);
+
+// ------------------------------------------------------------- geometry
+struct Geom {
+  int ecx, ey, ez; // ext size per sublattice
+  int gcx, gy, gz; // ghost widths (cells along x)
+  int bcx, by, bz; // box size per sublattice
+  int images;      // 1: sites write their periodic ghost images (device-resident mode)
+  long long E;     // sites per sublattice array
+  double Lx, Ly, Lz;
+};
+
+struct StencilSet {
+  int n;                          // entries per parity (equal for both)
+  int off[2][MB_MAX_STENCIL];     // [sublattice] split-layout linear offsets
+};
+
+// Convert reference-style doubled-x linear offsets to split-layout offsets.
+// parity_of_sublattice[s] selects which reference stencil (0 even, 1 odd) the sites
+// of sublattice s walk.
+int stencil_from_linear(const int64_t *even, size_t n_even, const int64_t *odd, size_t n_odd, int ext_x, int ext_y,
+                        const Geom &g, const int parity_of_sublattice[2], StencilSet *out);
+// BCC stencil of every site with ideal distance < reach (doubled-x linear form,
+// ordered dz, dy, dx ascending), for an ext array of ext_x x ext_y.
+int stencil_generate(double a0, double reach, int ext_x, int ext_y, int64_t *even, int64_t *odd, int cap, int *n,
+                     int *reach_x, int *reach_y, int *reach_z);
+
+// ------------------------------------------------------ kernel arguments
+struct Lattice64 {
+  double *px, *py, *pz; // positions (ext)
+  int8_t *code;         // type, < 0 vacant, MB_FLAG_ITL marks sites near an interstitial
+  double *df;           // F'(rho) (ext)
+  double *rho;          // optional rho output (ext) or nullptr
+  double *vx, *vy, *vz; // velocities (box sites used)
+  double *fx, *fy, *fz; // forces (box sites used)
+  double *nx, *ny, *nz; // positions written by the drift (ext) or nullptr
+};
+
+struct Itl64 {
+  int n;
+  int cap_flag;
+  double *px, *py, *pz;    // current positions
+  double *nx, *ny, *nz;    // next positions
+  double *vx, *vy, *vz, *fx, *fy, *fz, *rho, *df;
+  int8_t *type;
+  int *flag_list;          // flagged box sites (ext index)
+  int *flag_count;         // [0] this step, [1] overflow marker
+  double a0, reach;        // window radius in A (cutoff + skin)
+};
+
+struct StepParams {
+  double rc2;
+  double h;      // 0.5 * dt * ftm2v / mass
+  double dt;
+  double mass;
+  int kick_pre;  // 1: v += h f before the energy sample (closes the previous step)
+  int drift;     // 1: v += h f ; x_next = x + dt v
+};
+
+// kernels (mb_kernels64.cu)
+int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, double rc2,
+                 double *e_partial, int energy, int skip_flagged, cudaStream_t s);
+int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const StepParams &sp,
+                   double *e_partial, int energy, int skip_flagged, cudaStream_t s);
+int launch_itl_mark64(const Geom &g, const Lattice64 &L, const Itl64 &I, cudaStream_t s);
+int launch_itl_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const Itl64 &I,
+                     double rc2, double *e_partial, int energy, cudaStream_t s);
+int launch_itl_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const Itl64 &I,
+                       const StepParams &sp, double *e_partial, int energy, cudaStream_t s);
+int launch_images64(const Geom &g, const Lattice64 &L, int what, cudaStream_t s); // what: 1 pos+code, 2 df
+int launch_kick_drift64(const Geom &g, const Lattice64 &L, const Itl64 &I, const StepParams &sp, cudaStream_t s);
+int launch_reduce(const double *partials, int n, double *out, cudaStream_t s);
+int energy_partials_needed();
+
+// AoS conversion (mb_layout.cu)
+int launch_unpack_ext(const Geom &g, const mb_atom_element *aos, int ext_x, int ext_y, int ext_z, Lattice64 L,
+                      int with_df, int *bad_type, cudaStream_t s);
+int launch_pack_ext(const Geom &g, mb_atom_element *aos, int ext_x, int ext_y, const Lattice64 &L, int what,
+                    cudaStream_t s); // what: 1 rho+df, 2 force, 3 df only
+int launch_unpack_box(const Geom &g, const mb_atom_element *aos, Lattice64 L, int with_f, int *bad_type,
+                      cudaStream_t s);
+int launch_pack_box(const Geom &g, mb_atom_element *aos, const Lattice64 &L, const double *px, const double *py,
+                    const double *pz, double h, int unkick, cudaStream_t s);
+int launch_unpack_box_ids(const Geom &g, const mb_atom_element *aos, Lattice64 L, int with_f, int *bad_type,
+                          int64_t *ids, cudaStream_t s);
+int launch_pack_box_ids(const Geom &g, mb_atom_element *aos, const Lattice64 &L, const double *px, const double *py,
+                        const double *pz, double h, int unkick, const int64_t *ids, cudaStream_t s);
+int launch_df_from_rho(const Geom &g, const DevPot &pot, const Lattice64 &L, cudaStream_t s);
+
+// mixed-precision path (mb_mixed.cu)
+int launch_mixed_step(mb_sim *sim, int energy, int prime);
+int mixed_alloc(mb_sim *sim);
+void mixed_free(mb_sim *sim);
+int mixed_after_upload(mb_sim *sim);
+int mixed_pack_df_rho(mb_sim *sim);
+int mixed_kernel_times(mb_sim *sim, int nsteps, float *rho_ms, float *force_ms);
+
+// ------------------------------------------------------------ utilities
+int device_sm_count();
+
+} // namespace mb

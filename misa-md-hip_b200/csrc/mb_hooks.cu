@@ -1,0 +1,305 @@
+// Drop-in plugin hooks: the misa-md-hip arch-acceleration interface
+// (src/hip_arch_acc_imp.cpp:28-225, src/mem.cpp:14-32, src/cli.cpp:16-27) on the
+// host's ghost-extended AoS lattice.
+//
+// The reference streams z-slabs of the AoS array through two device buffers
+// with a fresh pair of streams per call (src/double-buffer/*).  Here each hook
+// makes one H2D copy of the array, converts it on the device to the split SoA
+// layout, runs one persistent kernel over the whole box and copies the box rows
+// back: same results, same synchronous semantics, no slab bookkeeping (and none
+// of the trailing-layer loss the slab split has when box_z % batches != 0,
+// src/double-buffer/double_buffer.cpp:12,42-47).
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+#include <vector>
+
+#include "mb_common.cuh"
+
+namespace mb {
+
+struct HookCtx {
+  bool env = false, domain = false, stencil = false, pot = false;
+  int device = 0;
+  unsigned int batches = 1;
+  mb_device_domain dom{};
+  Geom g{};
+  StencilSet st{};
+  std::vector<int64_t> even, odd;
+  PotHost *potp = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // device buffers sized for the ext lattice
+  size_t n_ext = 0;
+  mb_atom_element *aos = nullptr;
+  double *px = nullptr, *py = nullptr, *pz = nullptr, *df = nullptr, *rho = nullptr, *fx = nullptr, *fy = nullptr,
+         *fz = nullptr;
+  int8_t *code = nullptr;
+  int *bad = nullptr;
+  float kernel_ms = 0.f, copy_ms = 0.f;
+};
+
+static HookCtx g_ctx;
+static std::mutex g_mu;
+
+static void free_buffers(HookCtx &c) {
+  void *ptrs[] = {c.aos, c.px, c.py, c.pz, c.df, c.rho, c.fx, c.fy, c.fz, c.code, c.bad};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  c.aos = nullptr;
+  c.px = c.py = c.pz = c.df = c.rho = c.fx = c.fy = c.fz = nullptr;
+  c.code = nullptr;
+  c.bad = nullptr;
+  c.n_ext = 0;
+}
+
+static int ensure_buffers(HookCtx &c) {
+  const size_t n = (size_t)c.dom.ext_size_x * c.dom.ext_size_y * c.dom.ext_size_z;
+  if (c.n_ext == n && c.aos) return MB_OK;
+  free_buffers(c);
+  MB_CUDA(cudaMalloc(&c.aos, n * sizeof(mb_atom_element)));
+  double **dp[] = {&c.px, &c.py, &c.pz, &c.df, &c.rho, &c.fx, &c.fy, &c.fz};
+  for (double **p : dp) MB_CUDA(cudaMalloc(p, n * sizeof(double)));
+  MB_CUDA(cudaMalloc(&c.code, (n + 3) & ~(size_t)3));
+  MB_CUDA(cudaMalloc(&c.bad, sizeof(int)));
+  c.n_ext = n;
+  return MB_OK;
+}
+
+static Lattice64 lattice_view(HookCtx &c) {
+  Lattice64 L{};
+  L.px = c.px;
+  L.py = c.py;
+  L.pz = c.pz;
+  L.code = c.code;
+  L.df = c.df;
+  L.rho = c.rho;
+  L.fx = c.fx;
+  L.fy = c.fy;
+  L.fz = c.fz;
+  return L;
+}
+
+static int require_ready(const HookCtx &c) {
+  if (!c.env) return fail(MB_ERR_STATE, "mb_env_init has not been called");
+  if (!c.domain) return fail(MB_ERR_STATE, "mb_domain_init has not been called");
+  if (!c.stencil) return fail(MB_ERR_STATE, "mb_nei_offset_init has not been called");
+  if (!c.pot) return fail(MB_ERR_STATE, "mb_pot_init has not been called");
+  return MB_OK;
+}
+
+// Copy the whole ext array in, convert, run `body`, convert back, copy the box rows out.
+template <class Body>
+static int run_hook(HookCtx &c, mb_atom_element *atoms, int with_df, int pack_what, Body body) {
+  if (!atoms) return fail(MB_ERR_ARG, "null atoms array");
+  MB_TRY(require_ready(c));
+  MB_TRY(ensure_buffers(c));
+  const mb_device_domain &d = c.dom;
+  const size_t n = c.n_ext;
+  const size_t first = ((size_t)d.ghost_size_z * d.ext_size_y + d.ghost_size_y) * d.ext_size_x + d.ghost_size_x;
+  const size_t last = ((size_t)(d.ghost_size_z + d.box_size_z - 1) * d.ext_size_y + d.ghost_size_y + d.box_size_y - 1) *
+                          d.ext_size_x +
+                      d.ghost_size_x + d.box_size_x - 1;
+  cudaStream_t s = c.stream;
+  MB_CUDA(cudaMemsetAsync(c.bad, 0, sizeof(int), s));
+  MB_CUDA(cudaEventRecord(c.ev[0], s));
+  MB_CUDA(cudaMemcpyAsync(c.aos, atoms, n * sizeof(mb_atom_element), cudaMemcpyHostToDevice, s));
+  MB_CUDA(cudaEventRecord(c.ev[1], s));
+  Lattice64 L = lattice_view(c);
+  MB_TRY(launch_unpack_ext(c.g, c.aos, d.ext_size_x, d.ext_size_y, d.ext_size_z, L, with_df, c.bad, s));
+  MB_TRY(body(L, s));
+  MB_TRY(launch_pack_ext(c.g, c.aos, d.ext_size_x, d.ext_size_y, L, pack_what, s));
+  MB_CUDA(cudaEventRecord(c.ev[2], s));
+  MB_CUDA(cudaMemcpyAsync(atoms + first, c.aos + first, (last - first + 1) * sizeof(mb_atom_element),
+                          cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaEventRecord(c.ev[3], s));
+  int bad = 0;
+  MB_CUDA(cudaMemcpyAsync(&bad, c.bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  float a = 0, b = 0, k = 0;
+  cudaEventElapsedTime(&a, c.ev[0], c.ev[1]);
+  cudaEventElapsedTime(&k, c.ev[1], c.ev[2]);
+  cudaEventElapsedTime(&b, c.ev[2], c.ev[3]);
+  c.kernel_ms = k;
+  c.copy_ms = a + b;
+  if (bad) return fail(MB_ERR_ARG, "atom type >= 64 is not supported (treated as vacant)");
+  return MB_OK;
+}
+
+} // namespace mb
+
+using namespace mb;
+
+extern "C" {
+
+int mb_env_init(int device) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  HookCtx &c = g_ctx;
+  int n = 0;
+  MB_CUDA(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return fail(MB_ERR_ARG, "device index out of range");
+  MB_CUDA(cudaSetDevice(device));
+  if (!c.stream) {
+    MB_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    for (auto &e : c.ev) MB_CUDA(cudaEventCreate(&e));
+  }
+  c.device = device;
+  c.env = true;
+  return MB_OK;
+}
+
+int mb_env_clean(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  HookCtx &c = g_ctx;
+  if (c.stream) cudaStreamSynchronize(c.stream);
+  free_buffers(c);
+  if (c.potp) pot_free(c.potp);
+  c.potp = nullptr;
+  for (auto &e : c.ev)
+    if (e) cudaEventDestroy(e), e = nullptr;
+  if (c.stream) cudaStreamDestroy(c.stream);
+  c.stream = nullptr;
+  c.env = c.domain = c.stencil = c.pot = false;
+  return MB_OK;
+}
+
+int mb_domain_init(const mb_device_domain *d) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  HookCtx &c = g_ctx;
+  if (!d) return fail(MB_ERR_ARG, "null domain");
+  if (d->box_size_x <= 0 || d->box_size_y <= 0 || d->box_size_z <= 0) return fail(MB_ERR_ARG, "empty box");
+  if (d->ghost_size_x < 0 || d->ghost_size_y < 0 || d->ghost_size_z < 0) return fail(MB_ERR_ARG, "negative ghost");
+  if ((d->ghost_size_x & 1) || (d->box_size_x & 1))
+    return fail(MB_ERR_ARG, "ghost_size_x and box_size_x are doubled BCC sizes and must be even");
+  if (d->ext_size_x != d->box_size_x + 2 * d->ghost_size_x || d->ext_size_y != d->box_size_y + 2 * d->ghost_size_y ||
+      d->ext_size_z != d->box_size_z + 2 * d->ghost_size_z)
+    return fail(MB_ERR_ARG, "ext size must equal box + 2 * ghost");
+  const long long next = (long long)d->ext_size_x * d->ext_size_y * d->ext_size_z;
+  if (next / 2 > 0x3fffffffLL) return fail(MB_ERR_ARG, "lattice too large for 32-bit stencil offsets");
+  c.dom = *d;
+  Geom &g = c.g;
+  g.ecx = d->ext_size_x / 2;
+  g.ey = d->ext_size_y;
+  g.ez = d->ext_size_z;
+  g.gcx = d->ghost_size_x / 2;
+  g.gy = d->ghost_size_y;
+  g.gz = d->ghost_size_z;
+  g.bcx = d->box_size_x / 2;
+  g.by = d->box_size_y;
+  g.bz = d->box_size_z;
+  g.images = 0; // the host owns the ghost region in drop-in mode
+  g.E = (long long)g.ecx * g.ey * g.ez;
+  g.Lx = g.Ly = g.Lz = 0.0;
+  c.domain = true;
+  // linear offsets are tied to the ext sizes they were made for: a new domain needs
+  // mb_nei_offset_init again (the reference's init order: domain, then offsets)
+  c.stencil = false;
+  c.even.clear();
+  c.odd.clear();
+  return MB_OK;
+}
+
+int mb_nei_offset_init(const int64_t *nei_even, size_t n_even, const int64_t *nei_odd, size_t n_odd) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  HookCtx &c = g_ctx;
+  if (!c.domain) return fail(MB_ERR_STATE, "mb_domain_init must come before mb_nei_offset_init");
+  if ((n_even && !nei_even) || (n_odd && !nei_odd)) return fail(MB_ERR_ARG, "null stencil");
+  // sublattice s of the split layout holds doubled ext columns of parity s; with an
+  // even ghost the global parity of its sites is (s + box_index_start_x) & 1
+  // (the reference selects the stencil by (x + box_index_start_x) % 2,
+  // src/kernels/kernel_itl.hpp:82).
+  const int par[2] = {(int)(c.dom.box_index_start_x & 1), (int)((1 + c.dom.box_index_start_x) & 1)};
+  StencilSet st;
+  MB_TRY(stencil_from_linear(nei_even, n_even, nei_odd, n_odd, c.dom.ext_size_x, c.dom.ext_size_y, c.g, par, &st));
+  c.st = st;
+  c.even.assign(nei_even, nei_even + n_even);
+  c.odd.assign(nei_odd, nei_odd + n_odd);
+  c.stencil = true;
+  return MB_OK;
+}
+
+int mb_pot_init(const mb_eam_tables *t) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  HookCtx &c = g_ctx;
+  if (!c.env) return fail(MB_ERR_STATE, "mb_env_init has not been called");
+  PotHost *p = nullptr;
+  MB_TRY(pot_build(t, &p));
+  if (c.potp) pot_free(c.potp);
+  c.potp = p;
+  c.pot = true;
+  return MB_OK;
+}
+
+int mb_eam_rho_calc(mb_atom_element *atoms, double cutoff_radius) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  HookCtx &c = g_ctx;
+  if (!(cutoff_radius > 0)) return fail(MB_ERR_ARG, "cutoff must be > 0");
+  return run_hook(c, atoms, 0, 1, [&](Lattice64 &L, cudaStream_t s) {
+    return launch_rho64(c.g, c.st, pot_dev(c.potp), L, cutoff_radius * cutoff_radius, nullptr, 0, 0, s);
+  });
+}
+
+int mb_eam_df_calc(mb_atom_element *atoms, double cutoff_radius) {
+  // Full-neighbour build: df already came out of the rho pass
+  // (src/hip_arch_acc_imp.cpp:184-186 returns at once).
+  (void)atoms;
+  (void)cutoff_radius;
+  std::lock_guard<std::mutex> lk(g_mu);
+  return require_ready(g_ctx);
+}
+
+int mb_eam_df_from_rho(mb_atom_element *atoms) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  HookCtx &c = g_ctx;
+  return run_hook(c, atoms, 2, 3,
+                  [&](Lattice64 &L, cudaStream_t s) { return launch_df_from_rho(c.g, pot_dev(c.potp), L, s); });
+}
+
+int mb_eam_force_calc(mb_atom_element *atoms, double cutoff_radius) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  HookCtx &c = g_ctx;
+  if (!(cutoff_radius > 0)) return fail(MB_ERR_ARG, "cutoff must be > 0");
+  return run_hook(c, atoms, 1, 2, [&](Lattice64 &L, cudaStream_t s) {
+    StepParams sp{};
+    sp.rc2 = cutoff_radius * cutoff_radius;
+    Lattice64 Lf = L;
+    Lf.vx = Lf.vy = Lf.vz = nullptr; // forces only, no integration in drop-in mode
+    return launch_force64(c.g, c.st, pot_dev(c.potp), Lf, sp, nullptr, 0, 0, s);
+  });
+}
+
+int mb_create_atoms_mem(void **atoms, size_t data_type_size, int64_t size_x, int64_t size_y, int64_t size_z,
+                        int *allocated) {
+  if (!atoms) return fail(MB_ERR_ARG, "null out pointer");
+  if (allocated) *allocated = 0;
+  if (size_x <= 0 || size_y <= 0 || size_z <= 0 || data_type_size == 0) return fail(MB_ERR_ARG, "empty allocation");
+  const size_t bytes = (size_t)size_x * (size_t)size_y * (size_t)size_z * data_type_size;
+  MB_CUDA(cudaHostAlloc(atoms, bytes, cudaHostAllocPortable));
+  if (allocated) *allocated = 1;
+  return MB_OK;
+}
+
+int mb_release_atoms_mem(void *atoms, int *released) {
+  if (released) *released = 0;
+  if (!atoms) return MB_OK;
+  MB_CUDA(cudaFreeHost(atoms));
+  if (released) *released = 1;
+  return MB_OK;
+}
+
+int mb_cli_set_batches(unsigned int batches) {
+  if (batches == 0) return fail(MB_ERR_ARG, "batches must be >= 1");
+  g_ctx.batches = batches;
+  return MB_OK;
+}
+
+unsigned int mb_cli_batches(void) { return g_ctx.batches; }
+
+int mb_hook_last_timing(float *kernel_ms, float *copy_ms) {
+  if (kernel_ms) *kernel_ms = g_ctx.kernel_ms;
+  if (copy_ms) *copy_ms = g_ctx.copy_ms;
+  return MB_OK;
+}
+
+} // extern "C"

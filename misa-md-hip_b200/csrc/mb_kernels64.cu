@@ -1,0 +1,902 @@
+// Plain FP64 EAM lattice kernels (the drop-in path).
+//
+// Reference semantics (misa-md-hip): one result per box site with type >= 0; the
+// site walks the parity-selected stencil, skips vacant neighbours and pairs with
+// r^2 >= rc^2; rho takes the NEIGHBOUR's density function and df = F'(rho) is
+// fused after the sum (src/kernels/kernel_itl.hpp:69-105,
+// src/kernels/kernel_pairs.hpp:21-32); the force is sum del * fpair with
+// fpair = -(df_i f'_{t_j} + df_j f'_{t_i} + phi'_{t_i t_j}) / r, overwritten
+// (src/kernels/kernel_pairs.hpp:39-60).
+//
+// B200 design:
+//  * sublattice-split SoA: a warp is 32 consecutive sites of one sublattice row,
+//    so every stencil entry is one contiguous, coalesced 256-byte row fetch per
+//    coordinate, and the stencil offset is warp-uniform (read from the kernel's
+//    parameter bank);
+//  * vacant sites carry a far-away position, so the r^2 test rejects them with no
+//    type fetch;
+//  * the spline pieces of the hot function live in shared memory (loaded once per
+//    persistent CTA): random per-lane knot gathers are served by shared-memory
+//    banks instead of L1 tag lookups;
+//  * sites near the domain faces write their periodic ghost images themselves
+//    (no separate ghost-exchange pass), and the force pass closes the previous
+//    velocity-Verlet step and drifts to the next positions (double-buffered).
+#include <stdio.h>
+
+#include "mb_common.cuh"
+
+namespace mb {
+
+#define MB_EPART_CAP 4096 // CTA partial sums per energy region
+#define MB_MAIN_THREADS 512
+#define MB_ITL_THREADS 256
+
+int energy_partials_needed() { return 8 * MB_EPART_CAP; }
+
+// ------------------------------------------------------------ spline helpers
+__device__ __forceinline__ void spl_locate(double x, double rdx, int n, int &m, double &p) {
+  const double pp = x * rdx;
+  if (!(pp < (double)(n - 1))) {
+    m = n - 2;
+    p = 1.0;
+    return;
+  }
+  int mm = (int)pp;
+  mm = min(mm, n - 2);
+  p = fmin(pp - (double)mm, 1.0);
+  m = mm;
+}
+__device__ __forceinline__ double cubic(const double4 c, double p) { return ((c.w * p + c.z) * p + c.y) * p + c.x; }
+__device__ __forceinline__ double quad(const double4 d, double p) { return (d.z * p + d.y) * p + d.x; }
+__device__ __forceinline__ int pair_idx(int a, int b, int nt) {
+  if (a > b) {
+    int t = a;
+    a = b;
+    b = t;
+  }
+  return a * nt - a * (a - 1) / 2 + (b - a);
+}
+__device__ __forceinline__ double dF64(const DevPot &P, int t, double rho) {
+  int m;
+  double p;
+  spl_locate(rho, P.rdrho, P.nrho, m, p);
+  return quad(ldg4(&P.F_der[(size_t)t * P.nrho + m]), p);
+}
+__device__ __forceinline__ double F64(const DevPot &P, int t, double rho) {
+  if (rho > P.rho_max)
+    return ldg4(&P.F_val[(size_t)t * P.nrho + P.nrho - 1]).x + dF64(P, t, rho) * (rho - P.rho_max);
+  int m;
+  double p;
+  spl_locate(rho, P.rdrho, P.nrho, m, p);
+  return cubic(ldg4(&P.F_val[(size_t)t * P.nrho + m]), p);
+}
+__device__ __forceinline__ double rho_of_r(const DevPot &P, int t, double r) {
+  int m;
+  double p;
+  spl_locate(r, P.rdr, P.nr, m, p);
+  return cubic(ldg4(&P.f_val[(size_t)t * P.nr + m]), p);
+}
+// fpair * r for a pair (general types, global tables)
+__device__ __forceinline__ double pair_psip(const DevPot &P, int ti, int tj, double r, double dfi, double dfj,
+                                            double *phi_out) {
+  int m;
+  double p;
+  spl_locate(r, P.rdr, P.nr, m, p);
+  const double fj = quad(ldg4(&P.f_der[(size_t)tj * P.nr + m]), p);
+  const double fi = (ti == tj) ? fj : quad(ldg4(&P.f_der[(size_t)ti * P.nr + m]), p);
+  const int q = pair_idx(ti, tj, P.n_types);
+  const double ph = quad(ldg4(&P.phi_der[(size_t)q * P.nr + m]), p);
+  if (phi_out) *phi_out = cubic(ldg4(&P.phi_val[(size_t)q * P.nr + m]), p);
+  return dfi * fj + dfj * fi + ph;
+}
+
+// -------------------------------------------------------------- geometry
+__device__ __forceinline__ long long ext_index(const Geom &g, int s, int cx, int y, int z) {
+  return (long long)s * g.E + ((long long)(z + g.gz) * g.ey + (y + g.gy)) * g.ecx + (cx + g.gcx);
+}
+__device__ __forceinline__ void decode_ext(const Geom &g, long long i, int &s, int &cx, int &y, int &z) {
+  s = (int)(i / g.E);
+  long long r = i - (long long)s * g.E;
+  const long long row = r / g.ecx;
+  cx = (int)(r - row * g.ecx) - g.gcx;
+  z = (int)(row / g.ey) - g.gz;
+  y = (int)(row - (long long)(z + g.gz) * g.ey) - g.gy;
+}
+
+// Calls fn(ext_index, shift_x, shift_y, shift_z) for every periodic ghost image
+// of box site (s, cx, y, z).  Requires box >= ghost in every dimension.
+template <class Fn>
+__device__ __forceinline__ void for_images(const Geom &g, int s, int cx, int y, int z, Fn fn) {
+  const bool xo[3] = {true, cx >= g.bcx - g.gcx, cx < g.gcx};
+  const bool yo[3] = {true, y >= g.by - g.gy, y < g.gy};
+  const bool zo[3] = {true, z >= g.bz - g.gz, z < g.gz};
+  if (!(xo[1] || xo[2] || yo[1] || yo[2] || zo[1] || zo[2])) return;
+  const int xs[3] = {cx + g.gcx, cx + g.gcx - g.bcx, cx + g.gcx + g.bcx};
+  const int ys[3] = {y + g.gy, y + g.gy - g.by, y + g.gy + g.by};
+  const int zs[3] = {z + g.gz, z + g.gz - g.bz, z + g.gz + g.bz};
+  const double sx[3] = {0.0, -g.Lx, g.Lx}, sy[3] = {0.0, -g.Ly, g.Ly}, sz[3] = {0.0, -g.Lz, g.Lz};
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if (!zo[c]) continue;
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      if (!yo[b]) continue;
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        if (!xo[a] || (a == 0 && b == 0 && c == 0)) continue;
+        const long long idx = (long long)s * g.E + ((long long)zs[c] * g.ey + ys[b]) * g.ecx + xs[a];
+        fn(idx, sx[a], sy[b], sz[c]);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic block sum (fixed shuffle tree, then warps in order); result in thread 0.
+__device__ double block_sum(double v) {
+  __shared__ double red[32];
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += red[k];
+  return t;
+}
+
+// -------------------------------------------------------------- rho pass
+struct RhoArgs {
+  Geom g;
+  DevPot P;
+  Lattice64 L;
+  double rc2;
+  double *e_partial;
+  int skip_flagged;
+  int m_lo;      // first knot kept in shared memory
+  int chunks;    // 32-site chunks per row
+  long long n_items;
+};
+
+template <bool ENERGY, bool ONE_TYPE>
+__global__ void __launch_bounds__(MB_MAIN_THREADS, 1)
+    k_rho64(const __grid_constant__ StencilSet st, const __grid_constant__ RhoArgs a) {
+  extern __shared__ double4 s_fval[];
+  const DevPot &P = a.P;
+  const int nsm = P.nr - a.m_lo;
+  for (int k = threadIdx.x; k < nsm; k += blockDim.x) s_fval[k] = P.f_val[a.m_lo + k];
+  __syncthreads();
+
+  const Geom &g = a.g;
+  const Lattice64 &L = a.L;
+  const int lane = threadIdx.x & 31;
+  const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+  double e_acc = 0.0;
+  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.n_items; w += wstride) {
+    long long t = w;
+    const int chunk = (int)(t % a.chunks);
+    t /= a.chunks;
+    const int y = (int)(t % g.by);
+    t /= g.by;
+    const int s = (int)(t & 1);
+    const int z = (int)(t >> 1);
+    const int cx = chunk * 32 + lane;
+    if (cx >= g.bcx) continue;
+    const long long i = ext_index(g, s, cx, y, z);
+    const int code = L.code[i];
+    if (code < 0 || (a.skip_flagged && (code & MB_FLAG_ITL))) continue;
+    const int ti = code & 0x3F;
+    const double xi = L.px[i], yi = L.py[i], zi = L.pz[i];
+    const int *off = st.off[s];
+    double rho = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < st.n; k++) {
+      const long long j = i + off[k];
+      const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 < a.rc2) {
+        const double r = d2 * rsqrt(d2);
+        int m;
+        double p;
+        spl_locate(r, P.rdr, P.nr, m, p);
+        if (ONE_TYPE) {
+          const double4 c = (m >= a.m_lo) ? s_fval[m - a.m_lo] : ldg4(&P.f_val[m]);
+          rho += cubic(c, p);
+        } else {
+          const int tj = L.code[j] & 0x3F;
+          rho += cubic(ldg4(&P.f_val[(size_t)tj * P.nr + m]), p);
+        }
+      }
+    }
+    const double df = dF64(P, ti, rho);
+    L.df[i] = df;
+    if (L.rho) L.rho[i] = rho;
+    if (g.images) for_images(g, s, cx, y, z, [&](long long idx, double, double, double) { L.df[idx] = df; });
+    if (ENERGY) e_acc += F64(P, ti, rho);
+  }
+  if (ENERGY) {
+    const double t = block_sum(e_acc);
+    if (threadIdx.x == 0) a.e_partial[blockIdx.x] = t;
+  }
+}
+
+// ------------------------------------------------------------ force pass
+struct ForceArgs {
+  Geom g;
+  DevPot P;
+  Lattice64 L;
+  StepParams sp;
+  double *e_pair;    // CTA partials of 1/2 sum phi
+  double *e_kin;     // CTA partials of kinetic energy
+  int skip_flagged;
+  int m_lo;
+  int chunks;
+  long long n_items;
+};
+
+template <bool ENERGY, bool ONE_TYPE>
+__global__ void __launch_bounds__(MB_MAIN_THREADS, 1)
+    k_force64(const __grid_constant__ StencilSet st, const __grid_constant__ ForceArgs a) {
+  extern __shared__ double2 s_f1[]; // [knot][3]
+  const DevPot &P = a.P;
+  if (ONE_TYPE) {
+    const int nsm = (P.nr - a.m_lo) * 3;
+    for (int k = threadIdx.x; k < nsm; k += blockDim.x) s_f1[k] = P.force1[(size_t)a.m_lo * 3 + k];
+    __syncthreads();
+  }
+  const Geom &g = a.g;
+  const Lattice64 &L = a.L;
+  const StepParams &sp = a.sp;
+  const int lane = threadIdx.x & 31;
+  const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+  double e_pair = 0.0, e_kin = 0.0;
+  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.n_items; w += wstride) {
+    long long t = w;
+    const int chunk = (int)(t % a.chunks);
+    t /= a.chunks;
+    const int y = (int)(t % g.by);
+    t /= g.by;
+    const int s = (int)(t & 1);
+    const int z = (int)(t >> 1);
+    const int cx = chunk * 32 + lane;
+    if (cx >= g.bcx) continue;
+    const long long i = ext_index(g, s, cx, y, z);
+    const int code = L.code[i];
+    if (code < 0 || (a.skip_flagged && (code & MB_FLAG_ITL))) continue;
+    const int ti = code & 0x3F;
+    const double xi = L.px[i], yi = L.py[i], zi = L.pz[i];
+    const double dfi = L.df[i];
+    const int *off = st.off[s];
+    double fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < st.n; k++) {
+      const long long j = i + off[k];
+      const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 < sp.rc2) {
+        const double rinv = rsqrt(d2);
+        const double r = d2 * rinv;
+        const double dfj = L.df[j];
+        double psip;
+        if (ONE_TYPE) {
+          int m;
+          double p;
+          spl_locate(r, P.rdr, P.nr, m, p);
+          double2 c0, c1, c2;
+          if (m >= a.m_lo) {
+            const double2 *q = s_f1 + (size_t)(m - a.m_lo) * 3;
+            c0 = q[0];
+            c1 = q[1];
+            c2 = q[2];
+          } else {
+            const double2 *q = P.force1 + (size_t)m * 3;
+            c0 = __ldg(q);
+            c1 = __ldg(q + 1);
+            c2 = __ldg(q + 2);
+          }
+          const double fp = (c2.x * p + c1.x) * p + c0.x;
+          const double pp = (c2.y * p + c1.y) * p + c0.y;
+          psip = (dfi + dfj) * fp + pp;
+          if (ENERGY) ep += 0.5 * cubic(ldg4(&P.phi_val[m]), p);
+        } else {
+          const int tj = L.code[j] & 0x3F;
+          double ph = 0.0;
+          psip = pair_psip(P, ti, tj, r, dfi, dfj, ENERGY ? &ph : nullptr);
+          if (ENERGY) ep += 0.5 * ph;
+        }
+        const double fpair = -psip * rinv;
+        fx += dx * fpair;
+        fy += dy * fpair;
+        fz += dz * fpair;
+      }
+    }
+    if (L.fx) {
+      L.fx[i] = fx;
+      L.fy[i] = fy;
+      L.fz[i] = fz;
+    }
+    if (L.vx) {
+      double vx = L.vx[i], vy = L.vy[i], vz = L.vz[i];
+      if (sp.kick_pre) {
+        vx += sp.h * fx;
+        vy += sp.h * fy;
+        vz += sp.h * fz;
+      }
+      if (ENERGY) e_kin += 0.5 * sp.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E;
+      if (sp.drift) {
+        vx += sp.h * fx;
+        vy += sp.h * fy;
+        vz += sp.h * fz;
+        const double nx = xi + sp.dt * vx, ny = yi + sp.dt * vy, nz = zi + sp.dt * vz;
+        L.nx[i] = nx;
+        L.ny[i] = ny;
+        L.nz[i] = nz;
+        if (g.images)
+          for_images(g, s, cx, y, z, [&](long long idx, double ox, double oy, double oz) {
+            L.nx[idx] = nx + ox;
+            L.ny[idx] = ny + oy;
+            L.nz[idx] = nz + oz;
+          });
+      }
+      L.vx[i] = vx;
+      L.vy[i] = vy;
+      L.vz[i] = vz;
+    }
+    if (ENERGY) e_pair += ep;
+  }
+  if (ENERGY) {
+    const double t1 = block_sum(e_pair);
+    if (threadIdx.x == 0) a.e_pair[blockIdx.x] = t1;
+    const double t2 = block_sum(e_kin);
+    if (threadIdx.x == 0) a.e_kin[blockIdx.x] = t2;
+  }
+}
+
+// ----------------------------------------------------------- launchers
+static int grid_for(long long warps_needed, int threads) {
+  const long long ctas = (warps_needed * 32 + threads - 1) / threads;
+  long long cap = device_sm_count();
+  if (cap > MB_EPART_CAP) cap = MB_EPART_CAP;
+  return (int)(ctas < cap ? (ctas > 0 ? ctas : 1) : cap);
+}
+
+static const int kSmemCap = 200 * 1024;
+
+int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, double rc2,
+                 double *e_partial, int energy, int skip_flagged, cudaStream_t s) {
+  RhoArgs a;
+  a.g = g;
+  a.P = pot;
+  a.L = L;
+  a.rc2 = rc2;
+  a.e_partial = e_partial;
+  a.skip_flagged = skip_flagged;
+  const bool one = pot.n_types == 1;
+  int nsm = pot.nr;
+  if (nsm * (int)sizeof(double4) > kSmemCap) nsm = kSmemCap / (int)sizeof(double4);
+  if (!one) nsm = 0;
+  a.m_lo = pot.nr - nsm;
+  a.chunks = (g.bcx + 31) / 32;
+  a.n_items = (long long)a.chunks * g.by * 2 * g.bz;
+  const size_t smem = (size_t)nsm * sizeof(double4);
+  const int grid = grid_for(a.n_items, MB_MAIN_THREADS);
+  static bool attr_done = false;
+  if (!attr_done) {
+    MB_CUDA(cudaFuncSetAttribute(k_rho64<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap));
+    MB_CUDA(cudaFuncSetAttribute(k_rho64<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap));
+    attr_done = true;
+  }
+  if (one) {
+    if (energy)
+      k_rho64<true, true><<<grid, MB_MAIN_THREADS, smem, s>>>(st, a);
+    else
+      k_rho64<false, true><<<grid, MB_MAIN_THREADS, smem, s>>>(st, a);
+  } else {
+    if (energy)
+      k_rho64<true, false><<<grid, MB_MAIN_THREADS, 0, s>>>(st, a);
+    else
+      k_rho64<false, false><<<grid, MB_MAIN_THREADS, 0, s>>>(st, a);
+  }
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const StepParams &sp,
+                   double *e_partial, int energy, int skip_flagged, cudaStream_t s) {
+  ForceArgs a;
+  a.g = g;
+  a.P = pot;
+  a.L = L;
+  a.sp = sp;
+  a.e_pair = e_partial ? e_partial + MB_EPART_CAP : nullptr;
+  a.e_kin = e_partial ? e_partial + 2 * MB_EPART_CAP : nullptr;
+  a.skip_flagged = skip_flagged;
+  const bool one = pot.n_types == 1;
+  int nsm = pot.nr;
+  if (nsm * (int)(3 * sizeof(double2)) > kSmemCap) nsm = kSmemCap / (int)(3 * sizeof(double2));
+  if (!one) nsm = 0;
+  a.m_lo = pot.nr - nsm;
+  a.chunks = (g.bcx + 31) / 32;
+  a.n_items = (long long)a.chunks * g.by * 2 * g.bz;
+  const size_t smem = (size_t)nsm * 3 * sizeof(double2);
+  const int grid = grid_for(a.n_items, MB_MAIN_THREADS);
+  static bool attr_done = false;
+  if (!attr_done) {
+    MB_CUDA(cudaFuncSetAttribute(k_force64<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap));
+    MB_CUDA(cudaFuncSetAttribute(k_force64<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap));
+    attr_done = true;
+  }
+  if (one) {
+    if (energy)
+      k_force64<true, true><<<grid, MB_MAIN_THREADS, smem, s>>>(st, a);
+    else
+      k_force64<false, true><<<grid, MB_MAIN_THREADS, smem, s>>>(st, a);
+  } else {
+    if (energy)
+      k_force64<true, false><<<grid, MB_MAIN_THREADS, 0, s>>>(st, a);
+    else
+      k_force64<false, false><<<grid, MB_MAIN_THREADS, 0, s>>>(st, a);
+  }
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+// ----------------------------------------------------- interstitial passes
+// Lattice sites whose IDEAL position lies within reach of an interstitial are
+// flagged (site code bit MB_FLAG_ITL) and skipped by the lattice passes; the
+// warp-per-item kernels below recompute them in full (stencil + interstitials)
+// together with the interstitials themselves.  Every pair with r < cutoff is thus
+// seen from both sides as long as no lattice atom strays more than
+// (reach - cutoff) from its site.
+
+struct Window {
+  int gx0, gy0, gz0, nx, ny, nz;
+};
+
+__device__ __forceinline__ Window make_window(double qx, double qy, double qz, double a0, double R) {
+  Window w;
+  w.gx0 = (int)floor((qx - R) / (0.5 * a0));
+  const int gx1 = (int)ceil((qx + R) / (0.5 * a0));
+  w.gy0 = (int)floor((qy - R) / a0) - 1;
+  const int gy1 = (int)ceil((qy + R) / a0);
+  w.gz0 = (int)floor((qz - R) / a0) - 1;
+  const int gz1 = (int)ceil((qz + R) / a0);
+  w.nx = gx1 - w.gx0 + 1;
+  w.ny = gy1 - w.gy0 + 1;
+  w.nz = gz1 - w.gz0 + 1;
+  return w;
+}
+
+__device__ __forceinline__ int pmod_i(int a, int b) {
+  int r = a % b;
+  return r < 0 ? r + b : r;
+}
+
+// Candidate c of window w: returns false when its ideal site is out of reach;
+// otherwise the ext index of the box site and the periodic shift of the image.
+__device__ __forceinline__ bool window_site(const Geom &g, const Window &w, int c, double qx, double qy, double qz,
+                                            double a0, double R, long long &idx, double &sx, double &sy,
+                                            double &sz) {
+  const int ix = c % w.nx;
+  const int rest = c / w.nx;
+  const int iy = rest % w.ny;
+  const int iz = rest / w.ny;
+  const int gx = w.gx0 + ix, gy = w.gy0 + iy, gz = w.gz0 + iz;
+  const double h = 0.5 * (double)(gx & 1);
+  const double ox = 0.5 * a0 * gx - qx, oy = a0 * (gy + h) - qy, oz = a0 * (gz + h) - qz;
+  if (ox * ox + oy * oy + oz * oz >= R * R) return false;
+  const int bxd = 2 * g.bcx;
+  const int bx = pmod_i(gx, bxd), by = pmod_i(gy, g.by), bz = pmod_i(gz, g.bz);
+  sx = (double)((gx - bx) / bxd) * g.Lx;
+  sy = (double)((gy - by) / g.by) * g.Ly;
+  sz = (double)((gz - bz) / g.bz) * g.Lz;
+  idx = ext_index(g, bx & 1, bx >> 1, by, bz);
+  return true;
+}
+
+__device__ __forceinline__ double min_image(double d, double L) { return d - L * rint(d / L); }
+
+__global__ void __launch_bounds__(1024) k_itl_mark(const Geom g, const Lattice64 L, const Itl64 I) {
+  // clear last step's flags
+  const int nold = min(I.flag_count[0], I.cap_flag);
+  for (int k = threadIdx.x; k < nold; k += blockDim.x) {
+    const int idx = I.flag_list[k];
+    L.code[idx] = (int8_t)(L.code[idx] & ~MB_FLAG_ITL);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) I.flag_count[0] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int it = threadIdx.x >> 5; it < I.n; it += blockDim.x >> 5) {
+    const double qx = I.px[it], qy = I.py[it], qz = I.pz[it];
+    const Window w = make_window(qx, qy, qz, I.a0, I.reach);
+    const int ncand = w.nx * w.ny * w.nz;
+    for (int c = lane; c < ncand; c += 32) {
+      long long idx;
+      double sx, sy, sz;
+      if (!window_site(g, w, c, qx, qy, qz, I.a0, I.reach, idx, sx, sy, sz)) continue;
+      if (L.code[idx] < 0) continue;
+      const uintptr_t addr = (uintptr_t)(L.code + idx);
+      unsigned int *word = (unsigned int *)(addr & ~(uintptr_t)3);
+      const unsigned int bit = (unsigned int)MB_FLAG_ITL << (8 * (addr & 3));
+      const unsigned int old = atomicOr(word, bit);
+      if (!(old & bit)) {
+        const int slot = atomicAdd(&I.flag_count[0], 1);
+        if (slot < I.cap_flag)
+          I.flag_list[slot] = (int)idx;
+        else
+          I.flag_count[1] = 1; // overflow: reported by the host
+      }
+    }
+  }
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(MB_ITL_THREADS)
+    k_itl_rho64(const __grid_constant__ StencilSet st, const Geom g, const DevPot P, const Lattice64 L, const Itl64 I,
+                double rc2, double *e_partial) {
+  const int lane = threadIdx.x & 31;
+  const int nflag = min(I.flag_count[0], I.cap_flag);
+  const long long n_items = (long long)nflag + I.n;
+  const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+  double e_acc = 0.0;
+  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_items; w += wstride) {
+    if (w < nflag) {
+      const long long i = I.flag_list[w];
+      int s, cx, y, z;
+      decode_ext(g, i, s, cx, y, z);
+      const int ti = L.code[i] & 0x3F;
+      const double xi = L.px[i], yi = L.py[i], zi = L.pz[i];
+      double rho = 0.0;
+      for (int k = lane; k < st.n; k += 32) {
+        const long long j = i + st.off[s][k];
+        const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < rc2) rho += rho_of_r(P, L.code[j] & 0x3F, d2 * rsqrt(d2));
+      }
+      for (int K = lane; K < I.n; K += 32) {
+        const double dx = min_image(xi - I.px[K], g.Lx), dy = min_image(yi - I.py[K], g.Ly),
+                     dz = min_image(zi - I.pz[K], g.Lz);
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < rc2) rho += rho_of_r(P, I.type[K], d2 * rsqrt(d2));
+      }
+      rho = warp_sum(rho);
+      if (lane == 0) {
+        const double df = dF64(P, ti, rho);
+        L.df[i] = df;
+        if (L.rho) L.rho[i] = rho;
+        if (g.images) for_images(g, s, cx, y, z, [&](long long idx, double, double, double) { L.df[idx] = df; });
+        if (ENERGY) e_acc += F64(P, ti, rho);
+      }
+    } else {
+      const int it = (int)(w - nflag);
+      const double qx = I.px[it], qy = I.py[it], qz = I.pz[it];
+      const Window win = make_window(qx, qy, qz, I.a0, I.reach);
+      const int ncand = win.nx * win.ny * win.nz;
+      double rho = 0.0;
+      for (int c = lane; c < ncand; c += 32) {
+        long long j;
+        double sx, sy, sz;
+        if (!window_site(g, win, c, qx, qy, qz, I.a0, I.reach, j, sx, sy, sz)) continue;
+        const int cj = L.code[j];
+        if (cj < 0) continue;
+        const double dx = qx - (L.px[j] + sx), dy = qy - (L.py[j] + sy), dz = qz - (L.pz[j] + sz);
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < rc2) rho += rho_of_r(P, cj & 0x3F, d2 * rsqrt(d2));
+      }
+      for (int K = lane; K < I.n; K += 32) {
+        if (K == it) continue;
+        const double dx = min_image(qx - I.px[K], g.Lx), dy = min_image(qy - I.py[K], g.Ly),
+                     dz = min_image(qz - I.pz[K], g.Lz);
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < rc2) rho += rho_of_r(P, I.type[K], d2 * rsqrt(d2));
+      }
+      rho = warp_sum(rho);
+      if (lane == 0) {
+        const int t = I.type[it];
+        I.rho[it] = rho;
+        I.df[it] = dF64(P, t, rho);
+        if (ENERGY) e_acc += F64(P, t, rho);
+      }
+    }
+  }
+  if (ENERGY) {
+    const double t = block_sum(e_acc);
+    if (threadIdx.x == 0) e_partial[blockIdx.x] = t;
+  }
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(MB_ITL_THREADS)
+    k_itl_force64(const __grid_constant__ StencilSet st, const Geom g, const DevPot P, const Lattice64 L,
+                  const Itl64 I, const StepParams sp, double *e_pair, double *e_kin) {
+  const int lane = threadIdx.x & 31;
+  const int nflag = min(I.flag_count[0], I.cap_flag);
+  const long long n_items = (long long)nflag + I.n;
+  const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+  double ep_acc = 0.0, ek_acc = 0.0;
+  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_items; w += wstride) {
+    const bool is_site = w < nflag;
+    long long i = 0;
+    int s = 0, cx = 0, y = 0, z = 0, it = 0, ti;
+    double xi, yi, zi, dfi;
+    if (is_site) {
+      i = I.flag_list[w];
+      decode_ext(g, i, s, cx, y, z);
+      ti = L.code[i] & 0x3F;
+      xi = L.px[i];
+      yi = L.py[i];
+      zi = L.pz[i];
+      dfi = L.df[i];
+    } else {
+      it = (int)(w - nflag);
+      ti = I.type[it];
+      xi = I.px[it];
+      yi = I.py[it];
+      zi = I.pz[it];
+      dfi = I.df[it];
+    }
+    double fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
+    auto add_pair = [&](double dx, double dy, double dz, int tj, double dfj) {
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 >= sp.rc2) return;
+      const double rinv = rsqrt(d2);
+      double ph = 0.0;
+      const double psip = pair_psip(P, ti, tj, d2 * rinv, dfi, dfj, ENERGY ? &ph : nullptr);
+      const double fpair = -psip * rinv;
+      fx += dx * fpair;
+      fy += dy * fpair;
+      fz += dz * fpair;
+      if (ENERGY) ep += 0.5 * ph;
+    };
+    if (is_site) {
+      for (int k = lane; k < st.n; k += 32) {
+        const long long j = i + st.off[s][k];
+        const int cj = L.code[j];
+        if (cj < 0) continue;
+        add_pair(xi - L.px[j], yi - L.py[j], zi - L.pz[j], cj & 0x3F, L.df[j]);
+      }
+    } else {
+      const Window win = make_window(xi, yi, zi, I.a0, I.reach);
+      const int ncand = win.nx * win.ny * win.nz;
+      for (int c = lane; c < ncand; c += 32) {
+        long long j;
+        double sx, sy, sz;
+        if (!window_site(g, win, c, xi, yi, zi, I.a0, I.reach, j, sx, sy, sz)) continue;
+        const int cj = L.code[j];
+        if (cj < 0) continue;
+        add_pair(xi - (L.px[j] + sx), yi - (L.py[j] + sy), zi - (L.pz[j] + sz), cj & 0x3F, L.df[j]);
+      }
+    }
+    for (int K = lane; K < I.n; K += 32) {
+      if (!is_site && K == it) continue;
+      add_pair(min_image(xi - I.px[K], g.Lx), min_image(yi - I.py[K], g.Ly), min_image(zi - I.pz[K], g.Lz),
+               I.type[K], I.df[K]);
+    }
+    fx = warp_sum(fx);
+    fy = warp_sum(fy);
+    fz = warp_sum(fz);
+    if (ENERGY) ep = warp_sum(ep);
+    if (lane == 0) {
+      double *vxp = is_site ? L.vx : I.vx;
+      const long long vi = is_site ? i : it;
+      if (is_site) {
+        if (L.fx) {
+          L.fx[i] = fx;
+          L.fy[i] = fy;
+          L.fz[i] = fz;
+        }
+      } else {
+        I.fx[it] = fx;
+        I.fy[it] = fy;
+        I.fz[it] = fz;
+      }
+      if (vxp) {
+        double *vyp = is_site ? L.vy : I.vy, *vzp = is_site ? L.vz : I.vz;
+        double vx = vxp[vi], vy = vyp[vi], vz = vzp[vi];
+        if (sp.kick_pre) {
+          vx += sp.h * fx;
+          vy += sp.h * fy;
+          vz += sp.h * fz;
+        }
+        if (ENERGY) ek_acc += 0.5 * sp.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E;
+        if (sp.drift) {
+          vx += sp.h * fx;
+          vy += sp.h * fy;
+          vz += sp.h * fz;
+          const double nx = xi + sp.dt * vx, ny = yi + sp.dt * vy, nz = zi + sp.dt * vz;
+          if (is_site) {
+            L.nx[i] = nx;
+            L.ny[i] = ny;
+            L.nz[i] = nz;
+            if (g.images)
+              for_images(g, s, cx, y, z, [&](long long idx, double ox, double oy, double oz) {
+                L.nx[idx] = nx + ox;
+                L.ny[idx] = ny + oy;
+                L.nz[idx] = nz + oz;
+              });
+          } else {
+            I.nx[it] = nx;
+            I.ny[it] = ny;
+            I.nz[it] = nz;
+          }
+        }
+        vxp[vi] = vx;
+        vyp[vi] = vy;
+        vzp[vi] = vz;
+      }
+      if (ENERGY) ep_acc += ep;
+    }
+  }
+  if (ENERGY) {
+    const double t1 = block_sum(ep_acc);
+    if (threadIdx.x == 0) e_pair[blockIdx.x] = t1;
+    const double t2 = block_sum(ek_acc);
+    if (threadIdx.x == 0) e_kin[blockIdx.x] = t2;
+  }
+}
+
+int launch_itl_mark64(const Geom &g, const Lattice64 &L, const Itl64 &I, cudaStream_t s) {
+  k_itl_mark<<<1, 1024, 0, s>>>(g, L, I);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+static int itl_grid(const Itl64 &I) {
+  const long long warps = (long long)I.cap_flag + I.n;
+  long long ctas = (warps * 32 + MB_ITL_THREADS - 1) / MB_ITL_THREADS;
+  const long long cap = 4LL * device_sm_count();
+  if (ctas > cap) ctas = cap;
+  if (ctas > MB_EPART_CAP) ctas = MB_EPART_CAP;
+  return (int)(ctas > 0 ? ctas : 1);
+}
+
+int launch_itl_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const Itl64 &I,
+                     double rc2, double *e_partial, int energy, cudaStream_t s) {
+  if (I.n == 0) return MB_OK;
+  const int grid = itl_grid(I);
+  if (energy)
+    k_itl_rho64<true><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, rc2, e_partial + 3 * MB_EPART_CAP);
+  else
+    k_itl_rho64<false><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, rc2, nullptr);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+int launch_itl_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const Itl64 &I,
+                       const StepParams &sp, double *e_partial, int energy, cudaStream_t s) {
+  if (I.n == 0) return MB_OK;
+  const int grid = itl_grid(I);
+  if (energy)
+    k_itl_force64<true><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, sp, e_partial + 4 * MB_EPART_CAP,
+                                                         e_partial + 5 * MB_EPART_CAP);
+  else
+    k_itl_force64<false><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, sp, nullptr, nullptr);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+// ------------------------------------------------ images / kick-drift
+__global__ void k_images64(const Geom g, const Lattice64 L, int what) {
+  const long long n = 2LL * g.bcx * g.by * g.bz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int cx = (int)(t % g.bcx);
+    long long r = t / g.bcx;
+    const int y = (int)(r % g.by);
+    r /= g.by;
+    const int s = (int)(r & 1);
+    const int z = (int)(r >> 1);
+    const long long i = ext_index(g, s, cx, y, z);
+    if (what & 1) {
+      const double x0 = L.px[i], y0 = L.py[i], z0 = L.pz[i];
+      const int8_t c = L.code[i];
+      for_images(g, s, cx, y, z, [&](long long idx, double ox, double oy, double oz) {
+        L.px[idx] = x0 + ox;
+        L.py[idx] = y0 + oy;
+        L.pz[idx] = z0 + oz;
+        L.code[idx] = (int8_t)(c < 0 ? c : (c & 0x3F));
+      });
+    }
+    if (what & 2) {
+      const double d = L.df[i];
+      for_images(g, s, cx, y, z, [&](long long idx, double, double, double) { L.df[idx] = d; });
+    }
+  }
+}
+
+int launch_images64(const Geom &g, const Lattice64 &L, int what, cudaStream_t s) {
+  const long long n = 2LL * g.bcx * g.by * g.bz;
+  int grid = (int)((n + 255) / 256);
+  if (grid > 8 * device_sm_count()) grid = 8 * device_sm_count();
+  k_images64<<<grid, 256, 0, s>>>(g, L, what);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+// First half of a velocity-Verlet step in place (used when the state arrives
+// from the host each step): v += h f ; x += dt v, then refresh ghost images.
+__global__ void k_kick_drift64(const Geom g, const Lattice64 L, const Itl64 I, const StepParams sp) {
+  const long long n = 2LL * g.bcx * g.by * g.bz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n + I.n;
+       t += (long long)gridDim.x * blockDim.x) {
+    if (t >= n) {
+      const int it = (int)(t - n);
+      I.vx[it] += sp.h * I.fx[it];
+      I.vy[it] += sp.h * I.fy[it];
+      I.vz[it] += sp.h * I.fz[it];
+      I.px[it] += sp.dt * I.vx[it];
+      I.py[it] += sp.dt * I.vy[it];
+      I.pz[it] += sp.dt * I.vz[it];
+      continue;
+    }
+    const int cx = (int)(t % g.bcx);
+    long long r = t / g.bcx;
+    const int y = (int)(r % g.by);
+    r /= g.by;
+    const int s = (int)(r & 1);
+    const int z = (int)(r >> 1);
+    const long long i = ext_index(g, s, cx, y, z);
+    if (L.code[i] < 0) continue;
+    const double vx = L.vx[i] + sp.h * L.fx[i], vy = L.vy[i] + sp.h * L.fy[i], vz = L.vz[i] + sp.h * L.fz[i];
+    const double x0 = L.px[i] + sp.dt * vx, y0 = L.py[i] + sp.dt * vy, z0 = L.pz[i] + sp.dt * vz;
+    L.vx[i] = vx;
+    L.vy[i] = vy;
+    L.vz[i] = vz;
+    L.px[i] = x0;
+    L.py[i] = y0;
+    L.pz[i] = z0;
+    for_images(g, s, cx, y, z, [&](long long idx, double ox, double oy, double oz) {
+      L.px[idx] = x0 + ox;
+      L.py[idx] = y0 + oy;
+      L.pz[idx] = z0 + oz;
+    });
+  }
+}
+
+int launch_kick_drift64(const Geom &g, const Lattice64 &L, const Itl64 &I, const StepParams &sp, cudaStream_t s) {
+  const long long n = 2LL * g.bcx * g.by * g.bz + I.n;
+  int grid = (int)((n + 255) / 256);
+  if (grid > 8 * device_sm_count()) grid = 8 * device_sm_count();
+  k_kick_drift64<<<grid, 256, 0, s>>>(g, L, I, sp);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+// Sum of each energy region in a fixed order: out[0] = pe, out[1] = ke.
+__global__ void k_reduce_energy(const double *part, double *out) {
+  __shared__ double acc[2][256];
+  double pe = 0.0, ke = 0.0;
+  for (int k = threadIdx.x; k < MB_EPART_CAP; k += blockDim.x) {
+    pe += part[0 * MB_EPART_CAP + k] + part[1 * MB_EPART_CAP + k] + part[3 * MB_EPART_CAP + k] +
+          part[4 * MB_EPART_CAP + k];
+    ke += part[2 * MB_EPART_CAP + k] + part[5 * MB_EPART_CAP + k];
+  }
+  acc[0][threadIdx.x] = pe;
+  acc[1][threadIdx.x] = ke;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < 256; k++) {
+      a += acc[0][k];
+      b += acc[1][k];
+    }
+    out[0] = a;
+    out[1] = b;
+  }
+}
+
+int launch_reduce(const double *partials, int n, double *out, cudaStream_t s) {
+  (void)n;
+  k_reduce_energy<<<1, 256, 0, s>>>(partials, out);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+} // namespace mb

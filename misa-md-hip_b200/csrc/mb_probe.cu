@@ -1,0 +1,58 @@
+// CUDA-core FMA throughput probes: the FP64 / FP32 denominators of the roofline
+// (the driver-measured peaks cover HBM and bf16 tensor work only).
+#include "mb_common.cuh"
+
+namespace mb {
+
+template <class T>
+__global__ void __launch_bounds__(256) k_fma_chain(T *out, int iters, T a, T b) {
+  T x0 = threadIdx.x * (T)1e-3, x1 = x0 + (T)1, x2 = x0 + (T)2, x3 = x0 + (T)3, x4 = x0 + (T)4, x5 = x0 + (T)5,
+    x6 = x0 + (T)6, x7 = x0 + (T)7;
+  for (int k = 0; k < iters; k++) {
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      x0 = x0 * a + b;
+      x1 = x1 * a + b;
+      x2 = x2 * a + b;
+      x3 = x3 * a + b;
+      x4 = x4 * a + b;
+      x5 = x5 * a + b;
+      x6 = x6 * a + b;
+      x7 = x7 * a + b;
+    }
+  }
+  const T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == (T)-12345.678) out[0] = s; // never true; keeps the chains alive
+}
+
+template <class T>
+static int time_fma(double *tflops) {
+  T *out = nullptr;
+  MB_CUDA(cudaMalloc(&out, sizeof(T)));
+  cudaEvent_t e0, e1;
+  MB_CUDA(cudaEventCreate(&e0));
+  MB_CUDA(cudaEventCreate(&e1));
+  const int blocks = device_sm_count() * 8, threads = 256, iters = 4096;
+  k_fma_chain<T><<<blocks, threads>>>(out, 64, (T)0.999, (T)1e-4); // warm-up
+  MB_CUDA(cudaEventRecord(e0));
+  k_fma_chain<T><<<blocks, threads>>>(out, iters, (T)0.999, (T)1e-4);
+  MB_CUDA(cudaEventRecord(e1));
+  MB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  MB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  return MB_OK;
+}
+
+} // namespace mb
+
+extern "C" int mb_measure_fma_peaks(double *fp64_tflops, double *fp32_tflops) {
+  if (!fp64_tflops || !fp32_tflops) return mb::fail(MB_ERR_ARG, "null output");
+  MB_TRY(mb::time_fma<double>(fp64_tflops));
+  MB_TRY(mb::time_fma<float>(fp32_tflops));
+  return MB_OK;
+}
