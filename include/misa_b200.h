@@ -112,6 +112,18 @@ int mb_eam_df_calc(mb_atom_element *atoms, double cutoff_radius);
  * the stencil, overwriting f of every box site with type >= 0 (needs df of the
  * ghost sites filled by the host). */
 int mb_eam_force_calc(mb_atom_element *atoms, double cutoff_radius);
+/* The rho pass of mb_eam_rho_calc (same inputs, same results) for hosts that cannot
+ * let a plugin allocate device memory: a process whose device memory is already
+ * handed out by its own pool allocator, or a timestep loop that must not take the
+ * implicit synchronisation cudaMalloc / cudaFree can cause.  No counterpart in the
+ * reference.  It calls no cudaMalloc / cudaFree: its scratch is a fixed 16 MiB
+ * device array inside the library, present on every GPU that loads the library
+ * until exit, which limits the ghost-extended lattice to about 115,000 sites
+ * (145 bytes each); larger lattices are refused with MB_ERR_ARG.  The first call on
+ * a device looks the array's device address up (cudaGetSymbolAddress) and should
+ * come before any stream capture.  All calls share the array and it keeps the
+ * previous call's contents; calls that overlap on the GPU race. */
+int mb_eam_rho_calc_noalloc(mb_atom_element *atoms, double cutoff_radius);
 /* The calDf kernel of the half-neighbour build (src/kernels/hip_kernels.hip.cpp:21-40):
  * df = F'(rho) for every box site with type >= 0. */
 int mb_eam_df_from_rho(mb_atom_element *atoms);

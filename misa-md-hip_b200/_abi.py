@@ -82,6 +82,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_nei_offset_init": (_I, [_PI64, C.c_size_t, _PI64, C.c_size_t]),
     "mb_pot_init": (_I, [C.POINTER(MbEamTables)]),
     "mb_eam_rho_calc": (_I, [_P, _D]),
+    "mb_eam_rho_calc_noalloc": (_I, [_P, _D]),
     "mb_eam_df_calc": (_I, [_P, _D]),
     "mb_eam_force_calc": (_I, [_P, _D]),
     "mb_eam_df_from_rho": (_I, [_P]),

@@ -303,3 +303,110 @@ int mb_hook_last_timing(float *kernel_ms, float *copy_ms) {
 }
 
 } // extern "C"
+
+// ------------------------------------------------------------------------
+// Rho pass without any device allocation.
+//
+// Some hosts cannot let a plugin call cudaMalloc: a process whose device memory is
+// already handed out by its own pool allocator (a plugin allocation would fail or
+// fragment that pool), or a timestep loop that must not take the implicit device
+// synchronisation cudaMalloc / cudaFree can cause.  For them the rho pass can run
+// in a fixed scratch area that is part of the library image: a file-scope device
+// array of MB_NOALLOC_SCRATCH_BYTES (16 MiB), held by every GPU that loads the
+// library until the process exits.  It holds the device copy of the host's AoS
+// lattice and the split-layout arrays the kernels work on (145 bytes per
+// ghost-extended site), so lattices of up to about 115,000 ext sites fit (for
+// example 30^3 unit cells with a (4, 2, 2) ghost); larger ones are refused.
+//
+// The array's name is only a host-side stand-in for the device symbol: host code
+// must never pass it to a kernel.  The device address is fetched once per device
+// with cudaGetSymbolAddress, on the first call made with that device current; that
+// first call should therefore come before any stream capture.  Every call shares
+// the one array and leaves its contents behind, so calls that overlap on the GPU
+// (two host threads, two streams) race; this entry point serialises calls made
+// through it, but nothing guards the array against a concurrent kernel elsewhere.
+#define MB_NOALLOC_SCRATCH_BYTES (16u << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MB_NOALLOC_SCRATCH_BYTES];
+
+namespace mb {
+
+static unsigned char *g_noalloc_dev[64] = {}; // device address of g_noalloc_scratch, per device ordinal
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Bytes of scratch one ext site needs (AoS copy + positions + code + df + rho),
+// each array rounded up to 256 B, plus the error flag.
+static size_t noalloc_bytes(size_t n) {
+  return align256(n * sizeof(mb_atom_element)) + 5 * align256(n * sizeof(double)) + align256(n) + 256;
+}
+
+static size_t noalloc_max_sites() {
+  size_t lo = 0, hi = MB_NOALLOC_SCRATCH_BYTES;
+  while (lo < hi) {
+    const size_t mid = (lo + hi + 1) / 2;
+    if (noalloc_bytes(mid) <= MB_NOALLOC_SCRATCH_BYTES)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+} // namespace mb
+
+extern "C" int mb_eam_rho_calc_noalloc(mb_atom_element *atoms, double cutoff_radius) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  HookCtx &c = g_ctx;
+  if (!atoms) return fail(MB_ERR_ARG, "null atoms array");
+  if (!(cutoff_radius > 0)) return fail(MB_ERR_ARG, "cutoff must be > 0");
+  MB_TRY(require_ready(c));
+  const mb_device_domain &d = c.dom;
+  const size_t n = (size_t)d.ext_size_x * d.ext_size_y * d.ext_size_z;
+  if (noalloc_bytes(n) > MB_NOALLOC_SCRATCH_BYTES)
+    return fail(MB_ERR_ARG, "mb_eam_rho_calc_noalloc: the ghost-extended lattice has " + std::to_string(n) +
+                                " sites; the fixed scratch of " + std::to_string(MB_NOALLOC_SCRATCH_BYTES) +
+                                " bytes holds at most " + std::to_string(noalloc_max_sites()) +
+                                " (use mb_eam_rho_calc for larger lattices)");
+  int dev = 0;
+  MB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(MB_ERR_ARG, "device ordinal beyond 63");
+  if (!g_noalloc_dev[dev]) {
+    void *p = nullptr;
+    MB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_dev[dev] = (unsigned char *)p;
+  }
+  unsigned char *base = g_noalloc_dev[dev];
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    unsigned char *p = base + off;
+    off += align256(bytes);
+    return p;
+  };
+  mb_atom_element *aos = (mb_atom_element *)carve(n * sizeof(mb_atom_element));
+  Lattice64 L{};
+  L.px = (double *)carve(n * sizeof(double));
+  L.py = (double *)carve(n * sizeof(double));
+  L.pz = (double *)carve(n * sizeof(double));
+  L.df = (double *)carve(n * sizeof(double));
+  L.rho = (double *)carve(n * sizeof(double));
+  L.code = (int8_t *)carve(n);
+  int *bad = (int *)carve(sizeof(int));
+
+  const size_t first = ((size_t)d.ghost_size_z * d.ext_size_y + d.ghost_size_y) * d.ext_size_x + d.ghost_size_x;
+  const size_t last = ((size_t)(d.ghost_size_z + d.box_size_z - 1) * d.ext_size_y + d.ghost_size_y + d.box_size_y - 1) *
+                          d.ext_size_x +
+                      d.ghost_size_x + d.box_size_x - 1;
+  cudaStream_t s = c.stream;
+  MB_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s)); // the flag must start at zero on every call
+  MB_CUDA(cudaMemcpyAsync(aos, atoms, n * sizeof(mb_atom_element), cudaMemcpyHostToDevice, s));
+  MB_TRY(launch_unpack_ext(c.g, aos, d.ext_size_x, d.ext_size_y, d.ext_size_z, L, 0, bad, s));
+  MB_TRY(launch_rho64(c.g, c.st, pot_dev(c.potp), L, cutoff_radius * cutoff_radius, nullptr, 0, 0, s));
+  MB_TRY(launch_pack_ext(c.g, aos, d.ext_size_x, d.ext_size_y, L, 1, s));
+  MB_CUDA(cudaMemcpyAsync(atoms + first, aos + first, (last - first + 1) * sizeof(mb_atom_element),
+                          cudaMemcpyDeviceToHost, s));
+  int flag = 0;
+  MB_CUDA(cudaMemcpyAsync(&flag, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  if (flag) return fail(MB_ERR_ARG, "atom type >= 64 is not supported (treated as vacant)");
+  return MB_OK;
+}
