@@ -199,6 +199,59 @@ int mb_sim_info(mb_sim *sim, int64_t *n_sites, int64_t *n_stencil, int64_t *devi
 /* CUDA graph capture of the steady-state step (on by default). */
 int mb_sim_set_graphs(mb_sim *sim, int enable);
 
+/* ------------------------------------------- 3. ensembles and serving */
+
+/* Many independent periodic lattices (slots) advanced together, one persistent
+ * kernel launch per timestep, in mixed precision (FP32 pair and spline work with
+ * compensated FP32 sums; FP64 positions, velocities, integration and energies).
+ * Slots can be added and removed between launches while others are mid-run; each
+ * has its own step target, after which it stops advancing. */
+typedef struct mb_ensemble mb_ensemble;
+
+typedef struct mb_ensemble_config {
+  double lattice_const, mass, dt, cutoff, stencil_skin;
+  int64_t hbm_budget_bytes; /* 0: unlimited; otherwise mb_ensemble_add refuses beyond it */
+  int32_t max_lattices;     /* 0: unlimited */
+  int32_t pad_;
+} mb_ensemble_config;
+
+typedef struct mb_lattice_spec {
+  int32_t cells_x, cells_y, cells_z;
+  int32_t max_interstitials;
+} mb_lattice_spec;
+
+int mb_ensemble_create(const mb_ensemble_config *cfg, const mb_eam_tables *pot, mb_ensemble **out);
+int mb_ensemble_destroy(mb_ensemble *e);
+/* Device bytes one lattice of this spec occupies (what admission budgets with). */
+int mb_ensemble_lattice_bytes(const mb_lattice_spec *spec, int64_t *bytes);
+/* Upload a lattice (box-order records + interstitials) into a free slot; it will
+ * advance `steps` steps.  MB_ERR_NOMEM when the HBM budget or slot count is full. */
+int mb_ensemble_add(mb_ensemble *e, const mb_lattice_spec *spec, const mb_atom_element *box,
+                    const mb_atom_element *itl, int32_t n_itl, int64_t steps, int32_t *slot);
+int mb_ensemble_remove(mb_ensemble *e, int32_t slot);
+int mb_ensemble_set_steps(mb_ensemble *e, int32_t slot, int64_t steps_target);
+/* Up to max_launches launches, stopping early once every slot reached its target;
+ * energies are recorded at every multiple of energy_every of each slot's step. */
+int mb_ensemble_advance(mb_ensemble *e, int32_t max_launches, int32_t energy_every, int32_t *launches);
+/* Every slot advances nsteps more steps. */
+int mb_ensemble_run(mb_ensemble *e, int32_t nsteps, int32_t energy_every);
+int mb_ensemble_sync(mb_ensemble *e);
+int mb_ensemble_download(mb_ensemble *e, int32_t slot, mb_atom_element *box, mb_atom_element *itl, int32_t *n_itl);
+int mb_ensemble_status(mb_ensemble *e, int32_t slot, int64_t *steps_done, int64_t *steps_target,
+                       int64_t *device_bytes);
+/* Recorded (step, pe, ke) triples of a slot, eV. */
+int mb_ensemble_energies(mb_ensemble *e, int32_t slot, double *out, int32_t cap, int32_t *n);
+int mb_ensemble_clear_energies(mb_ensemble *e, int32_t slot);
+/* Device time of nsteps launches of every slot (CUDA events; advances the state). */
+int mb_ensemble_time(mb_ensemble *e, int32_t nsteps, float *ms);
+/* Tile-shape policy: -1 picks a shape per lattice from its size, 0..3 one shape for all. */
+int mb_ensemble_set_policy(mb_ensemble *e, int32_t policy);
+/* Times every policy for `steps` launches on a snapshot of the slots (state restored
+ * afterwards) and keeps the fastest. */
+int mb_ensemble_autotune(mb_ensemble *e, int32_t steps, int32_t *policy, float *best_ms);
+int mb_ensemble_info(mb_ensemble *e, int64_t *n_sites, int64_t *n_tiles, int64_t *device_bytes, int32_t *n_slots);
+int mb_ensemble_set_graphs(mb_ensemble *e, int enable);
+
 #ifdef __cplusplus
 }
 #endif

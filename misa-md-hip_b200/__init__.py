@@ -19,7 +19,7 @@ import numpy as np
 from . import _abi, lattice, potential
 from ._abi import ATOM_DTYPE, MB_PREC_FP64, MB_PREC_MIXED, MbError, check, lib, ptr
 
-__all__ = ["ATOM_DTYPE", "MB_PREC_FP64", "MB_PREC_MIXED", "MbError", "Hooks", "Sim", "lattice", "potential",
+__all__ = ["ATOM_DTYPE", "MB_PREC_FP64", "MB_PREC_MIXED", "MbError", "Hooks", "Sim", "Ensemble", "lattice", "potential",
            "lib", "build"]
 
 
@@ -154,3 +154,119 @@ class Sim:
 
     def set_graphs(self, enable: bool) -> None:
         check(lib().mb_sim_set_graphs(self._h, int(enable)))
+
+
+class Ensemble:
+    """Many independent periodic lattices advanced together in mixed precision:
+    one persistent kernel launch per timestep (C ABI: mb_ensemble_*)."""
+
+    def __init__(self, tables: potential.EamTables, lattice_const: float = 2.855, mass: float = 55.845,
+                 dt: float = 1.0, cutoff: float | None = None, stencil_skin: float = 0.7,
+                 hbm_budget_bytes: int = 0, max_lattices: int = 0):
+        self.lattice_const = lattice_const
+        cfg = _abi.MbEnsembleConfig(lattice_const, mass, dt, tables.cutoff if cutoff is None else cutoff,
+                                    stencil_skin, int(hbm_budget_bytes), int(max_lattices), 0)
+        t = tables.as_c()
+        h = C.c_void_p()
+        check(lib().mb_ensemble_create(C.byref(cfg), C.byref(t), C.byref(h)))
+        self._h = h
+        self._cells: dict[int, tuple] = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().mb_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @staticmethod
+    def lattice_bytes(cells, max_interstitials: int = 0) -> int:
+        spec = _abi.MbLatticeSpec(*[int(c) for c in cells], int(max_interstitials))
+        b = C.c_int64()
+        check(lib().mb_ensemble_lattice_bytes(C.byref(spec), C.byref(b)))
+        return b.value
+
+    def add(self, cells, box: np.ndarray, itl: np.ndarray | None = None, steps: int = 0,
+            max_interstitials: int | None = None) -> int:
+        cells = tuple(int(c) for c in cells)
+        n = 0 if itl is None else int(itl.shape[0])
+        cap = n if max_interstitials is None else max_interstitials
+        spec = _abi.MbLatticeSpec(cells[0], cells[1], cells[2], cap)
+        slot = C.c_int32()
+        box = np.ascontiguousarray(box)
+        itl_c = np.ascontiguousarray(itl) if n else None
+        check(lib().mb_ensemble_add(self._h, C.byref(spec), ptr(box), ptr(itl_c) if n else None, n, int(steps),
+                                    C.byref(slot)))
+        self._cells[slot.value] = (cells, cap)
+        return slot.value
+
+    def remove(self, slot: int) -> None:
+        check(lib().mb_ensemble_remove(self._h, slot))
+        self._cells.pop(slot, None)
+
+    def set_steps(self, slot: int, steps_target: int) -> None:
+        check(lib().mb_ensemble_set_steps(self._h, slot, int(steps_target)))
+
+    def advance(self, max_launches: int, energy_every: int = 0) -> int:
+        n = C.c_int32()
+        check(lib().mb_ensemble_advance(self._h, max_launches, energy_every, C.byref(n)))
+        return n.value
+
+    def run(self, nsteps: int, energy_every: int = 0) -> None:
+        check(lib().mb_ensemble_run(self._h, nsteps, energy_every))
+        check(lib().mb_ensemble_sync(self._h))
+
+    def sync(self) -> None:
+        check(lib().mb_ensemble_sync(self._h))
+
+    def download(self, slot: int) -> tuple[np.ndarray, np.ndarray]:
+        cells, cap = self._cells[slot]
+        box = np.zeros(2 * cells[0] * cells[1] * cells[2], dtype=ATOM_DTYPE)
+        itl = np.zeros(max(1, cap), dtype=ATOM_DTYPE)
+        n = C.c_int32()
+        check(lib().mb_ensemble_download(self._h, slot, ptr(box), ptr(itl), C.byref(n)))
+        return box, itl[:n.value].copy()
+
+    def status(self, slot: int) -> tuple[int, int, int]:
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().mb_ensemble_status(self._h, slot, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def energies(self, slot: int) -> np.ndarray:
+        n = C.c_int32()
+        check(lib().mb_ensemble_energies(self._h, slot, None, 0, C.byref(n)))
+        out = np.zeros((max(1, n.value), 3))
+        check(lib().mb_ensemble_energies(self._h, slot, out.ctypes.data_as(C.POINTER(C.c_double)), n.value,
+                                         C.byref(n)))
+        return out[:n.value]
+
+    def time(self, nsteps: int) -> float:
+        ms = C.c_float()
+        check(lib().mb_ensemble_time(self._h, nsteps, C.byref(ms)))
+        return ms.value
+
+    def set_policy(self, policy: int) -> None:
+        check(lib().mb_ensemble_set_policy(self._h, policy))
+
+    def autotune(self, steps: int = 5) -> tuple[int, float]:
+        p, ms = C.c_int32(), C.c_float()
+        check(lib().mb_ensemble_autotune(self._h, steps, C.byref(p), C.byref(ms)))
+        return p.value, ms.value
+
+    def info(self) -> dict:
+        a, b, c, d = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32()
+        check(lib().mb_ensemble_info(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
+        return {"n_sites": a.value, "n_tiles": b.value, "device_bytes": c.value, "n_slots": d.value}
+
+    def set_graphs(self, enable: bool) -> None:
+        check(lib().mb_ensemble_set_graphs(self._h, int(enable)))

@@ -106,7 +106,36 @@ SIGNATURES: dict[str, tuple] = {
     "mb_sim_kernel_times": (_I, [_P, _PF, _PF]),
     "mb_sim_info": (_I, [_P, _PI64, _PI64, _PI64]),
     "mb_sim_set_graphs": (_I, [_P, _I]),
+    "mb_ensemble_create": (_I, [C.c_void_p, C.POINTER(MbEamTables), C.POINTER(_P)]),
+    "mb_ensemble_destroy": (_I, [_P]),
+    "mb_ensemble_lattice_bytes": (_I, [C.c_void_p, _PI64]),
+    "mb_ensemble_add": (_I, [_P, C.c_void_p, _P, _P, C.c_int32, C.c_int64, C.POINTER(C.c_int32)]),
+    "mb_ensemble_remove": (_I, [_P, C.c_int32]),
+    "mb_ensemble_set_steps": (_I, [_P, C.c_int32, C.c_int64]),
+    "mb_ensemble_advance": (_I, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "mb_ensemble_run": (_I, [_P, C.c_int32, C.c_int32]),
+    "mb_ensemble_sync": (_I, [_P]),
+    "mb_ensemble_download": (_I, [_P, C.c_int32, _P, _P, C.POINTER(C.c_int32)]),
+    "mb_ensemble_status": (_I, [_P, C.c_int32, _PI64, _PI64, _PI64]),
+    "mb_ensemble_energies": (_I, [_P, C.c_int32, _PD, C.c_int32, C.POINTER(C.c_int32)]),
+    "mb_ensemble_clear_energies": (_I, [_P, C.c_int32]),
+    "mb_ensemble_time": (_I, [_P, C.c_int32, _PF]),
+    "mb_ensemble_set_policy": (_I, [_P, C.c_int32]),
+    "mb_ensemble_autotune": (_I, [_P, C.c_int32, C.POINTER(C.c_int32), _PF]),
+    "mb_ensemble_info": (_I, [_P, _PI64, _PI64, _PI64, C.POINTER(C.c_int32)]),
+    "mb_ensemble_set_graphs": (_I, [_P, _I]),
 }
+
+
+class MbEnsembleConfig(C.Structure):
+    _fields_ = [("lattice_const", C.c_double), ("mass", C.c_double), ("dt", C.c_double), ("cutoff", C.c_double),
+                ("stencil_skin", C.c_double), ("hbm_budget_bytes", C.c_int64), ("max_lattices", C.c_int32),
+                ("pad_", C.c_int32)]
+
+
+class MbLatticeSpec(C.Structure):
+    _fields_ = [("cells_x", C.c_int32), ("cells_y", C.c_int32), ("cells_z", C.c_int32),
+                ("max_interstitials", C.c_int32)]
 
 _lib = None
 

@@ -62,8 +62,9 @@ struct DevPot {
   const double4 *phi_der; // [np][nr]
   const double2 *force1;  // single type: [nr][3] {f d0, phi d0}, {f d1, phi d1}, {f d2, phi d2}
   // single precision copies for the mixed path
-  const float4 *f_val32;  // [nt][nr]
-  const float4 *force132; // single type: [nr][2] {f d0, f d1, f d2, phi d0}, {phi d1, phi d2, 0, 0}
+  const float4 *f_val32;   // [nt][nr]  {y, s, c2, c3}
+  const float2 *force32;   // single type: [nr][3] {f d0, phi d0}, {f d1, phi d1}, {f d2, phi d2}
+  const float4 *phi_val32; // single type: [nr]
 };
 
 struct PotHost;
@@ -157,14 +158,6 @@ int launch_unpack_box_ids(const Geom &g, const mb_atom_element *aos, Lattice64 L
 int launch_pack_box_ids(const Geom &g, mb_atom_element *aos, const Lattice64 &L, const double *px, const double *py,
                         const double *pz, double h, int unkick, const int64_t *ids, cudaStream_t s);
 int launch_df_from_rho(const Geom &g, const DevPot &pot, const Lattice64 &L, cudaStream_t s);
-
-// mixed-precision path (mb_mixed.cu)
-int launch_mixed_step(mb_sim *sim, int energy, int prime);
-int mixed_alloc(mb_sim *sim);
-void mixed_free(mb_sim *sim);
-int mixed_after_upload(mb_sim *sim);
-int mixed_pack_df_rho(mb_sim *sim);
-int mixed_kernel_times(mb_sim *sim, int nsteps, float *rho_ms, float *force_ms);
 
 // ------------------------------------------------------------ utilities
 int device_sm_count();

@@ -1,0 +1,215 @@
+// Mixed-precision, multi-lattice EAM timestep: device side.
+//
+// One persistent kernel advances every active lattice of an ensemble by one
+// velocity-Verlet step.  Phases, separated by a grid barrier with a bounded spin:
+//   A  interstitial bookkeeping: flag lattice sites within reach of an interstitial
+//   B  rho / df over lattice tiles (FP32 pair + spline work, two-sum accumulation)
+//   C  rho / df of flagged sites and interstitials (FP64, one warp per item)
+//   D  force + velocity-Verlet over lattice tiles (FP32 pairs, FP64 integration)
+//   E  force + velocity-Verlet of flagged sites and interstitials (FP64)
+//   F  per-lattice step bookkeeping (buffer parity, step counters)
+//
+// Lattice state per site: FP64 displacement from the ideal BCC site (u64) and FP64
+// velocity are the master copy; a float4 {u (FP32), df} array, ghost-extended by 2
+// cells, is what the pair passes read.  A tile of 2 x (TX x TY x TZ) sites plus its
+// 2-cell halo is staged into shared memory with one 5-D TMA load (float4 component,
+// x, y, z, sublattice), double-buffered so the next tile streams in while the
+// current one is computed.  Vacant sites carry a huge displacement so every r^2 test
+// rejects them.
+//
+// Precision of the pair distance: FP32 cannot hold r to better than ~1e-7 A near
+// 5 A, which alone gives force errors of ~2e-6 relative.  The spline index is
+// therefore taken from eps = r - R_k, with R_k the ideal length of stencil entry k:
+// eps = (2 C_k . d + d . d) / (r + R_k), d = u_i - u_j, is small and carries
+// ~1e-8 A absolute precision; R_k / dr is split on the host into an integer knot and
+// an FP32 fraction.
+#pragma once
+
+#include <cuda.h>
+
+#include "mb_common.cuh"
+#include "mb_device.cuh"
+
+namespace mb {
+
+#define ENS_THREADS 512
+#define ENS_NSHAPE 4
+#define ENS_MAX_ST 112
+#define ENS_BAR_SPINS (1u << 25)
+#define ENS_WAIT_SPINS (1u << 26)
+#define ENS_VACANT 1.0e15f
+#define ENS_TILE_MAX_BYTES 40960 // largest halo'd tile: 2 x 20 x 8 x 8 float4
+
+struct LatDesc {
+  int bcx, by, bz;       // box (cells along x per sublattice)
+  int ecx, ey, ez;       // ghost-extended (box + 4)
+  long long E;           // sites per sublattice array
+  int ntx, nty, ntz;     // tiles along x, y, z
+  int shape;             // tile shape id
+  int n_itl, cap_flag;
+  int cur;               // u4 buffer holding the current positions (flipped on the device)
+  int primed;            // 1 once forces at the start positions exist
+  long long steps_done, steps_target;
+  double Lx, Ly, Lz;
+  float4 *u4[2];         // {ux, uy, uz, df}, ghost-extended
+  double *ux, *uy, *uz;  // FP64 displacement (master), ext-indexed
+  double *vx, *vy, *vz;
+  float *fx, *fy, *fz, *rho;
+  int8_t *code;
+  int *flag_list, *flag_count;
+  double *ipx[2], *ipy[2], *ipz[2];
+  double *ivx, *ivy, *ivz, *ifx, *ify, *ifz, *irho, *idf;
+  int8_t *itype;
+  double *e_itl; // [2] interstitial-item energy (pe, ke), accumulated atomically
+};
+
+struct EnsParams {
+  int n_st;
+  int soff[ENS_NSHAPE][2][ENS_MAX_ST]; // shared-memory offset (float4 units) of entry k, per shape / sublattice
+  float4 ck[2][ENS_MAX_ST];            // ideal offset X_i - X_j (xyz) and its length (w)
+  int mk[2][ENS_MAX_ST];               // floor(|C_k| / dr)
+  float fk[2][ENS_MAX_ST];             // |C_k| / dr - mk
+  char4 sd[2][ENS_MAX_ST];             // target sublattice - own, dcx, dy, dz
+  int shape_dims[ENS_NSHAPE][4];       // TX, TY, TZ, bytes
+  DevPot P;
+  float rdr, rc2f;
+  int m_lo, nsm;
+  double h, dt, mass, a0, rc2, reach;
+  const LatDesc *lats;
+  int n_lats;
+  const int *tile_lat, *tile_idx;
+  int n_tiles;
+  const CUtensorMap *tmaps; // [lattice][buffer]
+  unsigned *bar;
+  int *err;
+  double *epart; // [tile][2]
+  const int *itl_lats;
+  int n_itl_lats;
+  int energy;
+};
+
+// ------------------------------------------------------------ primitives
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier (all CTAs co-resident: cooperative launch).  Gives up after a
+// bounded number of polls, raising err; returns false once err is set.
+__device__ __forceinline__ bool grid_sync(unsigned *bar, int *err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned gen = ld_acquire_u32(bar + 1);
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u) + 1u;
+    if (arrived == gridDim.x) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned spins = 0;
+      while (ld_acquire_u32(bar + 1) == gen) {
+        if (++spins > ENS_BAR_SPINS) {
+          atomicExch(err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (ok && *(volatile int *)err) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok)
+               : "r"(smem_addr(bar)), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+
+// 5-D tiled TMA load (no multicast): box {4, TX+4, TY+4, TZ+4, 2} of float32.
+__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+      "%6}], [%7];" ::"r"(smem_addr(dst)),
+      "l"((unsigned long long)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Knuth two-sum: s + c carries the running sum with the rounding error of every add.
+__device__ __forceinline__ void two_sum(float &s, float &c, float x) {
+  const float t = s + x;
+  const float bp = t - s;
+  c += (s - (t - bp)) + (x - bp);
+  s = t;
+}
+
+__device__ __forceinline__ Geom lat_geom(const LatDesc &d) {
+  Geom g;
+  g.ecx = d.ecx;
+  g.ey = d.ey;
+  g.ez = d.ez;
+  g.gcx = 2;
+  g.gy = 2;
+  g.gz = 2;
+  g.bcx = d.bcx;
+  g.by = d.by;
+  g.bz = d.bz;
+  g.images = 1;
+  g.E = d.E;
+  g.Lx = d.Lx;
+  g.Ly = d.Ly;
+  g.Lz = d.Lz;
+  return g;
+}
+
+__device__ __forceinline__ bool lat_active(const LatDesc &d) { return !d.primed || d.steps_done < d.steps_target; }
+
+// Absolute position of ext site j: ideal site + FP32 displacement (ghost sites are
+// periodic images: the ideal position continues past the box, the displacement is the
+// source site's).
+__device__ __forceinline__ void lat_pos(const LatDesc &d, const float4 *u4, long long j, double a0, double &x,
+                                        double &y, double &z) {
+  const int s = (int)(j / d.E);
+  const long long r = j - (long long)s * d.E;
+  const long long row = r / d.ecx;
+  const int cx = (int)(r - row * d.ecx);
+  const int zz = (int)(row / d.ey);
+  const int yy = (int)(row - (long long)zz * d.ey);
+  const float4 u = u4[j];
+  const double h = 0.5 * s;
+  x = 0.5 * a0 * (double)(2 * (cx - 2) + s) + (double)u.x;
+  y = a0 * ((double)(yy - 2) + h) + (double)u.y;
+  z = a0 * ((double)(zz - 2) + h) + (double)u.z;
+}
+
+__device__ __forceinline__ void ideal_pos(int s, int cx, int y, int z, double a0, double &X, double &Y, double &Z) {
+  const double h = 0.5 * s;
+  X = 0.5 * a0 * (double)(2 * cx + s);
+  Y = a0 * ((double)y + h);
+  Z = a0 * ((double)z + h);
+}
+
+} // namespace mb

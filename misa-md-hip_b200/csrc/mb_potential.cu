@@ -58,7 +58,8 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
   std::vector<double4> f_val((size_t)nt * nr), f_der((size_t)nt * nr), F_val((size_t)nt * nrho),
       F_der((size_t)nt * nrho), phi_val((size_t)np * nr), phi_der((size_t)np * nr);
   std::vector<double2> force1((size_t)nr * 3);
-  std::vector<float4> f_val32((size_t)nt * nr), force132((size_t)nr * 2);
+  std::vector<float4> f_val32((size_t)nt * nr), phi_val32((size_t)nr);
+  std::vector<float2> force32((size_t)nr * 3);
   std::vector<double> c7;
   auto split = [&](const std::vector<double> &c, std::vector<double4> &val, std::vector<double4> &der, size_t base,
                    int n) {
@@ -83,8 +84,11 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
     force1[(size_t)m * 3 + 0] = make_double2(fd.x, pd.x);
     force1[(size_t)m * 3 + 1] = make_double2(fd.y, pd.y);
     force1[(size_t)m * 3 + 2] = make_double2(fd.z, pd.z);
-    force132[(size_t)m * 2 + 0] = make_float4((float)fd.x, (float)fd.y, (float)fd.z, (float)pd.x);
-    force132[(size_t)m * 2 + 1] = make_float4((float)pd.y, (float)pd.z, 0.f, 0.f);
+    force32[(size_t)m * 3 + 0] = make_float2((float)fd.x, (float)pd.x);
+    force32[(size_t)m * 3 + 1] = make_float2((float)fd.y, (float)pd.y);
+    force32[(size_t)m * 3 + 2] = make_float2((float)fd.z, (float)pd.z);
+    const double4 pv = phi_val[m];
+    phi_val32[m] = make_float4((float)pv.x, (float)pv.y, (float)pv.z, (float)pv.w);
   }
   for (size_t i = 0; i < f_val.size(); i++) {
     const double4 v = f_val[i];
@@ -101,7 +105,7 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
                o_Fv = reserve(F_val.size() * sizeof(double4)), o_Fd = reserve(F_der.size() * sizeof(double4)),
                o_pv = reserve(phi_val.size() * sizeof(double4)), o_pd = reserve(phi_der.size() * sizeof(double4)),
                o_f1 = reserve(force1.size() * sizeof(double2)), o_fv32 = reserve(f_val32.size() * sizeof(float4)),
-               o_f132 = reserve(force132.size() * sizeof(float4));
+               o_f32 = reserve(force32.size() * sizeof(float2)), o_pv32 = reserve(phi_val32.size() * sizeof(float4));
   PotHost *p = new PotHost();
   cudaError_t e = cudaMalloc(&p->blob, off);
   if (e != cudaSuccess) {
@@ -118,7 +122,8 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
   memcpy(&staging[o_pd], phi_der.data(), phi_der.size() * sizeof(double4));
   memcpy(&staging[o_f1], force1.data(), force1.size() * sizeof(double2));
   memcpy(&staging[o_fv32], f_val32.data(), f_val32.size() * sizeof(float4));
-  memcpy(&staging[o_f132], force132.data(), force132.size() * sizeof(float4));
+  memcpy(&staging[o_f32], force32.data(), force32.size() * sizeof(float2));
+  memcpy(&staging[o_pv32], phi_val32.data(), phi_val32.size() * sizeof(float4));
   e = cudaMemcpy(p->blob, staging.data(), off, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     cudaFree(p->blob);
@@ -141,7 +146,8 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
   d.phi_der = (const double4 *)(b + o_pd);
   d.force1 = (const double2 *)(b + o_f1);
   d.f_val32 = (const float4 *)(b + o_fv32);
-  d.force132 = (const float4 *)(b + o_f132);
+  d.force32 = (const float2 *)(b + o_f32);
+  d.phi_val32 = (const float4 *)(b + o_pv32);
   *out = p;
   return MB_OK;
 }

@@ -54,8 +54,9 @@ struct mb_sim {
   cudaGraphExec_t graph = nullptr; // steady step pair starting at cur == 0
   size_t device_bytes = 0;
   float last_rho_ms = 0.f, last_force_ms = 0.f;
-  // mixed precision state (mb_mixed.cu)
-  void *mixed = nullptr;
+  // mixed precision: the lattice lives in a one-slot ensemble (mb_ens_host.cu)
+  mb_ensemble *ens = nullptr;
+  int slot = -1;
 };
 
 namespace mb {
@@ -170,11 +171,7 @@ static int record_energy(mb_sim *s) {
 }
 
 static int do_step(mb_sim *s, int energy, int prime) {
-  if (s->cfg.precision == MB_PREC_MIXED) {
-    MB_TRY(launch_mixed_step(s, energy, prime));
-  } else {
-    MB_TRY(step64(s, energy, prime ? 0 : 1, 1, 0));
-  }
+  MB_TRY(step64(s, energy, prime ? 0 : 1, 1, 0));
   if (energy) MB_TRY(record_energy(s));
   s->cur ^= 1;
   return MB_OK;
@@ -200,7 +197,7 @@ static int build_graph(mb_sim *s) {
   MB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
   int rc = MB_OK;
   for (int k = 0; k < 2 && rc == MB_OK; k++) {
-    rc = s->cfg.precision == MB_PREC_MIXED ? launch_mixed_step(s, 0, 0) : step64(s, 0, 1, 1, 0);
+    rc = step64(s, 0, 1, 1, 0);
     s->cur ^= 1;
   }
   cudaError_t e = cudaStreamEndCapture(s->stream, &gr);
@@ -238,6 +235,38 @@ static int run_steps(mb_sim *s, int nsteps, int energy_every) {
   return MB_OK;
 }
 
+// ----------------------------------------------- mixed precision delegation
+static int mixed_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **out) {
+  mb_ensemble_config ec{};
+  ec.lattice_const = cfg->lattice_const;
+  ec.mass = cfg->mass;
+  ec.dt = cfg->dt;
+  ec.cutoff = cfg->cutoff;
+  ec.stencil_skin = cfg->stencil_skin;
+  ec.max_lattices = 1;
+  mb_sim *s = new mb_sim();
+  s->cfg = *cfg;
+  s->n_box = 2LL * cfg->cells_x * cfg->cells_y * cfg->cells_z;
+  const int rc = mb_ensemble_create(&ec, pot, &s->ens);
+  if (rc != MB_OK) {
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return MB_OK;
+}
+
+static int mixed_upload(mb_sim *s, const mb_atom_element *box, const mb_atom_element *itl, int32_t n_itl) {
+  if (s->slot >= 0) MB_TRY(mb_ensemble_remove(s->ens, s->slot));
+  s->slot = -1;
+  mb_lattice_spec spec{s->cfg.cells_x, s->cfg.cells_y, s->cfg.cells_z, s->cfg.max_interstitials};
+  return mb_ensemble_add(s->ens, &spec, box, itl, n_itl, 0, &s->slot);
+}
+
+static int mixed_need_slot(mb_sim *s) {
+  return s->slot >= 0 ? MB_OK : fail(MB_ERR_STATE, "mb_sim_upload has not been called");
+}
+
 } // namespace mb
 
 using namespace mb;
@@ -254,6 +283,13 @@ int mb_sim_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **o
   if (cfg->precision != MB_PREC_FP64 && cfg->precision != MB_PREC_MIXED)
     return fail(MB_ERR_ARG, "unknown precision");
   if (cfg->max_interstitials < 0) return fail(MB_ERR_ARG, "max_interstitials < 0");
+  if (cfg->precision == MB_PREC_MIXED) {
+    const double reach0 = cfg->cutoff + cfg->stencil_skin;
+    if (cfg->cells_x * cfg->lattice_const <= 2 * reach0 || cfg->cells_y * cfg->lattice_const <= 2 * reach0 ||
+        cfg->cells_z * cfg->lattice_const <= 2 * reach0)
+      return fail(MB_ERR_ARG, "box edge must exceed 2 * (cutoff + stencil_skin)");
+    return mixed_create(cfg, pot, out);
+  }
   const double reach = cfg->cutoff + cfg->stencil_skin;
   // The box must hold more than two interaction spheres so periodic images are
   // unique (minimum image for interstitials, single-copy ghost images).
@@ -374,7 +410,6 @@ int mb_sim_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **o
   // vacant everywhere until an upload
   if (cudaMemsetAsync(s->code, 0xff, (ne + 3) & ~(size_t)3, s->stream) != cudaSuccess)
     return cleanup(fail(MB_ERR_CUDA, "memset failed"));
-  if (!fp64 && (rc = mixed_alloc(s)) != MB_OK) return cleanup(rc);
   if (cudaStreamSynchronize(s->stream) != cudaSuccess) return cleanup(fail(MB_ERR_CUDA, "sync failed"));
   *out = s;
   return MB_OK;
@@ -382,9 +417,14 @@ int mb_sim_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **o
 
 int mb_sim_destroy(mb_sim *s) {
   if (!s) return MB_OK;
+  if (s->ens) {
+    mb_ensemble_destroy(s->ens);
+    delete s;
+    return MB_OK;
+  }
   if (s->stream) cudaStreamSynchronize(s->stream);
   drop_graph(s);
-  mixed_free(s);
+  if (s->ens) mb_ensemble_destroy(s->ens);
   void *ptrs[] = {s->code, s->df, s->rho, s->id, s->epart, s->eout, s->stage, s->bad, s->irho, s->idf, s->itype,
                   s->iid, s->flag_list, s->flag_count};
   for (void *p : ptrs)
@@ -488,6 +528,7 @@ static int download_itl(mb_sim *s, mb_atom_element *itl, int which, int unkick) 
 }
 
 int mb_sim_upload(mb_sim *s, const mb_atom_element *box_atoms, const mb_atom_element *itl, int32_t n_itl) {
+  if (s && s->ens) return box_atoms ? mixed_upload(s, box_atoms, itl, n_itl) : fail(MB_ERR_ARG, "null argument");
   if (!s || !box_atoms) return fail(MB_ERR_ARG, "null argument");
   MB_CUDA(cudaStreamSynchronize(s->stream));
   drop_graph(s);
@@ -513,16 +554,18 @@ int mb_sim_upload(mb_sim *s, const mb_atom_element *box_atoms, const mb_atom_ele
   MB_CUDA(cudaStreamSynchronize(s->stream));
   if (bad) return fail(MB_ERR_ARG, "atom type >= 64 is not supported");
   MB_TRY(upload_itl(s, itl, n_itl, 1));
-  if (s->cfg.precision == MB_PREC_MIXED) MB_TRY(mixed_after_upload(s));
   return MB_OK;
 }
 
 int mb_sim_download(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t *n_itl) {
+  if (s && s->ens) {
+    MB_TRY(mixed_need_slot(s));
+    return mb_ensemble_download(s->ens, s->slot, box_atoms, itl, n_itl);
+  }
   if (!s || !box_atoms) return fail(MB_ERR_ARG, "null argument");
   MB_TRY(ensure_stage(s, (size_t)s->n_box));
   const int which = s->primed ? (s->cur ^ 1) : s->cur;
   const int unkick = s->primed ? 1 : 0;
-  if (s->cfg.precision == MB_PREC_MIXED) MB_TRY(mixed_pack_df_rho(s));
   Lattice64 L = sim_lattice(s, s->cur);
   MB_TRY(launch_pack_box_ids(s->g, s->stage, L, s->pos[which][0], s->pos[which][1], s->pos[which][2],
                              sim_params(s, 0, 0).h, unkick, s->id, s->stream));
@@ -535,6 +578,11 @@ int mb_sim_download(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl,
 }
 
 int mb_sim_run(mb_sim *s, int32_t nsteps, int32_t energy_every) {
+  if (s && s->ens) {
+    MB_TRY(mixed_need_slot(s));
+    MB_TRY(mb_ensemble_clear_energies(s->ens, s->slot));
+    return mb_ensemble_run(s->ens, nsteps, energy_every);
+  }
   if (!s || nsteps < 0) return fail(MB_ERR_ARG, "bad arguments");
   if (energy_every < 0) return fail(MB_ERR_ARG, "energy_every < 0");
   s->n_e = 0;
@@ -548,6 +596,7 @@ int mb_sim_run(mb_sim *s, int32_t nsteps, int32_t energy_every) {
 }
 
 int mb_sim_sync(mb_sim *s) {
+  if (s && s->ens) return mb_ensemble_sync(s->ens);
   if (!s) return fail(MB_ERR_ARG, "null sim");
   MB_CUDA(cudaStreamSynchronize(s->stream));
   int fc[2] = {0, 0};
@@ -559,6 +608,10 @@ int mb_sim_sync(mb_sim *s) {
 }
 
 int mb_sim_energies(mb_sim *s, double *out, int32_t cap, int32_t *n) {
+  if (s && s->ens) {
+    MB_TRY(mixed_need_slot(s));
+    return mb_ensemble_energies(s->ens, s->slot, out, cap, n);
+  }
   if (!s || !n) return fail(MB_ERR_ARG, "null argument");
   MB_CUDA(cudaStreamSynchronize(s->stream));
   const int m = std::min(cap, s->n_e);
@@ -575,6 +628,10 @@ int mb_sim_energies(mb_sim *s, double *out, int32_t cap, int32_t *n) {
 }
 
 int mb_sim_time_steps(mb_sim *s, int32_t nsteps, float *ms) {
+  if (s && s->ens) {
+    MB_TRY(mixed_need_slot(s));
+    return mb_ensemble_time(s->ens, nsteps, ms);
+  }
   if (!s || !ms || nsteps <= 0) return fail(MB_ERR_ARG, "bad arguments");
   if (!s->primed) MB_TRY(prime(s, 0));
   MB_CUDA(cudaStreamSynchronize(s->stream));
@@ -587,10 +644,17 @@ int mb_sim_time_steps(mb_sim *s, int32_t nsteps, float *ms) {
 }
 
 int mb_sim_kernel_times(mb_sim *s, float *rho_ms, float *force_ms) {
+  if (s && s->ens) { // both passes run inside the one persistent step kernel
+    MB_TRY(mixed_need_slot(s));
+    float ms = 0.f;
+    MB_TRY(mb_ensemble_time(s->ens, 4, &ms));
+    if (rho_ms) *rho_ms = 0.f;
+    if (force_ms) *force_ms = ms / 4;
+    return MB_OK;
+  }
   if (!s) return fail(MB_ERR_ARG, "null sim");
   if (!s->primed) MB_TRY(prime(s, 0));
   const int reps = 4;
-  if (s->cfg.precision == MB_PREC_MIXED) return mixed_kernel_times(s, reps, rho_ms, force_ms);
   float tr = 0, tf = 0;
   for (int k = 0; k < reps; k++) {
     MB_TRY(step64(s, 0, 1, 1, 1));
@@ -643,6 +707,12 @@ int mb_sim_step_host(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl
 }
 
 int mb_sim_info(mb_sim *s, int64_t *n_sites, int64_t *n_stencil, int64_t *device_bytes) {
+  if (s && s->ens) {
+    int32_t ns = 0;
+    MB_TRY(mb_ensemble_info(s->ens, n_sites, nullptr, device_bytes, &ns));
+    if (n_stencil) *n_stencil = -1;
+    return MB_OK;
+  }
   if (!s) return fail(MB_ERR_ARG, "null sim");
   if (n_sites) *n_sites = s->n_box;
   if (n_stencil) *n_stencil = s->st.n;
@@ -651,6 +721,7 @@ int mb_sim_info(mb_sim *s, int64_t *n_sites, int64_t *n_stencil, int64_t *device
 }
 
 int mb_sim_set_graphs(mb_sim *s, int enable) {
+  if (s && s->ens) return mb_ensemble_set_graphs(s->ens, enable);
   if (!s) return fail(MB_ERR_ARG, "null sim");
   s->use_graphs = enable != 0;
   if (!s->use_graphs) drop_graph(s);
