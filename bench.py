@@ -39,6 +39,7 @@ A0, MASS, RC, SKIN, DT = 2.855, 55.845, 5.6, 0.7, 1.0
 #   force pass reads x, type, df, v, f_old (84), writes x, v, f (72)         = 156 B
 #   flops: 58 pairs x (20 rho + 50 force) + 30 per atom                      = 4090
 BYTES_RHO, BYTES_FORCE = 36, 156
+BYTES_MIXED = 160  # mixed: rho pass 32 B + force/VV pass 128 B per atom-step
 FLOP_RHO, FLOP_FORCE = 58 * 20, 58 * 50 + 30
 
 WORKLOADS = {
@@ -46,6 +47,8 @@ WORKLOADS = {
                   vacancy=0.005, n_itl=200, seed=7, precision="fp64"),
     "mixed": dict(name="fe_bcc_200c_vac0.5pct_itl763_900K_mixed", cells=(200, 200, 200), temperature=900.0,
                   vacancy=0.005, n_itl=763, seed=7, precision="mixed"),
+    "scale_mixed": dict(name="fe_bcc_128c_vac0.5pct_itl200_300K_mixed", cells=(128, 128, 128), temperature=300.0,
+                        vacancy=0.005, n_itl=200, seed=7, precision="mixed"),
     "small": dict(name="fe_bcc_20c_600K_fp64", cells=(20, 20, 20), temperature=600.0, vacancy=0.0, n_itl=0,
                   seed=42, precision="fp64"),
 }
@@ -259,21 +262,28 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
     f64 = C.c_double()
     f32 = C.c_double()
     mb.check(mb.lib().mb_measure_fma_peaks(C.byref(f64), C.byref(f32)))
-    force_bytes = BYTES_FORCE * n_atoms
-    achieved = force_bytes / (force_ms * 1e-3) / 1e9
-    traffic = ncu_traffic("force")
+    if precision == mb.MB_PREC_FP64:
+        kname, kbytes, kflops, kms = "k_force64 (force + velocity-Verlet)", BYTES_FORCE * n_atoms, FLOP_FORCE, force_ms
+        fpeak, fname = f64.value, "fp64"
+    else:
+        # one persistent launch holds the rho, force and integration phases
+        kname, kbytes, kflops, kms = ("k_ens_step (rho + force + velocity-Verlet, one persistent launch)",
+                                      BYTES_MIXED * n_atoms, FLOP_RHO + FLOP_FORCE, force_ms)
+        fpeak, fname = f32.value, "fp32"
+    achieved = kbytes / (kms * 1e-3) / 1e9
+    traffic = ncu_traffic(kname.split()[0])
     roofline = {
-        "kernel": "k_force64 (force + velocity-Verlet)" if precision == mb.MB_PREC_FP64 else "force (mixed)",
-        "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+        "kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
-        "traffic": traffic, "algorithmic_bytes_per_launch": force_bytes, "launch_ms": force_ms,
-        "fp64": {"achieved_tflops": FLOP_FORCE * n_atoms / (force_ms * 1e-3) / 1e12,
-                 "peak_tflops": f64.value, "frac": FLOP_FORCE * n_atoms / (force_ms * 1e-3) / 1e12 / f64.value,
-                 "peak_source": "measured FMA-chain probe (mb_measure_fma_peaks)"},
-        "rho_kernel": {"launch_ms": rho_ms, "achieved_gbs": BYTES_RHO * n_atoms / (rho_ms * 1e-3) / 1e9,
-                       "achieved_tflops": FLOP_RHO * n_atoms / (rho_ms * 1e-3) / 1e12},
-        "fp32_peak_tflops": f32.value,
+        "traffic": traffic, "algorithmic_bytes_per_launch": kbytes, "launch_ms": kms,
+        fname: {"achieved_tflops": kflops * n_atoms / (kms * 1e-3) / 1e12, "peak_tflops": fpeak,
+                "frac": kflops * n_atoms / (kms * 1e-3) / 1e12 / fpeak,
+                "peak_source": "measured FMA-chain probe (mb_measure_fma_peaks)"},
+        "fp64_peak_tflops": f64.value, "fp32_peak_tflops": f32.value,
     }
+    if precision == mb.MB_PREC_FP64:
+        roofline["rho_kernel"] = {"launch_ms": rho_ms, "achieved_gbs": BYTES_RHO * n_atoms / (rho_ms * 1e-3) / 1e9,
+                                  "achieved_tflops": FLOP_RHO * n_atoms / (rho_ms * 1e-3) / 1e12}
 
     # end to end through the public host-buffer entry point: every step uploads the
     # lattice records from pinned host memory and reads the updated records back
@@ -307,8 +317,14 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
         na, dt, thr = cpu_oracle_rate(mb, wl, cells, 3, os.cpu_count())
         cpu = {"value": na * 3 / dt, "unit": "atom-steps/s", "cores": thr, "kind": "port",
                "sample": f"{cells[0]}x{cells[1]}x{cells[2]} cells of the same workload ({na} atoms), 3 steps"}
+    mixed = None
+    if precision == mb.MB_PREC_FP64 and not args.no_mixed:
+        mixed = mixed_comparison(args, mb, wl, box, itl, n_atoms, value / world, pg)
     sim.close()
-    launches_per_step = 5 if itl.shape[0] else 2
+    if precision == mb.MB_PREC_FP64:
+        launches_per_step = 5 if itl.shape[0] else 2
+    else:
+        launches_per_step = 1
     if rank == 0:
         line = {
             "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
@@ -321,7 +337,108 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
             "clocks": clk,
         }
+        if mixed is not None:
+            line["mixed"] = mixed
         print(json.dumps(line), flush=True)
+
+
+def mixed_comparison(args, mb, wl, box, itl, n_atoms, fp64_rate, pg) -> dict:
+    """Mixed precision on the same lattice: atom-steps/s, speed-up over the plain FP64
+    path and the relative force RMS error against the FP64 forces at the same state."""
+    t = mb.potential.fe_analytic()
+    forces = {}
+    for prec in (mb.MB_PREC_FP64, mb.MB_PREC_MIXED):
+        with mb.Sim(wl["cells"], t, lattice_const=A0, mass=MASS, dt=DT, cutoff=RC, stencil_skin=SKIN, precision=prec,
+                    max_interstitials=max(1, itl.shape[0])) as s:
+            s.upload(box, itl)
+            s.run(0)
+            b, i = s.download()
+            forces[prec] = np.concatenate([b["f"][b["type"] >= 0], i["f"]])
+    f64, f32 = forces[mb.MB_PREC_FP64], forces[mb.MB_PREC_MIXED]
+    err = float(np.sqrt(np.sum((f32 - f64) ** 2) / np.sum(f64 ** 2)))
+    with mb.Sim(wl["cells"], t, lattice_const=A0, mass=MASS, dt=DT, cutoff=RC, stencil_skin=SKIN,
+                precision=mb.MB_PREC_MIXED, max_interstitials=max(1, itl.shape[0])) as s:
+        s.upload(box, itl)
+        s.run(max(args.warmup, 3))
+        barrier(pg)
+        ms = s.time_steps(args.steps)
+        barrier(pg)
+        ms = reduce_max(pg, ms)
+    rate = n_atoms * args.steps / (ms * 1e-3)
+    return {"value": rate * (int(os.environ.get("WORLD_SIZE", "1"))), "unit": "atom-steps/s",
+            "ms_per_step": ms / args.steps, "speedup_vs_fp64": rate / fp64_rate,
+            "force_rms_rel_err_vs_fp64": err, "dtype": "f32 pairs + two-sum, f64 state",
+            "kernel": "k_ens_step (one persistent launch per step)"}
+
+
+def run_ensemble(args, mb, world, rank, local, pg) -> None:
+    """512 independent lattices (edges uniform in [8, 40] cells, seed 11; temperature
+    uniform in [300, 1200] K; 0-1% vacancies), mixed precision, one persistent
+    launch per step for all of them, tile shapes autotuned."""
+    mb.check(mb.lib().mb_env_init(local))
+    rng = np.random.default_rng(11)
+    n_lat = 512
+    edges = rng.integers(8, 41, size=(n_lat, 3))
+    temps = rng.uniform(300.0, 1200.0, size=n_lat)
+    vacs = rng.uniform(0.0, 0.01, size=n_lat)
+    ens = mb.Ensemble(mb.potential.fe_analytic(), lattice_const=A0, mass=MASS, dt=DT, cutoff=RC, stencil_skin=SKIN)
+    n_atoms = 0
+    for k in range(n_lat):
+        cells = tuple(int(e) for e in edges[k])
+        box = mb.lattice.bcc_box(cells, A0)
+        mb.lattice.add_vacancies(box, float(vacs[k]), 1000 + k)
+        mb.lattice.maxwell_boltzmann(box, None, float(temps[k]), MASS, 5000 + k)
+        ens.add(cells, box, steps=0)
+        n_atoms += int((box["type"] >= 0).sum())
+    policy, tune_ms = ens.autotune(5)
+    ens.run(max(args.warmup, 3))
+    clocks = ClockSampler(local).start()
+    barrier(pg)
+    ms = ens.time(args.steps)
+    barrier(pg)
+    clk = clocks.stop()
+    ms = reduce_max(pg, ms)
+    info = ens.info()
+    ens.close()
+    value = n_atoms * args.steps * world / (ms * 1e-3)
+    peaks = measured_peaks()
+    achieved = BYTES_MIXED * n_atoms / (ms / args.steps * 1e-3) / 1e9
+    if rank == 0:
+        print(json.dumps({
+            "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded lattices)",
+            "config": {"workload": "ensemble_512_lattices_8to40c_mixed", "lattices": n_lat, "atoms_per_gpu": n_atoms,
+                       "tiles": info["n_tiles"], "tile_policy": policy, "autotune_ms_5_steps": tune_ms,
+                       "l2": f"state {info['device_bytes'] / 1e6:.0f} MB > 126 MB L2 (no flush needed)"},
+            "roofline": {"kernel": "k_ens_step", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                         "traffic": None},
+            "gpu_launches": args.steps, "clocks": clk, "cpu_baseline": None, "e2e": None}), flush=True)
+
+
+def run_serve(args, mb, world, rank, local, pg) -> None:
+    """Continuous-batching serving: Poisson arrivals at 50 req/s (seed 13), atoms
+    log-uniform in [1e3, 2e6], steps uniform in [100, 5000], 300-1200 K, 0-1%
+    vacancies, 160 GB HBM admission budget; the first --requests requests."""
+    from misa_b200 import serve
+    mb.check(mb.lib().mb_env_init(local))
+    reqs = serve.poisson_stream(args.requests, rate=50.0, seed=13)
+    srv = serve.Server(hbm_budget_bytes=160 << 30, chunk=50)
+    clocks = ClockSampler(local).start()
+    stats = srv.serve(reqs, realtime=True)
+    clk = clocks.stop()
+    srv.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "atom-steps/s", "value": stats["atom_steps_per_s"] * world, "unit": "atom-steps/s",
+            "n_gpus": world, "steps": stats["launches"], "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic request stream",
+            "config": {"workload": "serve_poisson50_seed13", "requests": args.requests,
+                       "completed": stats["completed"], "rejected": stats["rejected"]},
+            "latency_p50_s": stats["latency_p50_s"], "latency_p99_s": stats["latency_p99_s"],
+            "makespan_s": stats["makespan_s"], "gpu_launches": stats["launches"], "clocks": clk,
+            "cpu_baseline": None, "e2e": None}), flush=True)
 
 
 def main() -> None:
@@ -330,16 +447,22 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=sorted(WORKLOADS), default="scale")
+    ap.add_argument("--config", choices=sorted(WORKLOADS) + ["ensemble", "serve"], default="scale")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    ap.add_argument("--requests", type=int, default=32, help="requests served by --config serve")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, pg = dist_setup()
     mb = _package()
-    wl = WORKLOADS[args.config]
+    wl = WORKLOADS.get(args.config, WORKLOADS["scale"])
     try:
         if args.impl == "reference":
             run_reference(args, mb, wl, world, rank)
+        elif args.config == "ensemble":
+            run_ensemble(args, mb, world, rank, local, pg)
+        elif args.config == "serve":
+            run_serve(args, mb, world, rank, local, pg)
         else:
             run_ours(args, mb, wl, world, rank, local, pg)
     finally:

@@ -1,0 +1,207 @@
+"""Continuous-batching MD server on one GPU.
+
+Requests (one periodic BCC lattice each, with its own size, temperature, vacancy
+fraction and number of steps) are admitted into slots of an ``Ensemble`` whenever
+their device memory fits the HBM budget; all admitted lattices advance together,
+one persistent kernel launch per timestep, each stopping at its own step target.
+Between chunks of launches the loop retires finished lattices (download + free)
+and admits queued requests, so work arriving while others run joins the batch as
+soon as memory frees up.  Per-request completion latency and aggregate
+atom-steps/s are reported.
+
+Host-side failure handling: malformed requests are rejected at submission; a
+request larger than the whole budget is rejected instead of queued forever; a
+request can be cancelled while queued or in flight (its slot is freed, the other
+lattices are untouched).
+"""
+from __future__ import annotations
+
+import dataclasses
+import heapq
+import time
+
+import numpy as np
+
+from . import Ensemble, lattice, potential
+from ._abi import MB_ERR_NOMEM, MbError
+
+A0 = 2.855
+MASS = 55.845
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    arrival: float          # s after the stream start
+    cells: tuple
+    steps: int
+    temperature: float
+    vacancy: float
+    seed: int
+    n_atoms: int = 0
+    # filled by the server
+    status: str = "new"     # new, queued, running, done, rejected, cancelled
+    slot: int = -1
+    admitted: float = float("nan")
+    finished: float = float("nan")
+    reason: str = ""
+    result: np.ndarray | None = None
+    energies: np.ndarray | None = None
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def cells_for_atoms(n_atoms: float, min_cells: int = 6) -> tuple:
+    """Near-cubic BCC box (2 sites per cell) with about n_atoms sites."""
+    c = max(min_cells, int(round((n_atoms / 2.0) ** (1.0 / 3.0))))
+    rest = n_atoms / (2.0 * c)
+    cy = max(min_cells, int(round(np.sqrt(rest))))
+    cz = max(min_cells, int(round(rest / cy)))
+    return (c, cy, cz)
+
+
+def poisson_stream(n: int, rate: float = 50.0, seed: int = 13, atoms=(1e3, 2e6), steps=(100, 5000),
+                   temperature=(300.0, 1200.0), vacancy=(0.0, 0.01)) -> list[Request]:
+    """Poisson arrivals (mean `rate` per s); atoms log-uniform, steps, temperature and
+    vacancy fraction uniform over the given ranges."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    out = []
+    for k in range(n):
+        na = float(np.exp(rng.uniform(np.log(atoms[0]), np.log(atoms[1]))))
+        cells = cells_for_atoms(na)
+        out.append(Request(rid=k, arrival=float(t[k]), cells=cells,
+                           steps=int(rng.integers(steps[0], steps[1] + 1)),
+                           temperature=float(rng.uniform(*temperature)), vacancy=float(rng.uniform(*vacancy)),
+                           seed=int(rng.integers(1 << 30)), n_atoms=2 * cells[0] * cells[1] * cells[2]))
+    return out
+
+
+def build_lattice(req: Request) -> np.ndarray:
+    box = lattice.bcc_box(req.cells, A0)
+    lattice.add_vacancies(box, req.vacancy, req.seed)
+    lattice.maxwell_boltzmann(box, None, req.temperature, MASS, req.seed + 1)
+    req.n_atoms = int((box["type"] >= 0).sum())
+    return box
+
+
+def validate_request(req: Request, budget: int) -> str:
+    """Why a request cannot be served at all ("" when it can)."""
+    if len(req.cells) != 3 or min(req.cells) < 6:
+        return "lattice edges must be >= 6 cells"
+    if req.steps < 1:
+        return "steps must be >= 1"
+    if not (0.0 <= req.vacancy < 0.5) or not (req.temperature >= 0.0):
+        return "bad vacancy fraction or temperature"
+    if Ensemble.lattice_bytes(req.cells, 0) > budget:
+        return "lattice larger than the whole HBM budget"
+    return ""
+
+
+class Server:
+    def __init__(self, tables: potential.EamTables | None = None, hbm_budget_bytes: int = 160 << 30,
+                 chunk: int = 50, energy_every: int = 0, keep_results: bool = False):
+        self.tables = tables or potential.fe_analytic()
+        self.budget = int(hbm_budget_bytes)
+        self.ens = Ensemble(self.tables, lattice_const=A0, mass=MASS, hbm_budget_bytes=self.budget)
+        self.chunk = chunk
+        self.energy_every = energy_every
+        self.keep_results = keep_results
+        self.queue: list[Request] = []
+        self.running: dict[int, Request] = {}
+        self.done: list[Request] = []
+        self.rejected: list[Request] = []
+        self.t0 = None
+        self.launches = 0
+
+    def close(self):
+        self.ens.close()
+
+    def now(self) -> float:
+        return time.perf_counter() - self.t0
+
+    # ------------------------------------------------------------ requests
+    def submit(self, req: Request) -> bool:
+        why = validate_request(req, self.budget)
+        if why:
+            req.status, req.reason = "rejected", why
+            self.rejected.append(req)
+            return False
+        req.status = "queued"
+        self.queue.append(req)
+        return True
+
+    def cancel(self, req: Request) -> None:
+        if req.status == "queued":
+            self.queue.remove(req)
+        elif req.status == "running":
+            self.ens.remove(req.slot)
+            del self.running[req.slot]
+        req.status = "cancelled"
+
+    def _admit(self) -> None:
+        while self.queue:
+            req = self.queue[0]
+            box = build_lattice(req)
+            try:
+                req.slot = self.ens.add(req.cells, box, steps=req.steps)
+            except MbError as e:
+                if e.code == MB_ERR_NOMEM and self.running:
+                    return  # wait for memory to free up
+                self.queue.pop(0)
+                req.status, req.reason = "rejected", str(e)
+                self.rejected.append(req)
+                continue
+            self.queue.pop(0)
+            req.status = "running"
+            req.admitted = self.now()
+            self.running[req.slot] = req
+
+    def _retire(self) -> None:
+        for slot, req in list(self.running.items()):
+            done, target, _ = self.ens.status(slot)
+            if done >= target:
+                if self.keep_results:
+                    req.result = self.ens.download(slot)[0]
+                    req.energies = self.ens.energies(slot)
+                self.ens.remove(slot)
+                del self.running[slot]
+                req.status = "done"
+                req.finished = self.now()
+                self.done.append(req)
+
+    # ------------------------------------------------------------ event loop
+    def serve(self, requests: list[Request], realtime: bool = True, max_seconds: float = 1e9,
+              on_tick=None) -> dict:
+        """Runs until every request is done, rejected or cancelled.  With realtime the
+        arrivals happen on the wall clock; otherwise all arrive at once."""
+        pending = [(r.arrival if realtime else 0.0, r.rid, r) for r in requests]
+        heapq.heapify(pending)
+        self.t0 = time.perf_counter()
+        work = 0
+        while pending or self.queue or self.running:
+            t = self.now()
+            if t > max_seconds:
+                break
+            while pending and pending[0][0] <= t:
+                self.submit(heapq.heappop(pending)[2])
+            self._admit()
+            if not self.running:
+                if pending:
+                    time.sleep(max(0.0, min(0.05, pending[0][0] - self.now())))
+                continue
+            self.launches += self.ens.advance(self.chunk, self.energy_every)
+            self._retire()
+            if on_tick:
+                on_tick(self)
+        makespan = self.now()
+        self.ens.sync()
+        for r in self.done:
+            work += r.n_atoms * r.steps
+        lat = np.array([r.latency for r in self.done]) if self.done else np.zeros(1)
+        return {"completed": len(self.done), "rejected": len(self.rejected), "makespan_s": makespan,
+                "atom_steps": work, "atom_steps_per_s": work / makespan if makespan > 0 else 0.0,
+                "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                "launches": self.launches}

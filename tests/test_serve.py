@@ -1,0 +1,82 @@
+"""Serving loop: request stream, validation, continuous batching, cancellation."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import misa_b200 as mb
+from misa_b200 import serve
+
+
+def test_poisson_stream_statistics():
+    reqs = serve.poisson_stream(2000, rate=50.0, seed=13)
+    gaps = np.diff([0.0] + [r.arrival for r in reqs])
+    assert abs(gaps.mean() - 1 / 50.0) < 0.002
+    sizes = np.array([r.n_atoms for r in reqs])
+    assert sizes.min() >= 2 * 6 ** 3 and sizes.max() <= 2.3e6
+    assert abs(np.median(np.log(sizes)) - 0.5 * (np.log(1e3) + np.log(2e6))) < 0.3
+    steps = np.array([r.steps for r in reqs])
+    assert steps.min() >= 100 and steps.max() <= 5000
+    assert all(300 <= r.temperature <= 1200 and 0 <= r.vacancy <= 0.01 for r in reqs)
+
+
+def test_request_validation_without_a_device():
+    budget = 64 << 20
+    ok = serve.Request(0, 0.0, (8, 8, 8), 10, 300.0, 0.0, 1)
+    assert serve.validate_request(ok, budget) == ""
+    assert "edges" in serve.validate_request(serve.Request(1, 0.0, (3, 8, 8), 10, 300.0, 0.0, 1), budget)
+    assert "steps" in serve.validate_request(serve.Request(2, 0.0, (8, 8, 8), 0, 300.0, 0.0, 1), budget)
+    assert "vacancy" in serve.validate_request(serve.Request(3, 0.0, (8, 8, 8), 5, 300.0, 0.9, 1), budget)
+    assert "budget" in serve.validate_request(serve.Request(4, 0.0, (200, 200, 200), 5, 300.0, 0.0, 1), budget)
+
+
+def _small_stream(n, seed=5):
+    return serve.poisson_stream(n, rate=200.0, seed=seed, atoms=(1e3, 2e4), steps=(10, 40))
+
+
+def _alone(req):
+    with mb.Ensemble(mb.potential.fe_analytic(), lattice_const=serve.A0, mass=serve.MASS) as ens:
+        s = ens.add(req.cells, serve.build_lattice(req), steps=req.steps)
+        ens.advance(10 * req.steps + 10)
+        return ens.download(s)[0]
+
+
+@pytest.mark.gpu
+def test_continuous_batching_results_match_alone_runs():
+    reqs = _small_stream(10)
+    srv = serve.Server(chunk=7, keep_results=True)
+    stats = srv.serve(reqs, realtime=True)
+    srv.close()
+    assert stats["completed"] == 10 and stats["rejected"] == 0
+    assert stats["atom_steps_per_s"] > 0 and stats["latency_p99_s"] >= stats["latency_p50_s"] > 0
+    # arrivals overlapped with running work: some request was admitted while others ran
+    assert any(r.admitted > min(q.admitted for q in reqs) for r in reqs)
+    for r in reqs[:4]:
+        assert np.array_equal(r.result["x"], _alone(r)["x"])
+
+
+@pytest.mark.gpu
+def test_budget_queues_and_faults_are_contained():
+    reqs = _small_stream(8, seed=9)
+    one = max(mb.Ensemble.lattice_bytes(r.cells, 0) for r in reqs)
+    srv = serve.Server(hbm_budget_bytes=int(1.6 * one), chunk=5, keep_results=True)
+    bad = serve.Request(100, 0.0, (2, 2, 2), 10, 300.0, 0.0, 1)
+    huge = serve.Request(101, 0.0, (300, 300, 300), 10, 300.0, 0.0, 1)
+    peak = []
+    victim = reqs[3]
+
+    def tick(s):
+        peak.append(len(s.running))
+        if victim.status == "running" and len(peak) == 2:
+            s.cancel(victim)
+
+    stats = srv.serve(reqs + [bad, huge], realtime=False, on_tick=tick)
+    srv.close()
+    assert bad.status == "rejected" and huge.status == "rejected"
+    assert max(peak) < len(reqs)  # the budget made later requests wait for memory
+    waited = [r for r in reqs if r.status == "done" and r.admitted > min(q.finished for q in reqs if q.status == "done")]
+    assert waited
+    finished = [r for r in reqs if r.status == "done"]
+    assert len(finished) + (victim.status == "cancelled") == len(reqs)
+    for r in finished[:3]:
+        assert np.array_equal(r.result["x"], _alone(r)["x"])
