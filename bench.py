@@ -89,13 +89,15 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def ncu_traffic(kernel: str) -> float | None:
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+def ncu_traffic(kernel: str, n_atoms: int) -> float | None:
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, scaled from the
+    profiled atom count to n_atoms (traffic grows in proportion to the lattice)."""
     p = ROOT / "profiles" / "traffic.json"
     if not p.exists():
         return None
     try:
-        return float(json.loads(p.read_text())[kernel]["dram_bytes_per_launch"])
+        d = json.loads(p.read_text())[kernel]
+        return float(d["dram_bytes_per_launch"]) * n_atoms / float(d["atoms"])
     except Exception:
         return None
 
@@ -271,7 +273,7 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
                                       BYTES_MIXED * n_atoms, FLOP_RHO + FLOP_FORCE, force_ms)
         fpeak, fname = f32.value, "fp32"
     achieved = kbytes / (kms * 1e-3) / 1e9
-    traffic = ncu_traffic(kname.split()[0])
+    traffic = ncu_traffic(kname.split()[0], n_atoms)
     roofline = {
         "kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
