@@ -214,10 +214,30 @@ static int ens_stencil(mb_ensemble *e) {
   EnsParams &P = e->P;
   P.n_st = n;
   const double rdr = P.P.rdr;
+  int n_near[2] = {0, 0};
   for (int s = 0; s < 2; s++) {
-    const int64_t *src = s ? odd : even;
+    const int64_t *src0 = s ? odd : even;
+    // entries ordered by ideal distance: the ones inside the cutoff first (walked
+    // without a per-pair branch), the outer shells after (mostly beyond the cutoff)
+    std::vector<std::pair<double, int64_t>> ord;
     for (int k = 0; k < n; k++) {
-      const long long o = src[k];
+      const long long o = src0[k];
+      long long dz = (o >= 0 ? (o + (long long)EX * EY / 2) : (o - (long long)EX * EY / 2)) / ((long long)EX * EY);
+      long long rem = o - dz * (long long)EX * EY;
+      long long dy = (rem >= 0 ? rem + EX / 2 : rem - EX / 2) / EX;
+      long long dx = rem - dy * EX;
+      const int s2 = (int)((s + dx) & 1);
+      const double ox = 0.5 * (double)dx, oy = (double)dy + 0.5 * (s2 - s), oz = (double)dz + 0.5 * (s2 - s);
+      ord.push_back({a0 * sqrt(ox * ox + oy * oy + oz * oz), o});
+    }
+    std::stable_sort(ord.begin(), ord.end(),
+                     [](const std::pair<double, int64_t> &x, const std::pair<double, int64_t> &y) {
+                       return x.first < y.first;
+                     });
+    for (int k = 0; k < n; k++)
+      if (ord[k].first < e->cfg.cutoff) n_near[s]++;
+    for (int k = 0; k < n; k++) {
+      const long long o = ord[k].second;
       long long dz = (o >= 0 ? (o + (long long)EX * EY / 2) : (o - (long long)EX * EY / 2)) / ((long long)EX * EY);
       long long rem = o - dz * (long long)EX * EY;
       long long dy = (rem >= 0 ? rem + EX / 2 : rem - EX / 2) / EX;
@@ -235,19 +255,29 @@ static int ens_stencil(mb_ensemble *e) {
       P.ck[s][k] = make_float4((float)cx, (float)cy, (float)cz, (float)R);
       const double pk = R * rdr;
       const double mk = floor(pk);
-      P.mk[s][k] = (int)mk;
-      P.fk[s][k] = (float)(pk - mk);
+      P.kf[s][k] = make_float2((float)(pk - mk), (float)mk);
       for (int sh = 0; sh < ENS_NSHAPE; sh++) {
         const int TXH = kShapes[sh][0] + 4, TYH = kShapes[sh][1] + 4, TZH = kShapes[sh][2] + 4;
         P.soff[sh][s][k] = (int)((s2 - s) * TXH * TYH * TZH + (dz * TYH + dy) * TXH + dcx);
       }
     }
   }
+  if (n_near[0] != n_near[1]) return fail(MB_ERR_STATE, "even and odd stencils differ inside the cutoff");
+  P.n_near = n_near[0];
   for (int sh = 0; sh < ENS_NSHAPE; sh++) {
     P.shape_dims[sh][0] = kShapes[sh][0];
     P.shape_dims[sh][1] = kShapes[sh][1];
     P.shape_dims[sh][2] = kShapes[sh][2];
     P.shape_dims[sh][3] = shape_bytes(sh);
+    auto lg = [](int v) {
+      int l = 0;
+      while ((1 << l) < v) l++;
+      return l;
+    };
+    P.shape_log[sh][0] = lg(kShapes[sh][0]);
+    P.shape_log[sh][1] = lg(kShapes[sh][1]);
+    P.shape_log[sh][2] = lg(kShapes[sh][2]);
+    P.shape_log[sh][3] = P.shape_log[sh][0] + P.shape_log[sh][1] + P.shape_log[sh][2];
   }
   return MB_OK;
 }
@@ -274,7 +304,7 @@ static size_t lattice_bytes(int cx, int cy, int cz, int cap_itl) {
   const int per = 2 * 4 * 64 + 64; // flagged sites per interstitial (upper bound of the window sphere)
   const size_t ci = (size_t)std::max(1, cap_itl);
   return 2 * a(n * 16) + 6 * a(n * 8) + 4 * a(n * 4) + a(n) + a(nb * 8) + a(ci * 8) * 16 + a(ci) +
-         a((size_t)std::max(1, cap_itl * per) * 4) + a(8) + a(ci * 8);
+         a((size_t)std::max(1, cap_itl * per) * 4) + a(16) + a(ci * 8);
 }
 
 static int sync_desc(mb_ensemble *e) {
@@ -315,7 +345,8 @@ static int rebuild(mb_ensemble *e) {
   const int nl = (int)e->order.size();
   std::vector<LatDesc> descs(nl);
   std::vector<CUtensorMap> maps(2 * (size_t)std::max(1, nl));
-  std::vector<int> tile_lat, tile_idx, tile_first(nl + 1, 0), itl_lats;
+  std::vector<int> tile_lat, tile_first(nl + 1, 0), itl_lats;
+  std::vector<unsigned> tile_idx;
   for (int c = 0; c < nl; c++) {
     LatHost &L = e->slots[e->order[c]];
     const int shape = e->policy >= 0 ? e->policy : (L.policy_shape >= 0 ? L.policy_shape : model_shape(L.d.bcx, L.d.by, L.d.bz));
@@ -328,10 +359,14 @@ static int rebuild(mb_ensemble *e) {
     maps[2 * c + 1] = L.tmap[1];
     const int nt = L.d.ntx * L.d.nty * L.d.ntz;
     tile_first[c] = (int)tile_lat.size();
-    for (int k = 0; k < nt; k++) {
-      tile_lat.push_back(c);
-      tile_idx.push_back(k);
-    }
+    for (int tz = 0; tz < L.d.ntz; tz++)
+      for (int ty = 0; ty < L.d.nty; ty++)
+        for (int tx = 0; tx < L.d.ntx; tx++) {
+          tile_lat.push_back(c);
+          tile_idx.push_back((unsigned)(tx * kShapes[shape][0]) | ((unsigned)(ty * kShapes[shape][1]) << 11) |
+                             ((unsigned)(tz * kShapes[shape][2]) << 22));
+        }
+    (void)nt;
     if (L.d.n_itl > 0) itl_lats.push_back(c);
     descs[c] = L.d;
   }
@@ -380,7 +415,7 @@ static int rebuild(mb_ensemble *e) {
                             e->stream));
     MB_CUDA(cudaMemcpyAsync(e->d_tile_lat, tile_lat.data(), sizeof(int) * tile_lat.size(), cudaMemcpyHostToDevice,
                             e->stream));
-    MB_CUDA(cudaMemcpyAsync(e->d_tile_idx, tile_idx.data(), sizeof(int) * tile_idx.size(), cudaMemcpyHostToDevice,
+    MB_CUDA(cudaMemcpyAsync(e->d_tile_idx, tile_idx.data(), sizeof(unsigned) * tile_idx.size(), cudaMemcpyHostToDevice,
                             e->stream));
     MB_CUDA(cudaMemcpyAsync(e->d_tile_first, tile_first.data(), sizeof(int) * (nl + 1), cudaMemcpyHostToDevice,
                             e->stream));
@@ -393,7 +428,7 @@ static int rebuild(mb_ensemble *e) {
   P.lats = e->d_lats;
   P.n_lats = nl;
   P.tile_lat = e->d_tile_lat;
-  P.tile_idx = e->d_tile_idx;
+  P.tile_org = (const unsigned *)e->d_tile_idx;
   P.n_tiles = e->n_tiles;
   P.tmaps = e->d_tmaps;
   P.epart = e->d_epart;
@@ -572,7 +607,7 @@ int mb_ensemble_create(const mb_ensemble_config *cfg, const mb_eam_tables *pot, 
   P.reach = cfg->cutoff + cfg->stencil_skin;
   if ((rc = ens_stencil(e)) != MB_OK) return bail(rc);
   // shared-memory knots: as many of the last ones as fit beside two tile buffers
-  const int budget = 232448 - 2048 - 2 * ENS_TILE_MAX_BYTES - 16;
+  const int budget = 232448 - 2048 - 2 * ENS_TILE_MAX_BYTES - 32;
   P.nsm = std::min(P.P.nr, budget / (int)(sizeof(float4) + 3 * sizeof(float2)));
   P.m_lo = P.P.nr - P.nsm;
   if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -620,6 +655,7 @@ int mb_ensemble_add(mb_ensemble *e, const mb_lattice_spec *spec, const mb_atom_e
   std::lock_guard<std::mutex> lk(e->mu);
   const int cx = spec->cells_x, cy = spec->cells_y, cz = spec->cells_z;
   if (cx < 2 || cy < 2 || cz < 2) return fail(MB_ERR_ARG, "lattice edges must be >= 2 cells");
+  if (cx > 2000 || cy > 2000 || cz > 1000) return fail(MB_ERR_ARG, "lattice edges must be <= 2000 x 2000 x 1000 cells");
   const double reach = e->cfg.cutoff + e->cfg.stencil_skin, a0 = e->cfg.lattice_const;
   if (cx * a0 <= 2 * reach || cy * a0 <= 2 * reach || cz * a0 <= 2 * reach)
     return fail(MB_ERR_ARG, "box edge must exceed 2 * (cutoff + stencil_skin)");
@@ -713,7 +749,7 @@ int mb_ensemble_add(mb_ensemble *e, const mb_lattice_spec *spec, const mb_atom_e
   L.iids = (int64_t *)take(ci * 8);
   d.itype = (int8_t *)take(ci);
   d.flag_list = (int *)take((size_t)d.cap_flag * 4);
-  d.flag_count = (int *)take(8);
+  d.flag_count = (int *)take(16); // [count parity 0, count parity 1, overflow, -]
   if ((size_t)(p - (char *)block) > bytes) return fail(MB_ERR_STATE, "lattice layout overflows its block");
   cudaStream_t s = e->stream;
   auto undo = [&](int code) {
@@ -815,9 +851,9 @@ int mb_ensemble_sync(mb_ensemble *e) {
   for (size_t c = 0; c < e->order.size(); c++) {
     const LatHost &L = e->slots[e->order[c]];
     if (L.d.n_itl > 0) {
-      int fc[2];
+      int fc[3];
       MB_CUDA(cudaMemcpy(fc, L.d.flag_count, sizeof(fc), cudaMemcpyDeviceToHost));
-      if (fc[1]) return fail(MB_ERR_ARG, "interstitial flag list overflowed");
+      if (fc[2]) return fail(MB_ERR_ARG, "interstitial flag list overflowed");
     }
   }
   return MB_OK;

@@ -7,59 +7,80 @@
 namespace mb {
 
 // ------------------------------------------------------------- tile phases
+// Pipeline: two tiles in flight.  Every warp waits for its tile's full mbarrier,
+// computes one site per thread and releases the buffer (empty mbarrier, one arrival
+// per warp); lane 0 of warp 0 then loads tile i + 2 into that buffer once all warps
+// released it.  No CTA-wide barrier per tile (except the energy reduction on energy
+// steps).  Every wait is bounded.
 struct TileCtx {
   char *buf[2];
-  uint64_t *bar;
-  unsigned phase; // bit b: parity of the next completion of buffer b
+  uint64_t *full;   // [2] completed by the TMA transaction count
+  uint64_t *empty;  // [2] completed by ENS_CONSUMERS / 32 warp arrivals
+  unsigned fphase;  // consumer: parity of the next full completion, bit per buffer
+  unsigned ephase;  // producer: parity of the next empty completion, bit per buffer
+  unsigned used;    // producer: buffers that have held a tile already
 };
 
-__device__ __forceinline__ bool tile_live(const EnsParams &P, int t) {
-  return lat_active(P.lats[P.tile_lat[t]]);
-}
+__device__ __forceinline__ bool tile_live(const EnsParams &P, int t) { return lat_active(P.lats[P.tile_lat[t]]); }
 
-// Thread 0 issues the TMA load of tile t into buffer b.
+// Thread issuing the TMA load of tile t into buffer b.
 __device__ __forceinline__ void issue_tile(const EnsParams &P, TileCtx &T, int t, int b) {
   const int l = P.tile_lat[t];
   const LatDesc &d = P.lats[l];
-  const int *sh = P.shape_dims[d.shape];
-  const int ti = P.tile_idx[t];
-  const int tx = ti % d.ntx, ty = (ti / d.ntx) % d.nty, tz = ti / (d.ntx * d.nty);
-  mbar_expect_tx(&T.bar[b], (unsigned)sh[3]);
-  tma_load_5d(T.buf[b], &P.tmaps[2 * l + d.cur], 0, tx * sh[0], ty * sh[1], tz * sh[2], 0, &T.bar[b]);
+  const unsigned org = P.tile_org[t];
+  mbar_expect_tx(&T.full[b], (unsigned)P.shape_dims[d.shape][3]);
+  tma_load_5d(T.buf[b], &P.tmaps[2 * l + d.cur], 0, (int)(org & 2047u), (int)((org >> 11) & 2047u), (int)(org >> 22),
+              0, &T.full[b]);
 }
 
-// All threads wait for buffer b with a bounded poll.  If any thread gives up, the
-// whole CTA raises err, drains the copy once more (bounded) and reports false.
-__device__ __forceinline__ bool wait_tile(const EnsParams &P, TileCtx &T, int b) {
-  __shared__ int s_timeout;
-  if (threadIdx.x == 0) s_timeout = 0;
-  __syncthreads();
-  const unsigned par = (T.phase >> b) & 1u;
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Bounded wait on an mbarrier phase; raises err (code) when it gives up.
+__device__ __forceinline__ void bounded_wait(const EnsParams &P, uint64_t *bar, unsigned parity, int code) {
   unsigned spins = 0;
-  bool ok = true;
-  while (!mbar_try_wait(&T.bar[b], par)) {
+  while (!mbar_try_wait(bar, parity)) {
     if (++spins > ENS_WAIT_SPINS) {
-      ok = false;
-      break;
-    }
-  }
-  if (!ok) s_timeout = 1;
-  __syncthreads();
-  if (s_timeout) {
-    if (threadIdx.x == 0) {
-      atomicExch(P.err, 2);
+      atomicExch(P.err, code);
+      // a second bounded wait lets a copy still in flight land before anyone moves on
       unsigned again = 0;
-      while (!mbar_try_wait(&T.bar[b], par) && ++again < ENS_WAIT_SPINS) {
+      while (!mbar_try_wait(bar, parity) && ++again < ENS_WAIT_SPINS) {
       }
+      return;
     }
-    __syncthreads();
-    return false;
   }
-  T.phase ^= 1u << b;
-  return true;
 }
 
-// Site of thread `tid` inside a tile of shape sh, and its indices.
+// Producer role, held by lane 0 of warp 0: keeps two live tiles in flight.  Tile
+// i + 2 goes into the buffer of tile i once every warp has released that buffer;
+// warp 0 therefore paces the CTA while the other warps run ahead by up to a tile.
+struct Producer {
+  int next; // next tile index to consider
+  int nb;   // buffer of the next issue
+};
+
+__device__ __forceinline__ void producer_start(const EnsParams &P, TileCtx &T, Producer &pr) {
+  pr.next = blockIdx.x;
+  pr.nb = 0;
+}
+
+__device__ __forceinline__ void producer_issue(const EnsParams &P, TileCtx &T, Producer &pr) {
+  while (pr.next < P.n_tiles && !tile_live(P, pr.next)) pr.next += gridDim.x;
+  if (pr.next >= P.n_tiles) return;
+  if (threadIdx.x == 0) {
+    if (T.used & (1u << pr.nb)) {
+      bounded_wait(P, &T.empty[pr.nb], (T.ephase >> pr.nb) & 1u, 3);
+      T.ephase ^= 1u << pr.nb;
+    }
+    T.used |= 1u << pr.nb;
+    issue_tile(P, T, pr.next, pr.nb);
+  }
+  pr.next += gridDim.x;
+  pr.nb ^= 1;
+}
+
+// Site of consumer thread `tid` inside a tile of shape sh, and its indices.
 struct SiteRef {
   bool valid;
   int s, x, y, z;      // tile-local
@@ -68,19 +89,17 @@ struct SiteRef {
   int bcx, by, bz;     // box coordinates (cx per sublattice)
 };
 
-__device__ __forceinline__ SiteRef site_of(const LatDesc &d, const int *sh, int ti, int tid) {
+__device__ __forceinline__ SiteRef site_of(const LatDesc &d, const int *sh, const int *lg, unsigned org, int tid) {
   SiteRef r;
   const int TX = sh[0], TY = sh[1], TZ = sh[2];
-  const int per = TX * TY * TZ;
-  r.s = tid / per;
-  const int rem = tid - r.s * per;
-  r.x = rem % TX;
-  r.y = (rem / TX) % TY;
-  r.z = rem / (TX * TY);
-  const int tx = ti % d.ntx, ty = (ti / d.ntx) % d.nty, tz = ti / (d.ntx * d.nty);
-  r.bcx = tx * TX + r.x;
-  r.by = ty * TY + r.y;
-  r.bz = tz * TZ + r.z;
+  r.s = tid >> lg[3];
+  const int rem = tid & ((1 << lg[3]) - 1);
+  r.x = rem & (TX - 1);
+  r.y = (rem >> lg[0]) & (TY - 1);
+  r.z = rem >> (lg[0] + lg[1]);
+  r.bcx = (int)(org & 2047u) + r.x;
+  r.by = (int)((org >> 11) & 2047u) + r.y;
+  r.bz = (int)(org >> 22) + r.z;
   r.valid = r.s < 2 && r.bcx < d.bcx && r.by < d.by && r.bz < d.bz;
   const int TXH = TX + 4, TYH = TY + 4, TZH = TZ + 4;
   r.o = ((r.s * TZH + r.z + 2) * TYH + r.y + 2) * TXH + r.x + 2;
@@ -90,230 +109,328 @@ __device__ __forceinline__ SiteRef site_of(const LatDesc &d, const int *sh, int 
 
 // Spline knot and local coordinate of a pair from its deviation eps = r - R_k.
 __device__ __forceinline__ void knot_of(const EnsParams &P, int s, int k, float eps, int &m, float &q) {
-  const float t = P.fk[s][k] + eps * P.rdr;
+  const float2 kf = P.kf[s][k];
+  const float t = kf.x + eps * P.rdr;
   const float fl = floorf(t);
-  m = P.mk[s][k] + (int)fl;
   q = t - fl;
-  if (m > P.P.nr - 2) {
-    m = P.P.nr - 2;
-    q = 1.0f;
-  }
-  if (m < 0) {
-    m = 0;
-    q = 0.0f;
-  }
+  m = min(max((int)(kf.y + fl), 0), P.P.nr - 2);
+}
+
+// Pair geometry shared by both passes (x and y in f32x2 lanes): returns false
+// beyond the cutoff; on success r2 and the spline deviation numerator are set.
+struct PairGeo {
+  float2 dxy;
+  float dz, r2, num;
+};
+
+// ALWAYS: also compute the numerator beyond the cutoff (branch-free walking).
+template <bool ALWAYS>
+__device__ __forceinline__ bool pair_geo(const EnsParams &P, const float4 &u, const float4 &nb, const float4 &C,
+                                         PairGeo &g) {
+  const float2 m1 = make_float2(-1.f, -1.f);
+  const float2 exy = __ffma2_rn(make_float2(nb.x, nb.y), m1, make_float2(u.x, u.y)); // u - nb
+  const float ez = u.z - nb.z;
+  g.dxy = __fadd2_rn(make_float2(C.x, C.y), exy);
+  g.dz = C.z + ez;
+  const float2 sq = __fmul2_rn(g.dxy, g.dxy);
+  g.r2 = sq.x + sq.y + g.dz * g.dz;
+  const bool in = g.r2 < P.rc2f;
+  if (!ALWAYS && !in) return false;
+  const float2 pe = __fmul2_rn(__ffma2_rn(make_float2(2.f, 2.f), make_float2(C.x, C.y), exy), exy); // (2C + e) e
+  g.num = pe.x + pe.y + (2.f * C.z + ez) * ez;
+  return in;
+}
+
+// One density pair.  BF (branch-free): entries inside the cutoff for nearly every
+// lane; the value is masked instead of branched around so iterations overlap.
+template <bool BF>
+__device__ __forceinline__ void rho_pair(const EnsParams &P, const float4 &u, const float4 &nb, const float4 &C, int s,
+                                         int k, const float4 *s_fv, float &rs, float &rc) {
+  PairGeo g;
+  const bool in = pair_geo<BF>(P, u, nb, C, g);
+  if (!BF && !in) return;
+  const float r = g.r2 * rsqrtf(g.r2);
+  int m;
+  float q;
+  knot_of(P, s, k, __fdividef(g.num, r + C.w), m, q);
+  const float4 c = (m >= P.m_lo) ? s_fv[m - P.m_lo] : __ldg(&P.P.f_val32[m]);
+  float v = ((c.w * q + c.z) * q + c.y) * q + c.x;
+  if (BF) v = in ? v : 0.f;
+  two_sum(rs, rc, v);
 }
 
 template <bool ENERGY>
-__device__ void rho_tiles(const EnsParams &P, TileCtx &T, const float4 *s_fv, double *e_acc) {
+__device__ void rho_tiles(const EnsParams &P, TileCtx &T, const float4 *s_fv) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int b = 0;
-  int t = blockIdx.x;
-  if (t < P.n_tiles && threadIdx.x == 0 && tile_live(P, t)) issue_tile(P, T, t, 0);
-  for (; t < P.n_tiles; t += gridDim.x) {
-    const int tn = t + gridDim.x;
-    if (tn < P.n_tiles && threadIdx.x == 0 && tile_live(P, tn)) issue_tile(P, T, tn, b ^ 1);
-    if (tile_live(P, t)) {
-      if (!wait_tile(P, T, b)) return;
-      const LatDesc &d = P.lats[P.tile_lat[t]];
-      const int *sh = P.shape_dims[d.shape];
-      const SiteRef me = site_of(d, sh, P.tile_idx[t], threadIdx.x);
-      const float4 *tile = reinterpret_cast<const float4 *>(T.buf[b]);
-      double e_site = 0.0;
-      if (me.valid) {
-        const int code = d.code[me.i];
-        if (code >= 0 && !(code & MB_FLAG_ITL)) {
-          const float4 u = tile[me.o];
-          const int *soff = P.soff[d.shape][me.s];
-          float rs = 0.f, rc = 0.f;
-#pragma unroll 4
-          for (int k = 0; k < P.n_st; k++) {
-            const float4 nb = tile[me.o + soff[k]];
-            const float4 C = P.ck[me.s][k];
-            const float ex = u.x - nb.x, ey = u.y - nb.y, ez = u.z - nb.z;
-            const float dx = C.x + ex, dy = C.y + ey, dz = C.z + ez;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 < P.rc2f) {
-              const float num = 2.f * (C.x * ex + C.y * ey + C.z * ez) + (ex * ex + ey * ey + ez * ez);
-              const float r = r2 * rsqrtf(r2);
-              const float eps = __fdividef(num, r + C.w);
-              int m;
-              float q;
-              knot_of(P, me.s, k, eps, m, q);
-              const float4 c = (m >= P.m_lo) ? s_fv[m - P.m_lo] : __ldg(&P.P.f_val32[m]);
-              two_sum(rs, rc, ((c.w * q + c.z) * q + c.y) * q + c.x);
-            }
-          }
-          const double rho = (double)rs + (double)rc;
-          const double df = dF64(P.P, code & 0x3F, rho);
-          float4 *u4 = d.u4[d.cur];
-          reinterpret_cast<float *>(u4 + me.i)[3] = (float)df;
-          d.rho[me.i] = (float)rho;
-          const Geom g = lat_geom(d);
-          for_images(g, me.s, me.bcx, me.by, me.bz,
-                     [&](long long idx, double, double, double) { reinterpret_cast<float *>(u4 + idx)[3] = (float)df; });
-          if (ENERGY) e_site = F64(P.P, code & 0x3F, rho);
-        }
-      }
-      if (ENERGY) {
-        const double tsum = block_sum(e_site);
-        if (threadIdx.x == 0) P.epart[2 * t] = tsum;
-      }
-    } else if (ENERGY && threadIdx.x == 0) {
-      P.epart[2 * t] = 0.0;
+  Producer pr;
+  producer_start(P, T, pr);
+  if (warp == 0) {
+    producer_issue(P, T, pr);
+    producer_issue(P, T, pr);
+  }
+  for (int t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+    if (!tile_live(P, t)) {
+      if (ENERGY && threadIdx.x == 0) P.epart[2 * t] = 0.0;
+      continue;
     }
-    __syncthreads(); // buffer b is free again
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    bounded_wait(P, &T.full[b], (T.fphase >> b) & 1u, 2);
+    T.fphase ^= 1u << b;
+    const LatDesc &d = P.lats[P.tile_lat[t]];
+    const SiteRef me = site_of(d, P.shape_dims[d.shape], P.shape_log[d.shape], P.tile_org[t], threadIdx.x);
+    const float4 *tile = reinterpret_cast<const float4 *>(T.buf[b]);
+    double e_site = 0.0;
+    int code = -1;
+    if (me.valid) code = d.code[me.i];
+    const bool work = me.valid && code >= 0 && !(code & MB_FLAG_ITL);
+    float rs0 = 0.f, rc0 = 0.f, rs1 = 0.f, rc1 = 0.f;
+    if (work) {
+      const float4 u = tile[me.o];
+      const int *soff = P.soff[d.shape][me.s];
+      const int n = P.n_st, nn = P.n_near;
+      const int s = me.s;
+      int k = 0;
+      for (; k + 1 < nn; k += 2) {
+        const float4 nb0 = tile[me.o + soff[k]], nb1 = tile[me.o + soff[k + 1]];
+        rho_pair<true>(P, u, nb0, P.ck[s][k], s, k, s_fv, rs0, rc0);
+        rho_pair<true>(P, u, nb1, P.ck[s][k + 1], s, k + 1, s_fv, rs1, rc1);
+      }
+      if (k < nn) {
+        rho_pair<true>(P, u, tile[me.o + soff[k]], P.ck[s][k], s, k, s_fv, rs0, rc0);
+        k++;
+      }
+      for (; k + 1 < n; k += 2) {
+        const float4 nb0 = tile[me.o + soff[k]], nb1 = tile[me.o + soff[k + 1]];
+        rho_pair<false>(P, u, nb0, P.ck[s][k], s, k, s_fv, rs0, rc0);
+        rho_pair<false>(P, u, nb1, P.ck[s][k + 1], s, k + 1, s_fv, rs1, rc1);
+      }
+      if (k < n) rho_pair<false>(P, u, tile[me.o + soff[k]], P.ck[s][k], s, k, s_fv, rs0, rc0);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&T.empty[b]); // tile data no longer needed by this warp
+    if (warp == 0) producer_issue(P, T, pr);  // tile i + 2 into this buffer
+    if (work) {
+      const double rho = ((double)rs0 + (double)rs1) + ((double)rc0 + (double)rc1);
+      const double df = dF64(P.P, code & 0x3F, rho);
+      float4 *u4 = d.u4[d.cur];
+      reinterpret_cast<float *>(u4 + me.i)[3] = (float)df;
+      d.rho[me.i] = (float)rho;
+      const Geom g = lat_geom(d);
+      for_images(g, me.s, me.bcx, me.by, me.bz,
+                 [&](long long idx, double, double, double) { reinterpret_cast<float *>(u4 + idx)[3] = (float)df; });
+      if (ENERGY) e_site = F64(P.P, code & 0x3F, rho);
+    }
+    if (ENERGY) {
+      const double tsum = block_sum(e_site);
+      if (threadIdx.x == 0) P.epart[2 * t] = tsum;
+    }
+    (void)warp;
     b ^= 1;
   }
-  (void)e_acc;
+}
+
+// Knuth two-sum on packed pairs of lanes (f32x2 instructions).
+__device__ __forceinline__ void two_sum2(float2 &s, float2 &c, float2 x) {
+  const float2 m1 = make_float2(-1.f, -1.f);
+  const float2 t = __fadd2_rn(s, x);
+  const float2 bp = __ffma2_rn(s, m1, t);                  // t - s
+  const float2 sa = __ffma2_rn(__ffma2_rn(bp, m1, t), m1, s); // s - (t - bp)
+  const float2 xb = __ffma2_rn(bp, m1, x);                  // x - bp
+  c = __fadd2_rn(c, __fadd2_rn(sa, xb));
+  s = t;
+}
+
+// One pair of the force pass: x and y components ride together in f32x2 lanes, and
+// the derivative pieces of f and phi (stored as {f', phi'} pairs per knot) are
+// evaluated by one packed Horner chain.
+template <bool ENERGY, bool BF>
+__device__ __forceinline__ void force_pair(const EnsParams &P, const float4 &u, const float4 &nb, const float4 &C,
+                                           int s, int k, const float2 *s_fd, float2 &fxy_s, float2 &fxy_c, float &zs,
+                                           float &zc, float &ps, float &pc) {
+  PairGeo g;
+  const bool in = pair_geo<BF>(P, u, nb, C, g);
+  if (!BF && !in) return;
+  const float r2 = g.r2, num = g.num, dz = g.dz;
+  const float2 dxy = g.dxy;
+  float rinv = rsqrtf(r2);
+  rinv = rinv * (1.5f - 0.5f * r2 * rinv * rinv);
+  const float r = r2 * rinv;
+  int m;
+  float q;
+  knot_of(P, s, k, __fdividef(num, r + C.w), m, q);
+  float2 c0, c1, c2;
+  if (m >= P.m_lo) {
+    const float2 *cp = s_fd + 3 * (m - P.m_lo);
+    c0 = cp[0];
+    c1 = cp[1];
+    c2 = cp[2];
+  } else {
+    const float2 *cp = P.P.force32 + 3 * m;
+    c0 = __ldg(cp);
+    c1 = __ldg(cp + 1);
+    c2 = __ldg(cp + 2);
+  }
+  const float2 qq = make_float2(q, q);
+  const float2 dd = __ffma2_rn(__ffma2_rn(c2, qq, c1), qq, c0); // {f'(r), phi'(r)}
+  float fpair = -((u.w + nb.w) * dd.x + dd.y) * rinv;
+  if (BF) fpair = in ? fpair : 0.f;
+  two_sum2(fxy_s, fxy_c, __fmul2_rn(dxy, make_float2(fpair, fpair)));
+  two_sum(zs, zc, dz * fpair);
+  if (ENERGY) {
+    const float4 pv = __ldg(&P.P.phi_val32[m]);
+    float e = 0.5f * (((pv.w * q + pv.z) * q + pv.y) * q + pv.x);
+    if (BF) e = in ? e : 0.f;
+    two_sum(ps, pc, e);
+  }
 }
 
 template <bool ENERGY>
 __device__ void force_tiles(const EnsParams &P, TileCtx &T, const float2 *s_fd) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int b = 0;
-  int t = blockIdx.x;
-  if (t < P.n_tiles && threadIdx.x == 0 && tile_live(P, t)) issue_tile(P, T, t, 0);
-  for (; t < P.n_tiles; t += gridDim.x) {
-    const int tn = t + gridDim.x;
-    if (tn < P.n_tiles && threadIdx.x == 0 && tile_live(P, tn)) issue_tile(P, T, tn, b ^ 1);
-    if (tile_live(P, t)) {
-      if (!wait_tile(P, T, b)) return;
-      const LatDesc &d = P.lats[P.tile_lat[t]];
-      const int *sh = P.shape_dims[d.shape];
-      const SiteRef me = site_of(d, sh, P.tile_idx[t], threadIdx.x);
-      const float4 *tile = reinterpret_cast<const float4 *>(T.buf[b]);
-      double e_pair = 0.0, e_kin = 0.0;
-      if (me.valid) {
-        const int code = d.code[me.i];
-        if (code >= 0 && !(code & MB_FLAG_ITL)) {
-          const float4 u = tile[me.o];
-          const int *soff = P.soff[d.shape][me.s];
-          float xs = 0.f, xc = 0.f, ys = 0.f, yc = 0.f, zs = 0.f, zc = 0.f, ps = 0.f, pc = 0.f;
-#pragma unroll 2
-          for (int k = 0; k < P.n_st; k++) {
-            const float4 nb = tile[me.o + soff[k]];
-            const float4 C = P.ck[me.s][k];
-            const float ex = u.x - nb.x, ey = u.y - nb.y, ez = u.z - nb.z;
-            const float dx = C.x + ex, dy = C.y + ey, dz = C.z + ez;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 < P.rc2f) {
-              const float num = 2.f * (C.x * ex + C.y * ey + C.z * ez) + (ex * ex + ey * ey + ez * ez);
-              float rinv = rsqrtf(r2);
-              rinv = rinv * (1.5f - 0.5f * r2 * rinv * rinv);
-              const float r = r2 * rinv;
-              const float eps = __fdividef(num, r + C.w);
-              int m;
-              float q;
-              knot_of(P, me.s, k, eps, m, q);
-              float2 c0, c1, c2;
-              if (m >= P.m_lo) {
-                const float2 *cp = s_fd + 3 * (m - P.m_lo);
-                c0 = cp[0];
-                c1 = cp[1];
-                c2 = cp[2];
-              } else {
-                const float2 *cp = P.P.force32 + 3 * m;
-                c0 = __ldg(cp);
-                c1 = __ldg(cp + 1);
-                c2 = __ldg(cp + 2);
-              }
-              const float fd = (c2.x * q + c1.x) * q + c0.x;
-              const float pd = (c2.y * q + c1.y) * q + c0.y;
-              const float fpair = -((u.w + nb.w) * fd + pd) * rinv;
-              two_sum(xs, xc, dx * fpair);
-              two_sum(ys, yc, dy * fpair);
-              two_sum(zs, zc, dz * fpair);
-              if (ENERGY) {
-                const float4 pv = __ldg(&P.P.phi_val32[m]);
-                two_sum(ps, pc, 0.5f * (((pv.w * q + pv.z) * q + pv.y) * q + pv.x));
-              }
-            }
-          }
-          const double fx = (double)xs + (double)xc, fy = (double)ys + (double)yc, fz = (double)zs + (double)zc;
-          const long long i = me.i;
-          d.fx[i] = (float)fx;
-          d.fy[i] = (float)fy;
-          d.fz[i] = (float)fz;
-          double vx = d.vx[i], vy = d.vy[i], vz = d.vz[i];
-          if (d.primed) {
-            vx += P.h * fx;
-            vy += P.h * fy;
-            vz += P.h * fz;
-          }
-          if (ENERGY) {
-            e_kin = 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E;
-            e_pair = (double)ps + (double)pc;
-          }
-          vx += P.h * fx;
-          vy += P.h * fy;
-          vz += P.h * fz;
-          const double nx = d.ux[i] + P.dt * vx, ny = d.uy[i] + P.dt * vy, nz = d.uz[i] + P.dt * vz;
-          d.vx[i] = vx;
-          d.vy[i] = vy;
-          d.vz[i] = vz;
-          d.ux[i] = nx;
-          d.uy[i] = ny;
-          d.uz[i] = nz;
-          const float4 nu = make_float4((float)nx, (float)ny, (float)nz, 0.f);
-          float4 *un = d.u4[d.cur ^ 1];
-          un[i] = nu;
-          const Geom g = lat_geom(d);
-          for_images(g, me.s, me.bcx, me.by, me.bz, [&](long long idx, double, double, double) { un[idx] = nu; });
-        }
+  Producer pr;
+  producer_start(P, T, pr);
+  if (warp == 0) {
+    producer_issue(P, T, pr);
+    producer_issue(P, T, pr);
+  }
+  for (int t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+    if (!tile_live(P, t)) {
+      if (ENERGY && threadIdx.x == 0) P.epart[2 * t + 1] = 0.0;
+      continue;
+    }
+    bounded_wait(P, &T.full[b], (T.fphase >> b) & 1u, 2);
+    T.fphase ^= 1u << b;
+    const LatDesc &d = P.lats[P.tile_lat[t]];
+    const SiteRef me = site_of(d, P.shape_dims[d.shape], P.shape_log[d.shape], P.tile_org[t], threadIdx.x);
+    const float4 *tile = reinterpret_cast<const float4 *>(T.buf[b]);
+    double e_pair = 0.0, e_kin = 0.0;
+    int code = -1;
+    double vx = 0, vy = 0, vz = 0, ux = 0, uy = 0, uz = 0;
+    if (me.valid) {
+      code = d.code[me.i];
+      // own-site master state, fetched early so its latency hides behind the pair loop
+      vx = d.vx[me.i];
+      vy = d.vy[me.i];
+      vz = d.vz[me.i];
+      ux = d.ux[me.i];
+      uy = d.uy[me.i];
+      uz = d.uz[me.i];
+    }
+    const bool work = me.valid && code >= 0 && !(code & MB_FLAG_ITL);
+    float2 fs0 = make_float2(0.f, 0.f), fc0 = fs0, fs1 = fs0, fc1 = fs0;
+    float zs0 = 0.f, zc0 = 0.f, ps0 = 0.f, pc0 = 0.f, zs1 = 0.f, zc1 = 0.f, ps1 = 0.f, pc1 = 0.f;
+    if (work) {
+      const float4 u = tile[me.o];
+      const int *soff = P.soff[d.shape][me.s];
+      const int n = P.n_st, nn = P.n_near;
+      const int s = me.s;
+      int k = 0;
+      for (; k + 1 < nn; k += 2) {
+        const float4 nb0 = tile[me.o + soff[k]], nb1 = tile[me.o + soff[k + 1]];
+        force_pair<ENERGY, true>(P, u, nb0, P.ck[s][k], s, k, s_fd, fs0, fc0, zs0, zc0, ps0, pc0);
+        force_pair<ENERGY, true>(P, u, nb1, P.ck[s][k + 1], s, k + 1, s_fd, fs1, fc1, zs1, zc1, ps1, pc1);
+      }
+      if (k < nn) {
+        force_pair<ENERGY, true>(P, u, tile[me.o + soff[k]], P.ck[s][k], s, k, s_fd, fs0, fc0, zs0, zc0, ps0, pc0);
+        k++;
+      }
+      for (; k + 1 < n; k += 2) {
+        const float4 nb0 = tile[me.o + soff[k]], nb1 = tile[me.o + soff[k + 1]];
+        force_pair<ENERGY, false>(P, u, nb0, P.ck[s][k], s, k, s_fd, fs0, fc0, zs0, zc0, ps0, pc0);
+        force_pair<ENERGY, false>(P, u, nb1, P.ck[s][k + 1], s, k + 1, s_fd, fs1, fc1, zs1, zc1, ps1, pc1);
+      }
+      if (k < n)
+        force_pair<ENERGY, false>(P, u, tile[me.o + soff[k]], P.ck[s][k], s, k, s_fd, fs0, fc0, zs0, zc0, ps0, pc0);
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&T.empty[b]);
+    if (warp == 0) producer_issue(P, T, pr);
+    if (work) {
+      const double fx = ((double)fs0.x + (double)fs1.x) + ((double)fc0.x + (double)fc1.x);
+      const double fy = ((double)fs0.y + (double)fs1.y) + ((double)fc0.y + (double)fc1.y);
+      const double fz = ((double)zs0 + (double)zs1) + ((double)zc0 + (double)zc1);
+      const long long i = me.i;
+      d.fx[i] = (float)fx;
+      d.fy[i] = (float)fy;
+      d.fz[i] = (float)fz;
+      if (d.primed) {
+        vx += P.h * fx;
+        vy += P.h * fy;
+        vz += P.h * fz;
       }
       if (ENERGY) {
-        const double t1 = block_sum(e_pair);
-        const double t2 = block_sum(e_kin);
-        if (threadIdx.x == 0) {
-          P.epart[2 * t] += t1;
-          P.epart[2 * t + 1] = t2;
-        }
+        e_kin = 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E;
+        e_pair = ((double)ps0 + (double)ps1) + ((double)pc0 + (double)pc1);
       }
-    } else if (ENERGY && threadIdx.x == 0) {
-      P.epart[2 * t + 1] = 0.0;
+      vx += P.h * fx;
+      vy += P.h * fy;
+      vz += P.h * fz;
+      const double nx = ux + P.dt * vx, ny = uy + P.dt * vy, nz = uz + P.dt * vz;
+      d.vx[i] = vx;
+      d.vy[i] = vy;
+      d.vz[i] = vz;
+      d.ux[i] = nx;
+      d.uy[i] = ny;
+      d.uz[i] = nz;
+      const float4 nu = make_float4((float)nx, (float)ny, (float)nz, 0.f);
+      float4 *un = d.u4[d.cur ^ 1];
+      un[i] = nu;
+      const Geom g = lat_geom(d);
+      for_images(g, me.s, me.bcx, me.by, me.bz, [&](long long idx, double, double, double) { un[idx] = nu; });
     }
-    __syncthreads();
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (ENERGY) {
+      const double t1 = block_sum(e_pair);
+      const double t2 = block_sum(e_kin);
+      if (threadIdx.x == 0) {
+        P.epart[2 * t] += t1;
+        P.epart[2 * t + 1] = t2;
+      }
+    }
     b ^= 1;
   }
 }
 
 // ------------------------------------------------------- interstitial items
-__device__ __forceinline__ void itl_mark_lattice(const EnsParams &P, const LatDesc &d) {
-  const int nold = min(d.flag_count[0], d.cap_flag);
-  for (int k = threadIdx.x; k < nold; k += blockDim.x) {
+// Sites flagged at the previous step of lattice d lose their flag (all CTAs share
+// the old list); the count this step will fill starts at zero.  Counts alternate
+// with the buffer parity: count[cur] is this step's list, count[cur ^ 1] the last.
+__device__ __forceinline__ void itl_clear_flags(const LatDesc &d) {
+  const int cur = d.cur;
+  const int nold = min(d.flag_count[cur ^ 1], d.cap_flag);
+  const int stride = gridDim.x * blockDim.x;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nold; k += stride) {
     const int idx = d.flag_list[k];
     d.code[idx] = (int8_t)(d.code[idx] & ~MB_FLAG_ITL);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) d.flag_count[0] = 0;
-  __syncthreads();
+  if (blockIdx.x == 0 && threadIdx.x == 0) d.flag_count[cur] = 0;
+}
+
+// Warp `w` of the grid flags the lattice sites within reach of interstitial w.
+__device__ __forceinline__ void itl_mark_one(const EnsParams &P, const LatDesc &d, int it) {
   const Geom g = lat_geom(d);
   const int lane = threadIdx.x & 31;
   const int cur = d.cur;
-  for (int it = threadIdx.x >> 5; it < d.n_itl; it += blockDim.x >> 5) {
-    const double qx = d.ipx[cur][it], qy = d.ipy[cur][it], qz = d.ipz[cur][it];
-    const Window w = make_window(qx, qy, qz, P.a0, P.reach);
-    const int ncand = w.nx * w.ny * w.nz;
-    for (int c = lane; c < ncand; c += 32) {
-      long long idx;
-      double sx, sy, sz;
-      if (!window_site(g, w, c, qx, qy, qz, P.a0, P.reach, idx, sx, sy, sz)) continue;
-      if (d.code[idx] < 0) continue;
-      const uintptr_t addr = (uintptr_t)(d.code + idx);
-      unsigned int *word = (unsigned int *)(addr & ~(uintptr_t)3);
-      const unsigned int bit = (unsigned int)MB_FLAG_ITL << (8 * (addr & 3));
-      const unsigned int old = atomicOr(word, bit);
-      if (!(old & bit)) {
-        const int slot = atomicAdd(&d.flag_count[0], 1);
-        if (slot < d.cap_flag)
-          d.flag_list[slot] = (int)idx;
-        else
-          d.flag_count[1] = 1;
-      }
+  const double qx = d.ipx[cur][it], qy = d.ipy[cur][it], qz = d.ipz[cur][it];
+  const Window w = make_window(qx, qy, qz, P.a0, P.reach);
+  const int ncand = w.nx * w.ny * w.nz;
+  for (int c = lane; c < ncand; c += 32) {
+    long long idx;
+    double sx, sy, sz;
+    if (!window_site(g, w, c, qx, qy, qz, P.a0, P.reach, idx, sx, sy, sz)) continue;
+    if (d.code[idx] < 0) continue;
+    const uintptr_t addr = (uintptr_t)(d.code + idx);
+    unsigned int *word = (unsigned int *)(addr & ~(uintptr_t)3);
+    const unsigned int bit = (unsigned int)MB_FLAG_ITL << (8 * (addr & 3));
+    const unsigned int old = atomicOr(word, bit);
+    if (!(old & bit)) {
+      const int slot = atomicAdd(&d.flag_count[cur], 1);
+      if (slot < d.cap_flag)
+        d.flag_list[slot] = (int)idx;
+      else
+        d.flag_count[2] = 1; // overflow: reported by the host
     }
   }
-  __syncthreads();
 }
 
 // Work of one warp on item w of lattice d: a flagged site (w < nflag) or an
@@ -473,7 +590,7 @@ __device__ void itl_items(const EnsParams &P) {
   for (int q = 0; q < P.n_itl_lats; q++) {
     const LatDesc &d = P.lats[P.itl_lats[q]];
     if (!lat_active(d)) continue;
-    const int nflag = min(d.flag_count[0], d.cap_flag);
+    const int nflag = min(d.flag_count[d.cur], d.cap_flag);
     const int n = nflag + d.n_itl;
     for (int w = gw; w < n; w += warps) itl_item<FORCE, ENERGY>(P, d, w, nflag);
   }
@@ -489,8 +606,9 @@ __global__ void __launch_bounds__(ENS_THREADS, 1) k_ens_step(const __grid_consta
   TileCtx T;
   T.buf[0] = smem + tab_bytes;
   T.buf[1] = smem + tab_bytes + ENS_TILE_MAX_BYTES;
-  T.bar = reinterpret_cast<uint64_t *>(smem + tab_bytes + 2 * ENS_TILE_MAX_BYTES);
-  T.phase = 0;
+  T.full = reinterpret_cast<uint64_t *>(smem + tab_bytes + 2 * ENS_TILE_MAX_BYTES);
+  T.empty = T.full + 2;
+  T.fphase = T.ephase = T.used = 0;
   for (int k = threadIdx.x; k < P.nsm; k += blockDim.x) {
     s_fv[k] = P.P.f_val32[P.m_lo + k];
     s_fd[3 * k + 0] = P.P.force32[3 * (P.m_lo + k) + 0];
@@ -498,22 +616,32 @@ __global__ void __launch_bounds__(ENS_THREADS, 1) k_ens_step(const __grid_consta
     s_fd[3 * k + 2] = P.P.force32[3 * (P.m_lo + k) + 2];
   }
   if (threadIdx.x == 0) {
-    mbar_init(&T.bar[0], 1);
-    mbar_init(&T.bar[1], 1);
+    mbar_init(&T.full[0], 1);
+    mbar_init(&T.full[1], 1);
+    mbar_init(&T.empty[0], ENS_CONSUMERS / 32);
+    mbar_init(&T.empty[1], ENS_CONSUMERS / 32);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
-  // A: interstitial flags (one CTA per lattice with interstitials)
+  // A: interstitial flags: clear the last step's, then flag this step's (all CTAs)
   if (P.n_itl_lats > 0) {
-    for (int q = blockIdx.x; q < P.n_itl_lats; q += gridDim.x) {
+    for (int q = 0; q < P.n_itl_lats; q++) {
       const LatDesc &d = P.lats[P.itl_lats[q]];
-      if (lat_active(d)) itl_mark_lattice(P, d);
+      if (lat_active(d)) itl_clear_flags(d);
+    }
+    if (!grid_sync(P.bar, P.err)) return;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    for (int q = 0; q < P.n_itl_lats; q++) {
+      const LatDesc &d = P.lats[P.itl_lats[q]];
+      if (!lat_active(d)) continue;
+      for (int it = gw; it < d.n_itl; it += warps) itl_mark_one(P, d, it);
     }
     if (!grid_sync(P.bar, P.err)) return;
   }
   // B: density over lattice tiles
-  rho_tiles<ENERGY>(P, T, s_fv, nullptr);
+  rho_tiles<ENERGY>(P, T, s_fv);
   if (!grid_sync(P.bar, P.err)) return;
   // C: density of flagged sites and interstitials
   if (P.n_itl_lats > 0) {
@@ -554,7 +682,7 @@ __global__ void k_ens_energy(const LatDesc *lats, int n_lats, const int *tile_fi
 
 size_t ens_smem_bytes(int nsm) {
   const size_t tab = ((size_t)nsm * (sizeof(float4) + 3 * sizeof(float2)) + 127) & ~(size_t)127;
-  return tab + 2 * ENS_TILE_MAX_BYTES + 2 * sizeof(uint64_t);
+  return tab + 2 * ENS_TILE_MAX_BYTES + 4 * sizeof(uint64_t);
 }
 
 int ens_launch(const EnsParams &P, int grid, cudaStream_t s) {

@@ -32,6 +32,7 @@
 
 namespace mb {
 
+#define ENS_CONSUMERS 512 // one site per thread per tile
 #define ENS_THREADS 512
 #define ENS_NSHAPE 4
 #define ENS_MAX_ST 112
@@ -64,20 +65,22 @@ struct LatDesc {
 };
 
 struct EnsParams {
-  int n_st;
+  int n_st;                            // stencil entries, ordered by ideal distance
+  int n_near;                          // entries whose ideal distance is inside the cutoff
   int soff[ENS_NSHAPE][2][ENS_MAX_ST]; // shared-memory offset (float4 units) of entry k, per shape / sublattice
   float4 ck[2][ENS_MAX_ST];            // ideal offset X_i - X_j (xyz) and its length (w)
-  int mk[2][ENS_MAX_ST];               // floor(|C_k| / dr)
-  float fk[2][ENS_MAX_ST];             // |C_k| / dr - mk
+  float2 kf[2][ENS_MAX_ST];            // {|C_k| / dr - floor(|C_k| / dr), floor(|C_k| / dr)}
   char4 sd[2][ENS_MAX_ST];             // target sublattice - own, dcx, dy, dz
   int shape_dims[ENS_NSHAPE][4];       // TX, TY, TZ, bytes
+  int shape_log[ENS_NSHAPE][4];        // log2 TX, log2 TY, log2 TZ, log2 (TX TY TZ)
   DevPot P;
   float rdr, rc2f;
   int m_lo, nsm;
   double h, dt, mass, a0, rc2, reach;
   const LatDesc *lats;
   int n_lats;
-  const int *tile_lat, *tile_idx;
+  const int *tile_lat;
+  const unsigned *tile_org; // tile origin: cx0 | y0 << 11 | z0 << 22 (box cells)
   int n_tiles;
   const CUtensorMap *tmaps; // [lattice][buffer]
   unsigned *bar;
