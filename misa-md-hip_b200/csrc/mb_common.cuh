@@ -80,10 +80,12 @@ struct Geom {
   int images;      // 1: sites write their periodic ghost images (device-resident mode)
   long long E;     // sites per sublattice array
   double Lx, Ly, Lz;
+  double iLx, iLy, iLz; // 1 / L (0 when there is no periodic box)
 };
 
 struct StencilSet {
   int n;                          // entries per parity (equal for both)
+  int n_near;                     // leading entries inside the cutoff at the ideal lattice (0: unknown)
   int off[2][MB_MAX_STENCIL];     // [sublattice] split-layout linear offsets
 };
 
@@ -96,6 +98,8 @@ int stencil_from_linear(const int64_t *even, size_t n_even, const int64_t *odd, 
 // ordered dz, dy, dx ascending), for an ext array of ext_x x ext_y.
 int stencil_generate(double a0, double reach, int ext_x, int ext_y, int64_t *even, int64_t *odd, int cap, int *n,
                      int *reach_x, int *reach_y, int *reach_z);
+int stencil_sort_by_distance(double a0, double cutoff, int ext_x, int ext_y, int64_t *even, int64_t *odd, int n,
+                             int *n_near);
 
 // ------------------------------------------------------ kernel arguments
 struct Lattice64 {

@@ -171,6 +171,6 @@ __device__ __forceinline__ bool window_site(const Geom &g, const Window &w, int 
   return true;
 }
 
-__device__ __forceinline__ double min_image(double d, double L) { return d - L * rint(d / L); }
+__device__ __forceinline__ double min_image(double d, double L, double iL) { return d - L * rint(d * iL); }
 
 } // namespace mb

@@ -507,7 +507,7 @@ __device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag)
   }
   for (int K = lane; K < d.n_itl; K += 32) {
     if (!is_site && K == it) continue;
-    pair(min_image(xi - d.ipx[cur][K], d.Lx), min_image(yi - d.ipy[cur][K], d.Ly), min_image(zi - d.ipz[cur][K], d.Lz),
+    pair(min_image(xi - d.ipx[cur][K], g.Lx, g.iLx), min_image(yi - d.ipy[cur][K], g.Ly, g.iLy), min_image(zi - d.ipz[cur][K], g.Lz, g.iLz),
          d.itype[K], FORCE ? d.idf[K] : 0.0);
   }
   if (!FORCE) {

@@ -185,6 +185,9 @@ __device__ __forceinline__ Geom lat_geom(const LatDesc &d) {
   g.Lx = d.Lx;
   g.Ly = d.Ly;
   g.Lz = d.Lz;
+  g.iLx = 1.0 / d.Lx;
+  g.iLy = 1.0 / d.Ly;
+  g.iLz = 1.0 / d.Lz;
   return g;
 }
 

@@ -2,8 +2,10 @@
 #include <math.h>
 #include <stdio.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "mb_common.cuh"
 
@@ -71,6 +73,7 @@ int stencil_from_linear(const int64_t *even, size_t n_even, const int64_t *odd, 
   if (n_even != n_odd) return fail(MB_ERR_ARG, "even and odd stencils must have the same length");
   if (n_even > MB_MAX_STENCIL) return fail(MB_ERR_ARG, "stencil longer than MB_MAX_STENCIL");
   out->n = (int)n_even;
+  out->n_near = 0;
   const long long plane = (long long)ext_x * ext_y;
   for (int s = 0; s < 2; s++) {
     const int64_t *src = parity_of_sublattice[s] ? odd : even;
@@ -91,6 +94,34 @@ int stencil_from_linear(const int64_t *even, size_t n_even, const int64_t *odd, 
       out->off[s][k] = (int)lin;
     }
   }
+  return MB_OK;
+}
+
+// Reorders both parities' doubled-x linear stencils by ideal distance (stable) and
+// returns how many lead entries lie inside `cutoff` (equal for both parities).
+int stencil_sort_by_distance(double a0, double cutoff, int ext_x, int ext_y, int64_t *even, int64_t *odd, int n,
+                             int *n_near) {
+  const long long plane = (long long)ext_x * ext_y;
+  int near[2] = {0, 0};
+  for (int par = 0; par < 2; par++) {
+    int64_t *src = par ? odd : even;
+    std::vector<std::pair<double, int64_t>> ord;
+    for (int k = 0; k < n; k++) {
+      const long long o = src[k];
+      const long long dz = round_div(o, plane), rem = o - dz * plane, dy = round_div(rem, ext_x),
+                      dx = rem - dy * ext_x;
+      const int npar = (int)((par + dx) & 1);
+      const double ox = 0.5 * dx, oy = dy + 0.5 * (npar - par), oz = dz + 0.5 * (npar - par);
+      const double R = a0 * sqrt(ox * ox + oy * oy + oz * oz);
+      ord.push_back({R, o});
+      if (R < cutoff) near[par]++;
+    }
+    std::stable_sort(ord.begin(), ord.end(), [](const std::pair<double, int64_t> &x,
+                                                 const std::pair<double, int64_t> &y) { return x.first < y.first; });
+    for (int k = 0; k < n; k++) src[k] = ord[k].second;
+  }
+  if (near[0] != near[1]) return fail(MB_ERR_STATE, "even and odd stencils differ inside the cutoff");
+  *n_near = near[0];
   return MB_OK;
 }
 

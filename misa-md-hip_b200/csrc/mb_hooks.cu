@@ -191,6 +191,7 @@ int mb_domain_init(const mb_device_domain *d) {
   g.images = 0; // the host owns the ghost region in drop-in mode
   g.E = (long long)g.ecx * g.ey * g.ez;
   g.Lx = g.Ly = g.Lz = 0.0;
+  g.iLx = g.iLy = g.iLz = 0.0;
   c.domain = true;
   // linear offsets are tied to the ext sizes they were made for: a new domain needs
   // mb_nei_offset_init again (the reference's init order: domain, then offsets)

@@ -47,6 +47,25 @@ struct RhoArgs {
   long long n_items;
 };
 
+// One density term of a one-type lattice.  BF (branch-free): the stencil entry lies
+// inside the cutoff at the ideal lattice, so nearly every lane needs the spline; the
+// value is masked instead of branched around, which lets iterations overlap.
+template <bool BF>
+__device__ __forceinline__ double rho_term(const RhoArgs &a, const Lattice64 &L, const double4 *s_fval, long long j,
+                                           double xi, double yi, double zi) {
+  const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  const bool in = d2 < a.rc2;
+  if (!BF && !in) return 0.0;
+  const double r = d2 * rsqrt(d2);
+  int m;
+  double p;
+  spl_locate(r, a.P.rdr, a.P.nr, m, p);
+  const double4 c = (m >= a.m_lo) ? s_fval[m - a.m_lo] : ldg4(&a.P.f_val[m]);
+  const double v = cubic(c, p);
+  return (BF && !in) ? 0.0 : v;
+}
+
 template <bool ENERGY, bool ONE_TYPE>
 __global__ void __launch_bounds__(MB_MAIN_THREADS, 1)
     k_rho64(const __grid_constant__ StencilSet st, const __grid_constant__ RhoArgs a) {
@@ -78,20 +97,28 @@ __global__ void __launch_bounds__(MB_MAIN_THREADS, 1)
     const double xi = L.px[i], yi = L.py[i], zi = L.pz[i];
     const int *off = st.off[s];
     double rho = 0.0;
+    if (ONE_TYPE) {
+      double r0 = 0.0, r1 = 0.0;
+      int k = 0;
+      for (; k + 1 < st.n_near; k += 2) {
+        r0 += rho_term<true>(a, L, s_fval, i + off[k], xi, yi, zi);
+        r1 += rho_term<true>(a, L, s_fval, i + off[k + 1], xi, yi, zi);
+      }
+      if (k < st.n_near) r0 += rho_term<true>(a, L, s_fval, i + off[k++], xi, yi, zi);
+#pragma unroll 2
+      for (; k < st.n; k++) r1 += rho_term<false>(a, L, s_fval, i + off[k], xi, yi, zi);
+      rho = r0 + r1;
+    } else {
 #pragma unroll 4
-    for (int k = 0; k < st.n; k++) {
-      const long long j = i + off[k];
-      const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
-      const double d2 = dx * dx + dy * dy + dz * dz;
-      if (d2 < a.rc2) {
-        const double r = d2 * rsqrt(d2);
-        int m;
-        double p;
-        spl_locate(r, P.rdr, P.nr, m, p);
-        if (ONE_TYPE) {
-          const double4 c = (m >= a.m_lo) ? s_fval[m - a.m_lo] : ldg4(&P.f_val[m]);
-          rho += cubic(c, p);
-        } else {
+      for (int k = 0; k < st.n; k++) {
+        const long long j = i + off[k];
+        const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < a.rc2) {
+          const double r = d2 * rsqrt(d2);
+          int m;
+          double p;
+          spl_locate(r, P.rdr, P.nr, m, p);
           const int tj = L.code[j] & 0x3F;
           rho += cubic(ldg4(&P.f_val[(size_t)tj * P.nr + m]), p);
         }
@@ -122,6 +149,46 @@ struct ForceArgs {
   int chunks;
   long long n_items;
 };
+
+// One force term of a one-type lattice (see rho_term for BF).
+template <bool ENERGY, bool BF>
+__device__ __forceinline__ void force_term(const ForceArgs &a, const Lattice64 &L, const double2 *s_f1, long long j,
+                                           double xi, double yi, double zi, double dfi, double &fx, double &fy,
+                                           double &fz, double &ep) {
+  const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  const bool in = d2 < a.sp.rc2;
+  if (!BF && !in) return;
+  const double rinv = rsqrt(d2);
+  const double r = d2 * rinv;
+  const double dfj = L.df[j];
+  int m;
+  double p;
+  spl_locate(r, a.P.rdr, a.P.nr, m, p);
+  double2 c0, c1, c2;
+  if (m >= a.m_lo) {
+    const double2 *q = s_f1 + (size_t)(m - a.m_lo) * 3;
+    c0 = q[0];
+    c1 = q[1];
+    c2 = q[2];
+  } else {
+    const double2 *q = a.P.force1 + (size_t)m * 3;
+    c0 = __ldg(q);
+    c1 = __ldg(q + 1);
+    c2 = __ldg(q + 2);
+  }
+  const double fp = (c2.x * p + c1.x) * p + c0.x;
+  const double pp = (c2.y * p + c1.y) * p + c0.y;
+  double fpair = -((dfi + dfj) * fp + pp) * rinv;
+  if (BF && !in) fpair = 0.0;
+  fx += dx * fpair;
+  fy += dy * fpair;
+  fz += dz * fpair;
+  if (ENERGY) {
+    const double e = 0.5 * cubic(ldg4(&a.P.phi_val[m]), p);
+    ep += (BF && !in) ? 0.0 : e;
+  }
+}
 
 template <bool ENERGY, bool ONE_TYPE>
 __global__ void __launch_bounds__(MB_MAIN_THREADS, 1)
@@ -157,46 +224,39 @@ __global__ void __launch_bounds__(MB_MAIN_THREADS, 1)
     const double dfi = L.df[i];
     const int *off = st.off[s];
     double fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
+    if (ONE_TYPE) {
+      double gx = 0.0, gy = 0.0, gz = 0.0, eq = 0.0;
+      int k = 0;
+      for (; k + 1 < st.n_near; k += 2) {
+        force_term<ENERGY, true>(a, L, s_f1, i + off[k], xi, yi, zi, dfi, fx, fy, fz, ep);
+        force_term<ENERGY, true>(a, L, s_f1, i + off[k + 1], xi, yi, zi, dfi, gx, gy, gz, eq);
+      }
+      if (k < st.n_near) force_term<ENERGY, true>(a, L, s_f1, i + off[k++], xi, yi, zi, dfi, fx, fy, fz, ep);
+#pragma unroll 2
+      for (; k < st.n; k++) force_term<ENERGY, false>(a, L, s_f1, i + off[k], xi, yi, zi, dfi, gx, gy, gz, eq);
+      fx += gx;
+      fy += gy;
+      fz += gz;
+      ep += eq;
+    } else {
 #pragma unroll 4
-    for (int k = 0; k < st.n; k++) {
-      const long long j = i + off[k];
-      const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
-      const double d2 = dx * dx + dy * dy + dz * dz;
-      if (d2 < sp.rc2) {
-        const double rinv = rsqrt(d2);
-        const double r = d2 * rinv;
-        const double dfj = L.df[j];
-        double psip;
-        if (ONE_TYPE) {
-          int m;
-          double p;
-          spl_locate(r, P.rdr, P.nr, m, p);
-          double2 c0, c1, c2;
-          if (m >= a.m_lo) {
-            const double2 *q = s_f1 + (size_t)(m - a.m_lo) * 3;
-            c0 = q[0];
-            c1 = q[1];
-            c2 = q[2];
-          } else {
-            const double2 *q = P.force1 + (size_t)m * 3;
-            c0 = __ldg(q);
-            c1 = __ldg(q + 1);
-            c2 = __ldg(q + 2);
-          }
-          const double fp = (c2.x * p + c1.x) * p + c0.x;
-          const double pp = (c2.y * p + c1.y) * p + c0.y;
-          psip = (dfi + dfj) * fp + pp;
-          if (ENERGY) ep += 0.5 * cubic(ldg4(&P.phi_val[m]), p);
-        } else {
+      for (int k = 0; k < st.n; k++) {
+        const long long j = i + off[k];
+        const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < sp.rc2) {
+          const double rinv = rsqrt(d2);
+          const double r = d2 * rinv;
+          const double dfj = L.df[j];
           const int tj = L.code[j] & 0x3F;
           double ph = 0.0;
-          psip = pair_psip(P, ti, tj, r, dfi, dfj, ENERGY ? &ph : nullptr);
+          const double psip = pair_psip(P, ti, tj, r, dfi, dfj, ENERGY ? &ph : nullptr);
           if (ENERGY) ep += 0.5 * ph;
+          const double fpair = -psip * rinv;
+          fx += dx * fpair;
+          fy += dy * fpair;
+          fz += dz * fpair;
         }
-        const double fpair = -psip * rinv;
-        fx += dx * fpair;
-        fy += dy * fpair;
-        fz += dz * fpair;
       }
     }
     if (L.fx) {
@@ -338,37 +398,39 @@ int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const
 // seen from both sides as long as no lattice atom strays more than
 // (reach - cutoff) from its site.
 
-__global__ void __launch_bounds__(1024) k_itl_mark(const Geom g, const Lattice64 L, const Itl64 I) {
-  // clear last step's flags
+// Last step's flags come off (grid-stride over the old list) ...
+__global__ void k_itl_clear(const Lattice64 L, const Itl64 I) {
   const int nold = min(I.flag_count[0], I.cap_flag);
-  for (int k = threadIdx.x; k < nold; k += blockDim.x) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nold; k += gridDim.x * blockDim.x) {
     const int idx = I.flag_list[k];
     L.code[idx] = (int8_t)(L.code[idx] & ~MB_FLAG_ITL);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) I.flag_count[0] = 0;
-  __syncthreads();
+}
+
+// ... then one warp per interstitial flags the sites within reach (the count was
+// reset in between).
+__global__ void k_itl_mark(const Geom g, const Lattice64 L, const Itl64 I) {
   const int lane = threadIdx.x & 31;
-  for (int it = threadIdx.x >> 5; it < I.n; it += blockDim.x >> 5) {
-    const double qx = I.px[it], qy = I.py[it], qz = I.pz[it];
-    const Window w = make_window(qx, qy, qz, I.a0, I.reach);
-    const int ncand = w.nx * w.ny * w.nz;
-    for (int c = lane; c < ncand; c += 32) {
-      long long idx;
-      double sx, sy, sz;
-      if (!window_site(g, w, c, qx, qy, qz, I.a0, I.reach, idx, sx, sy, sz)) continue;
-      if (L.code[idx] < 0) continue;
-      const uintptr_t addr = (uintptr_t)(L.code + idx);
-      unsigned int *word = (unsigned int *)(addr & ~(uintptr_t)3);
-      const unsigned int bit = (unsigned int)MB_FLAG_ITL << (8 * (addr & 3));
-      const unsigned int old = atomicOr(word, bit);
-      if (!(old & bit)) {
-        const int slot = atomicAdd(&I.flag_count[0], 1);
-        if (slot < I.cap_flag)
-          I.flag_list[slot] = (int)idx;
-        else
-          I.flag_count[1] = 1; // overflow: reported by the host
-      }
+  const int it = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  if (it >= I.n) return;
+  const double qx = I.px[it], qy = I.py[it], qz = I.pz[it];
+  const Window w = make_window(qx, qy, qz, I.a0, I.reach);
+  const int ncand = w.nx * w.ny * w.nz;
+  for (int c = lane; c < ncand; c += 32) {
+    long long idx;
+    double sx, sy, sz;
+    if (!window_site(g, w, c, qx, qy, qz, I.a0, I.reach, idx, sx, sy, sz)) continue;
+    if (L.code[idx] < 0) continue;
+    const uintptr_t addr = (uintptr_t)(L.code + idx);
+    unsigned int *word = (unsigned int *)(addr & ~(uintptr_t)3);
+    const unsigned int bit = (unsigned int)MB_FLAG_ITL << (8 * (addr & 3));
+    const unsigned int old = atomicOr(word, bit);
+    if (!(old & bit)) {
+      const int slot = atomicAdd(&I.flag_count[0], 1);
+      if (slot < I.cap_flag)
+        I.flag_list[slot] = (int)idx;
+      else
+        I.flag_count[1] = 1; // overflow: reported by the host
     }
   }
 }
@@ -397,8 +459,8 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
         if (d2 < rc2) rho += rho_of_r(P, L.code[j] & 0x3F, d2 * rsqrt(d2));
       }
       for (int K = lane; K < I.n; K += 32) {
-        const double dx = min_image(xi - I.px[K], g.Lx), dy = min_image(yi - I.py[K], g.Ly),
-                     dz = min_image(zi - I.pz[K], g.Lz);
+        const double dx = min_image(xi - I.px[K], g.Lx, g.iLx), dy = min_image(yi - I.py[K], g.Ly, g.iLy),
+                     dz = min_image(zi - I.pz[K], g.Lz, g.iLz);
         const double d2 = dx * dx + dy * dy + dz * dz;
         if (d2 < rc2) rho += rho_of_r(P, I.type[K], d2 * rsqrt(d2));
       }
@@ -428,8 +490,8 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
       }
       for (int K = lane; K < I.n; K += 32) {
         if (K == it) continue;
-        const double dx = min_image(qx - I.px[K], g.Lx), dy = min_image(qy - I.py[K], g.Ly),
-                     dz = min_image(qz - I.pz[K], g.Lz);
+        const double dx = min_image(qx - I.px[K], g.Lx, g.iLx), dy = min_image(qy - I.py[K], g.Ly, g.iLy),
+                     dz = min_image(qz - I.pz[K], g.Lz, g.iLz);
         const double d2 = dx * dx + dy * dy + dz * dz;
         if (d2 < rc2) rho += rho_of_r(P, I.type[K], d2 * rsqrt(d2));
       }
@@ -512,7 +574,7 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
     }
     for (int K = lane; K < I.n; K += 32) {
       if (!is_site && K == it) continue;
-      add_pair(min_image(xi - I.px[K], g.Lx), min_image(yi - I.py[K], g.Ly), min_image(zi - I.pz[K], g.Lz),
+      add_pair(min_image(xi - I.px[K], g.Lx, g.iLx), min_image(yi - I.py[K], g.Ly, g.iLy), min_image(zi - I.pz[K], g.Lz, g.iLz),
                I.type[K], I.df[K]);
     }
     fx = warp_sum(fx);
@@ -579,7 +641,12 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
 }
 
 int launch_itl_mark64(const Geom &g, const Lattice64 &L, const Itl64 &I, cudaStream_t s) {
-  k_itl_mark<<<1, 1024, 0, s>>>(g, L, I);
+  int grid = (I.cap_flag + 255) / 256;
+  if (grid > 4 * device_sm_count()) grid = 4 * device_sm_count();
+  k_itl_clear<<<grid, 256, 0, s>>>(L, I);
+  MB_CUDA(cudaGetLastError());
+  MB_CUDA(cudaMemsetAsync(I.flag_count, 0, sizeof(int), s));
+  k_itl_mark<<<(I.n * 32 + 255) / 256, 256, 0, s>>>(g, L, I);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }

@@ -340,6 +340,9 @@ int mb_sim_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **o
   g.Lx = cfg->cells_x * cfg->lattice_const;
   g.Ly = cfg->cells_y * cfg->lattice_const;
   g.Lz = cfg->cells_z * cfg->lattice_const;
+  g.iLx = 1.0 / g.Lx;
+  g.iLy = 1.0 / g.Ly;
+  g.iLz = 1.0 / g.Lz;
   if (2 * g.E > 0x3fffffffLL) {
     pot_free(s->pot);
     delete s;
@@ -352,7 +355,11 @@ int mb_sim_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **o
   s->n_box = 2LL * g.bcx * g.by * g.bz;
   rc = stencil_generate(cfg->lattice_const, reach, s->ext_x, s->ext_y, even, odd, MB_MAX_STENCIL, &n, &rx, &ry, &rz);
   const int par[2] = {0, 1};
+  int n_near = 0;
+  if (rc == MB_OK && pot->n_types == 1)
+    rc = stencil_sort_by_distance(cfg->lattice_const, cfg->cutoff, s->ext_x, s->ext_y, even, odd, n, &n_near);
   if (rc == MB_OK) rc = stencil_from_linear(even, n, odd, n, s->ext_x, s->ext_y, g, par, &s->st);
+  s->st.n_near = n_near;
   if (rc != MB_OK) {
     pot_free(s->pot);
     delete s;
