@@ -29,7 +29,8 @@
 namespace mb {
 
 #define MB_EPART_CAP 4096 // CTA partial sums per energy region
-#define MB_MAIN_THREADS 512
+#define MB_RHO_THREADS 1024  // 52 registers: a full SM of warps
+#define MB_FORCE_THREADS 768 // up to 85 registers
 #define MB_ITL_THREADS 256
 
 int energy_partials_needed() { return 8 * MB_EPART_CAP; }
@@ -67,7 +68,7 @@ __device__ __forceinline__ double rho_term(const RhoArgs &a, const Lattice64 &L,
 }
 
 template <bool ENERGY, bool ONE_TYPE>
-__global__ void __launch_bounds__(MB_MAIN_THREADS, 1)
+__global__ void __launch_bounds__(MB_RHO_THREADS, 1)
     k_rho64(const __grid_constant__ StencilSet st, const __grid_constant__ RhoArgs a) {
   extern __shared__ double4 s_fval[];
   const DevPot &P = a.P;
@@ -191,7 +192,7 @@ __device__ __forceinline__ void force_term(const ForceArgs &a, const Lattice64 &
 }
 
 template <bool ENERGY, bool ONE_TYPE>
-__global__ void __launch_bounds__(MB_MAIN_THREADS, 1)
+__global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
     k_force64(const __grid_constant__ StencilSet st, const __grid_constant__ ForceArgs a) {
   extern __shared__ double2 s_f1[]; // [knot][3]
   const DevPot &P = a.P;
@@ -311,6 +312,18 @@ static int grid_for(long long warps_needed, int threads) {
 
 static const int kSmemCap = 200 * 1024;
 
+// Knots kept in shared memory: those at r >= 0.3 cutoff (lattice neighbours sit near
+// 0.45 cutoff and beyond; closer pairs read the global table), within kSmemCap, so
+// the rest of the SM's on-chip memory stays L1 for the neighbour rows.
+static int smem_knots(const DevPot &pot, int bytes_per_knot) {
+  int lo = (int)(0.3 * pot.cutoff * pot.rdr);
+  if (lo < 0) lo = 0;
+  if (lo > pot.nr - 2) lo = pot.nr - 2;
+  int n = pot.nr - lo;
+  if (n * bytes_per_knot > kSmemCap) n = kSmemCap / bytes_per_knot;
+  return n;
+}
+
 int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, double rc2,
                  double *e_partial, int energy, int skip_flagged, cudaStream_t s) {
   RhoArgs a;
@@ -321,14 +334,13 @@ int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const L
   a.e_partial = e_partial;
   a.skip_flagged = skip_flagged;
   const bool one = pot.n_types == 1;
-  int nsm = pot.nr;
-  if (nsm * (int)sizeof(double4) > kSmemCap) nsm = kSmemCap / (int)sizeof(double4);
+  int nsm = smem_knots(pot, (int)sizeof(double4));
   if (!one) nsm = 0;
   a.m_lo = pot.nr - nsm;
   a.chunks = (g.bcx + 31) / 32;
   a.n_items = (long long)a.chunks * g.by * 2 * g.bz;
   const size_t smem = (size_t)nsm * sizeof(double4);
-  const int grid = grid_for(a.n_items, MB_MAIN_THREADS);
+  const int grid = grid_for(a.n_items, MB_RHO_THREADS);
   static bool attr_done = false;
   if (!attr_done) {
     MB_CUDA(cudaFuncSetAttribute(k_rho64<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap));
@@ -337,14 +349,14 @@ int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const L
   }
   if (one) {
     if (energy)
-      k_rho64<true, true><<<grid, MB_MAIN_THREADS, smem, s>>>(st, a);
+      k_rho64<true, true><<<grid, MB_RHO_THREADS, smem, s>>>(st, a);
     else
-      k_rho64<false, true><<<grid, MB_MAIN_THREADS, smem, s>>>(st, a);
+      k_rho64<false, true><<<grid, MB_RHO_THREADS, smem, s>>>(st, a);
   } else {
     if (energy)
-      k_rho64<true, false><<<grid, MB_MAIN_THREADS, 0, s>>>(st, a);
+      k_rho64<true, false><<<grid, MB_RHO_THREADS, 0, s>>>(st, a);
     else
-      k_rho64<false, false><<<grid, MB_MAIN_THREADS, 0, s>>>(st, a);
+      k_rho64<false, false><<<grid, MB_RHO_THREADS, 0, s>>>(st, a);
   }
   MB_CUDA(cudaGetLastError());
   return MB_OK;
@@ -361,14 +373,13 @@ int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const
   a.e_kin = e_partial ? e_partial + 2 * MB_EPART_CAP : nullptr;
   a.skip_flagged = skip_flagged;
   const bool one = pot.n_types == 1;
-  int nsm = pot.nr;
-  if (nsm * (int)(3 * sizeof(double2)) > kSmemCap) nsm = kSmemCap / (int)(3 * sizeof(double2));
+  int nsm = smem_knots(pot, (int)(3 * sizeof(double2)));
   if (!one) nsm = 0;
   a.m_lo = pot.nr - nsm;
   a.chunks = (g.bcx + 31) / 32;
   a.n_items = (long long)a.chunks * g.by * 2 * g.bz;
   const size_t smem = (size_t)nsm * 3 * sizeof(double2);
-  const int grid = grid_for(a.n_items, MB_MAIN_THREADS);
+  const int grid = grid_for(a.n_items, MB_FORCE_THREADS);
   static bool attr_done = false;
   if (!attr_done) {
     MB_CUDA(cudaFuncSetAttribute(k_force64<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap));
@@ -377,14 +388,14 @@ int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const
   }
   if (one) {
     if (energy)
-      k_force64<true, true><<<grid, MB_MAIN_THREADS, smem, s>>>(st, a);
+      k_force64<true, true><<<grid, MB_FORCE_THREADS, smem, s>>>(st, a);
     else
-      k_force64<false, true><<<grid, MB_MAIN_THREADS, smem, s>>>(st, a);
+      k_force64<false, true><<<grid, MB_FORCE_THREADS, smem, s>>>(st, a);
   } else {
     if (energy)
-      k_force64<true, false><<<grid, MB_MAIN_THREADS, 0, s>>>(st, a);
+      k_force64<true, false><<<grid, MB_FORCE_THREADS, 0, s>>>(st, a);
     else
-      k_force64<false, false><<<grid, MB_MAIN_THREADS, 0, s>>>(st, a);
+      k_force64<false, false><<<grid, MB_FORCE_THREADS, 0, s>>>(st, a);
   }
   MB_CUDA(cudaGetLastError());
   return MB_OK;
