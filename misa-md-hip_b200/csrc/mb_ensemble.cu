@@ -190,6 +190,19 @@ __device__ void rho_tiles(const EnsParams &P, TileCtx &T, const float4 *s_fv) {
       const int n = P.n_st, nn = P.n_near;
       const int s = me.s;
       int k = 0;
+      float rs2 = 0.f, rc2 = 0.f, rs3 = 0.f, rc3 = 0.f;
+      for (; k + 3 < nn; k += 4) {
+        const float4 nb0 = tile[me.o + soff[k]], nb1 = tile[me.o + soff[k + 1]];
+        const float4 nb2 = tile[me.o + soff[k + 2]], nb3 = tile[me.o + soff[k + 3]];
+        rho_pair<true>(P, u, nb0, P.ck[s][k], s, k, s_fv, rs0, rc0);
+        rho_pair<true>(P, u, nb1, P.ck[s][k + 1], s, k + 1, s_fv, rs1, rc1);
+        rho_pair<true>(P, u, nb2, P.ck[s][k + 2], s, k + 2, s_fv, rs2, rc2);
+        rho_pair<true>(P, u, nb3, P.ck[s][k + 3], s, k + 3, s_fv, rs3, rc3);
+      }
+      two_sum(rs0, rc0, rs2);
+      two_sum(rs1, rc1, rs3);
+      rc0 += rc2;
+      rc1 += rc3;
       for (; k + 1 < nn; k += 2) {
         const float4 nb0 = tile[me.o + soff[k]], nb1 = tile[me.o + soff[k + 1]];
         rho_pair<true>(P, u, nb0, P.ck[s][k], s, k, s_fv, rs0, rc0);
@@ -326,6 +339,30 @@ __device__ void force_tiles(const EnsParams &P, TileCtx &T, const float2 *s_fd) 
       const int n = P.n_st, nn = P.n_near;
       const int s = me.s;
       int k = 0;
+      {
+        float2 fs2 = make_float2(0.f, 0.f), fc2 = fs2, fs3 = fs2, fc3 = fs2;
+        float zs2 = 0.f, zc2 = 0.f, ps2 = 0.f, pc2 = 0.f, zs3 = 0.f, zc3 = 0.f, ps3 = 0.f, pc3 = 0.f;
+        for (; k + 3 < nn; k += 4) {
+          const float4 nb0 = tile[me.o + soff[k]], nb1 = tile[me.o + soff[k + 1]];
+          const float4 nb2 = tile[me.o + soff[k + 2]], nb3 = tile[me.o + soff[k + 3]];
+          force_pair<ENERGY, true>(P, u, nb0, P.ck[s][k], s, k, s_fd, fs0, fc0, zs0, zc0, ps0, pc0);
+          force_pair<ENERGY, true>(P, u, nb1, P.ck[s][k + 1], s, k + 1, s_fd, fs1, fc1, zs1, zc1, ps1, pc1);
+          force_pair<ENERGY, true>(P, u, nb2, P.ck[s][k + 2], s, k + 2, s_fd, fs2, fc2, zs2, zc2, ps2, pc2);
+          force_pair<ENERGY, true>(P, u, nb3, P.ck[s][k + 3], s, k + 3, s_fd, fs3, fc3, zs3, zc3, ps3, pc3);
+        }
+        two_sum2(fs0, fc0, fs2);
+        two_sum2(fs1, fc1, fs3);
+        fc0 = __fadd2_rn(fc0, fc2);
+        fc1 = __fadd2_rn(fc1, fc3);
+        two_sum(zs0, zc0, zs2);
+        two_sum(zs1, zc1, zs3);
+        zc0 += zc2;
+        zc1 += zc3;
+        two_sum(ps0, pc0, ps2);
+        two_sum(ps1, pc1, ps3);
+        pc0 += pc2;
+        pc1 += pc3;
+      }
       for (; k + 1 < nn; k += 2) {
         const float4 nb0 = tile[me.o + soff[k]], nb1 = tile[me.o + soff[k + 1]];
         force_pair<ENERGY, true>(P, u, nb0, P.ck[s][k], s, k, s_fd, fs0, fc0, zs0, zc0, ps0, pc0);
