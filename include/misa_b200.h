@@ -251,6 +251,11 @@ int mb_ensemble_set_policy(mb_ensemble *e, int32_t policy);
 int mb_ensemble_autotune(mb_ensemble *e, int32_t steps, int32_t *policy, float *best_ms);
 int mb_ensemble_info(mb_ensemble *e, int64_t *n_sites, int64_t *n_tiles, int64_t *device_bytes, int32_t *n_slots);
 int mb_ensemble_set_graphs(mb_ensemble *e, int enable);
+/* Kernel structure: 0 (default) runs a single lattice of >= 2^19 sites as separate
+ * density and force kernels (higher occupancy) and everything else with the
+ * persistent one-launch-per-step kernel; 1 always persistent; 2 always split (one
+ * lattice only). */
+int mb_ensemble_set_mode(mb_ensemble *e, int32_t mode);
 
 #ifdef __cplusplus
 }

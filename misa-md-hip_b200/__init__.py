@@ -270,3 +270,7 @@ class Ensemble:
 
     def set_graphs(self, enable: bool) -> None:
         check(lib().mb_ensemble_set_graphs(self._h, int(enable)))
+
+    def set_mode(self, mode: int) -> None:
+        """0: split kernels for one large lattice (default), 1: persistent, 2: split."""
+        check(lib().mb_ensemble_set_mode(self._h, mode))

@@ -124,6 +124,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_ensemble_autotune": (_I, [_P, C.c_int32, C.POINTER(C.c_int32), _PF]),
     "mb_ensemble_info": (_I, [_P, _PI64, _PI64, _PI64, C.POINTER(C.c_int32)]),
     "mb_ensemble_set_graphs": (_I, [_P, _I]),
+    "mb_ensemble_set_mode": (_I, [_P, C.c_int32]),
 }
 
 

@@ -20,6 +20,12 @@ int ens_launch(const EnsParams &P, int grid, cudaStream_t s);
 int ens_max_grid(int nsm);
 int ens_energy_launch(const LatDesc *lats, int n, const int *tile_first, const double *epart, double *out,
                       cudaStream_t s);
+int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s);
+int mx_energy_launch(const LatDesc *lats, int lat, const double *epart, double *out, cudaStream_t s);
+int mx_grid();
+
+// Split mode (separate rho / force kernels) pays off for one large lattice.
+static const long long kSplitMinSites = 1LL << 19;
 
 static const int kShapes[ENS_NSHAPE][3] = {{16, 4, 4}, {8, 8, 4}, {8, 4, 8}, {4, 8, 8}};
 
@@ -183,6 +189,9 @@ struct mb_ensemble {
   cudaGraphExec_t graph = nullptr;
   bool graphs_ok = true;
   int policy = -1; // -1: size model per lattice; 0..3: one shape for all
+  int mode = 0;    // 0: split kernels for a single large lattice, else persistent; 1: persistent; 2: split
+  bool split = false;
+  mb::MxStencil mxs{};
   size_t device_bytes = 0;
   size_t fixed_bytes = 0;
   long long launches = 0;
@@ -437,6 +446,20 @@ static int rebuild(mb_ensemble *e) {
   P.bar = e->d_bar;
   P.err = e->d_err;
   e->grid = std::max(1, std::min(e->max_grid, e->n_tiles));
+  // split mode: one lattice, big enough for separate full-occupancy kernels
+  e->split = false;
+  if (nl == 1) {
+    const LatDesc &d = descs[0];
+    const long long sites = 2LL * d.bcx * d.by * d.bz;
+    e->split = e->mode == 2 || (e->mode == 0 && sites >= kSplitMinSites);
+    if (e->split && e->cap_tiles < (size_t)mx_grid()) e->split = false; // one energy partial per CTA
+    if (e->split)
+      for (int s = 0; s < 2; s++)
+        for (int k = 0; k < P.n_st; k++) {
+          const char4 q = P.sd[s][k];
+          e->mxs.off[s][k] = (int)((long long)q.x * d.E + ((long long)q.w * d.ey + q.z) * d.ecx + q.y);
+        }
+  }
   e->dirty = false;
   return MB_OK;
 }
@@ -463,9 +486,14 @@ static int launch_step(mb_ensemble *e, int energy) {
   if (energy) {
     MB_CUDA(cudaMemsetAsync(e->d_eitl, 0, sizeof(double) * 2 * e->order.size(), e->stream));
     P.energy = 1;
-    MB_TRY(ens_launch(P, e->grid, e->stream));
+    if (e->split) {
+      MB_TRY(mx_launch_step(P, e->mxs, 0, 1, e->stream));
+      MB_TRY(mx_energy_launch(e->d_lats, 0, e->d_epart, e->d_eout, e->stream));
+    } else {
+      MB_TRY(ens_launch(P, e->grid, e->stream));
+      MB_TRY(ens_energy_launch(e->d_lats, (int)e->order.size(), e->d_tile_first, e->d_epart, e->d_eout, e->stream));
+    }
     P.energy = 0;
-    MB_TRY(ens_energy_launch(e->d_lats, (int)e->order.size(), e->d_tile_first, e->d_epart, e->d_eout, e->stream));
     e->launches++;
     return MB_OK;
   }
@@ -475,7 +503,7 @@ static int launch_step(mb_ensemble *e, int energy) {
       cudaGraph_t g = nullptr;
       cudaError_t r = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
       if (r == cudaSuccess) {
-        const int rc = ens_launch(P, e->grid, e->stream);
+        const int rc = e->split ? mx_launch_step(P, e->mxs, 0, 0, e->stream) : ens_launch(P, e->grid, e->stream);
         r = cudaStreamEndCapture(e->stream, &g);
         if (rc == MB_OK && r == cudaSuccess && g) {
           if (cudaGraphInstantiate(&e->graph, g, 0) != cudaSuccess) e->graph = nullptr;
@@ -491,7 +519,10 @@ static int launch_step(mb_ensemble *e, int energy) {
       return MB_OK;
     }
   }
-  MB_TRY(ens_launch(P, e->grid, e->stream));
+  if (e->split)
+    MB_TRY(mx_launch_step(P, e->mxs, 0, 0, e->stream));
+  else
+    MB_TRY(ens_launch(P, e->grid, e->stream));
   e->launches++;
   return MB_OK;
 }
@@ -1073,6 +1104,15 @@ int mb_ensemble_info(mb_ensemble *e, int64_t *n_sites, int64_t *n_tiles, int64_t
   if (n_tiles) *n_tiles = e->n_tiles;
   if (device_bytes) *device_bytes = (int64_t)e->device_bytes;
   if (n_slots) *n_slots = used;
+  return MB_OK;
+}
+
+int mb_ensemble_set_mode(mb_ensemble *e, int32_t mode) {
+  if (!e || mode < 0 || mode > 2) return fail(MB_ERR_ARG, "mode must be 0 (auto), 1 (persistent) or 2 (split)");
+  std::lock_guard<std::mutex> lk(e->mu);
+  MB_TRY(sync_desc(e));
+  e->mode = mode;
+  e->dirty = true;
   return MB_OK;
 }
 

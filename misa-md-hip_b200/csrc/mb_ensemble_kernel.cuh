@@ -91,6 +91,11 @@ struct EnsParams {
   int energy;
 };
 
+// Split mode: per-lattice linear neighbour offsets in the ghost-extended arrays.
+struct MxStencil {
+  int off[2][ENS_MAX_ST];
+};
+
 // ------------------------------------------------------------ primitives
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
   unsigned v;

@@ -1,0 +1,322 @@
+// Per-pair FP32 arithmetic and interstitial items of the mixed-precision step,
+// shared by the persistent tile kernel (mb_ensemble.cu) and the split kernels of
+// single large lattices (mb_ensemble_split.cu).
+#pragma once
+
+#include "mb_ensemble_kernel.cuh"
+
+namespace mb {
+
+// Spline knot and local coordinate of a pair from its deviation eps = r - R_k.
+__device__ __forceinline__ void knot_of(const EnsParams &P, int s, int k, float eps, int &m, float &q) {
+  const float2 kf = P.kf[s][k];
+  const float t = kf.x + eps * P.rdr;
+  const float fl = floorf(t);
+  q = t - fl;
+  m = min(max((int)(kf.y + fl), 0), P.P.nr - 2);
+}
+
+// Pair geometry shared by both passes (x and y in f32x2 lanes): returns false
+// beyond the cutoff; on success r2 and the spline deviation numerator are set.
+struct PairGeo {
+  float2 dxy;
+  float dz, r2, num;
+};
+
+// ALWAYS: also compute the numerator beyond the cutoff (branch-free walking).
+template <bool ALWAYS>
+__device__ __forceinline__ bool pair_geo(const EnsParams &P, const float4 &u, const float4 &nb, const float4 &C,
+                                         PairGeo &g) {
+  const float2 m1 = make_float2(-1.f, -1.f);
+  const float2 exy = __ffma2_rn(make_float2(nb.x, nb.y), m1, make_float2(u.x, u.y)); // u - nb
+  const float ez = u.z - nb.z;
+  g.dxy = __fadd2_rn(make_float2(C.x, C.y), exy);
+  g.dz = C.z + ez;
+  const float2 sq = __fmul2_rn(g.dxy, g.dxy);
+  g.r2 = sq.x + sq.y + g.dz * g.dz;
+  const bool in = g.r2 < P.rc2f;
+  if (!ALWAYS && !in) return false;
+  const float2 pe = __fmul2_rn(__ffma2_rn(make_float2(2.f, 2.f), make_float2(C.x, C.y), exy), exy); // (2C + e) e
+  g.num = pe.x + pe.y + (2.f * C.z + ez) * ez;
+  return in;
+}
+
+// One density pair.  BF (branch-free): entries inside the cutoff for nearly every
+// lane; the value is masked instead of branched around so iterations overlap.
+template <bool BF>
+__device__ __forceinline__ void rho_pair(const EnsParams &P, const float4 &u, const float4 &nb, const float4 &C, int s,
+                                         int k, const float4 *s_fv, float &rs, float &rc) {
+  PairGeo g;
+  const bool in = pair_geo<BF>(P, u, nb, C, g);
+  if (!BF && !in) return;
+  const float r = g.r2 * rsqrtf(g.r2);
+  int m;
+  float q;
+  knot_of(P, s, k, __fdividef(g.num, r + C.w), m, q);
+  const float4 c = (m >= P.m_lo) ? s_fv[m - P.m_lo] : __ldg(&P.P.f_val32[m]);
+  float v = ((c.w * q + c.z) * q + c.y) * q + c.x;
+  if (BF) v = in ? v : 0.f;
+  two_sum(rs, rc, v);
+}
+
+// Knuth two-sum on packed pairs of lanes (f32x2 instructions).
+__device__ __forceinline__ void two_sum2(float2 &s, float2 &c, float2 x) {
+  const float2 m1 = make_float2(-1.f, -1.f);
+  const float2 t = __fadd2_rn(s, x);
+  const float2 bp = __ffma2_rn(s, m1, t);                  // t - s
+  const float2 sa = __ffma2_rn(__ffma2_rn(bp, m1, t), m1, s); // s - (t - bp)
+  const float2 xb = __ffma2_rn(bp, m1, x);                  // x - bp
+  c = __fadd2_rn(c, __fadd2_rn(sa, xb));
+  s = t;
+}
+
+// One pair of the force pass: x and y components ride together in f32x2 lanes, and
+// the derivative pieces of f and phi (stored as {f', phi'} pairs per knot) are
+// evaluated by one packed Horner chain.
+template <bool ENERGY, bool BF>
+__device__ __forceinline__ void force_pair(const EnsParams &P, const float4 &u, const float4 &nb, const float4 &C,
+                                           int s, int k, const float2 *s_fd, float2 &fxy_s, float2 &fxy_c, float &zs,
+                                           float &zc, float &ps, float &pc) {
+  PairGeo g;
+  const bool in = pair_geo<BF>(P, u, nb, C, g);
+  if (!BF && !in) return;
+  const float r2 = g.r2, num = g.num, dz = g.dz;
+  const float2 dxy = g.dxy;
+  float rinv = rsqrtf(r2);
+  rinv = rinv * (1.5f - 0.5f * r2 * rinv * rinv);
+  const float r = r2 * rinv;
+  int m;
+  float q;
+  knot_of(P, s, k, __fdividef(num, r + C.w), m, q);
+  float2 c0, c1, c2;
+  if (m >= P.m_lo) {
+    const float2 *cp = s_fd + 3 * (m - P.m_lo);
+    c0 = cp[0];
+    c1 = cp[1];
+    c2 = cp[2];
+  } else {
+    const float2 *cp = P.P.force32 + 3 * m;
+    c0 = __ldg(cp);
+    c1 = __ldg(cp + 1);
+    c2 = __ldg(cp + 2);
+  }
+  const float2 qq = make_float2(q, q);
+  const float2 dd = __ffma2_rn(__ffma2_rn(c2, qq, c1), qq, c0); // {f'(r), phi'(r)}
+  float fpair = -((u.w + nb.w) * dd.x + dd.y) * rinv;
+  if (BF) fpair = in ? fpair : 0.f;
+  two_sum2(fxy_s, fxy_c, __fmul2_rn(dxy, make_float2(fpair, fpair)));
+  two_sum(zs, zc, dz * fpair);
+  if (ENERGY) {
+    const float4 pv = __ldg(&P.P.phi_val32[m]);
+    float e = 0.5f * (((pv.w * q + pv.z) * q + pv.y) * q + pv.x);
+    if (BF) e = in ? e : 0.f;
+    two_sum(ps, pc, e);
+  }
+}
+
+// ------------------------------------------------------- interstitial items
+// Sites flagged at the previous step of lattice d lose their flag (all CTAs share
+// the old list); the count this step will fill starts at zero.  Counts alternate
+// with the buffer parity: count[cur] is this step's list, count[cur ^ 1] the last.
+__device__ __forceinline__ void itl_clear_flags(const LatDesc &d) {
+  const int cur = d.cur;
+  const int nold = min(d.flag_count[cur ^ 1], d.cap_flag);
+  const int stride = gridDim.x * blockDim.x;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nold; k += stride) {
+    const int idx = d.flag_list[k];
+    d.code[idx] = (int8_t)(d.code[idx] & ~MB_FLAG_ITL);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) d.flag_count[cur] = 0;
+}
+
+// Warp `w` of the grid flags the lattice sites within reach of interstitial w.
+__device__ __forceinline__ void itl_mark_one(const EnsParams &P, const LatDesc &d, int it) {
+  const Geom g = lat_geom(d);
+  const int lane = threadIdx.x & 31;
+  const int cur = d.cur;
+  const double qx = d.ipx[cur][it], qy = d.ipy[cur][it], qz = d.ipz[cur][it];
+  const Window w = make_window(qx, qy, qz, P.a0, P.reach);
+  const int ncand = w.nx * w.ny * w.nz;
+  for (int c = lane; c < ncand; c += 32) {
+    long long idx;
+    double sx, sy, sz;
+    if (!window_site(g, w, c, qx, qy, qz, P.a0, P.reach, idx, sx, sy, sz)) continue;
+    if (d.code[idx] < 0) continue;
+    const uintptr_t addr = (uintptr_t)(d.code + idx);
+    unsigned int *word = (unsigned int *)(addr & ~(uintptr_t)3);
+    const unsigned int bit = (unsigned int)MB_FLAG_ITL << (8 * (addr & 3));
+    const unsigned int old = atomicOr(word, bit);
+    if (!(old & bit)) {
+      const int slot = atomicAdd(&d.flag_count[cur], 1);
+      if (slot < d.cap_flag)
+        d.flag_list[slot] = (int)idx;
+      else
+        d.flag_count[2] = 1; // overflow: reported by the host
+    }
+  }
+}
+
+// Work of one warp on item w of lattice d: a flagged site (w < nflag) or an
+// interstitial.  FORCE = false: density pass; true: force + integration pass.
+template <bool FORCE, bool ENERGY>
+__device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag) {
+  const int lane = threadIdx.x & 31;
+  const Geom g = lat_geom(d);
+  const int cur = d.cur;
+  const float4 *u4 = d.u4[cur];
+  const bool is_site = w < nflag;
+  long long i = 0;
+  int s = 0, cx = 0, y = 0, z = 0, it = 0, ti;
+  double xi, yi, zi, dfi = 0.0;
+  if (is_site) {
+    i = d.flag_list[w];
+    decode_ext(g, i, s, cx, y, z);
+    ti = d.code[i] & 0x3F;
+    double X, Y, Z;
+    ideal_pos(s, cx, y, z, P.a0, X, Y, Z);
+    xi = X + d.ux[i];
+    yi = Y + d.uy[i];
+    zi = Z + d.uz[i];
+    if (FORCE) dfi = (double)u4[i].w;
+  } else {
+    it = w - nflag;
+    ti = d.itype[it];
+    xi = d.ipx[cur][it];
+    yi = d.ipy[cur][it];
+    zi = d.ipz[cur][it];
+    if (FORCE) dfi = d.idf[it];
+  }
+  double acc0 = 0.0, fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
+  auto pair = [&](double dx, double dy, double dz, int tj, double dfj) {
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 >= P.rc2) return;
+    const double rinv = rsqrt(d2);
+    const double r = d2 * rinv;
+    if (!FORCE) {
+      acc0 += rho_of_r(P.P, tj, r);
+    } else {
+      double ph = 0.0;
+      const double psip = pair_psip(P.P, ti, tj, r, dfi, dfj, ENERGY ? &ph : nullptr);
+      const double fpair = -psip * rinv;
+      fx += dx * fpair;
+      fy += dy * fpair;
+      fz += dz * fpair;
+      if (ENERGY) ep += 0.5 * ph;
+    }
+  };
+  if (is_site) {
+    for (int k = lane; k < P.n_st; k += 32) {
+      const char4 e = P.sd[s][k];
+      const long long j = i + (long long)e.x * d.E + ((long long)e.w * d.ey + e.z) * d.ecx + e.y;
+      const int cj = d.code[j];
+      if (cj < 0) continue;
+      double xj, yj, zj;
+      lat_pos(d, u4, j, P.a0, xj, yj, zj);
+      pair(xi - xj, yi - yj, zi - zj, cj & 0x3F, FORCE ? (double)u4[j].w : 0.0);
+    }
+  } else {
+    const Window win = make_window(xi, yi, zi, P.a0, P.reach);
+    const int ncand = win.nx * win.ny * win.nz;
+    for (int c = lane; c < ncand; c += 32) {
+      long long j;
+      double sx, sy, sz;
+      if (!window_site(g, win, c, xi, yi, zi, P.a0, P.reach, j, sx, sy, sz)) continue;
+      const int cj = d.code[j];
+      if (cj < 0) continue;
+      double xj, yj, zj;
+      lat_pos(d, u4, j, P.a0, xj, yj, zj);
+      pair(xi - (xj + sx), yi - (yj + sy), zi - (zj + sz), cj & 0x3F, FORCE ? (double)u4[j].w : 0.0);
+    }
+  }
+  for (int K = lane; K < d.n_itl; K += 32) {
+    if (!is_site && K == it) continue;
+    pair(min_image(xi - d.ipx[cur][K], g.Lx, g.iLx), min_image(yi - d.ipy[cur][K], g.Ly, g.iLy), min_image(zi - d.ipz[cur][K], g.Lz, g.iLz),
+         d.itype[K], FORCE ? d.idf[K] : 0.0);
+  }
+  if (!FORCE) {
+    acc0 = warp_sum(acc0);
+    if (lane == 0) {
+      const double df = dF64(P.P, ti, acc0);
+      if (is_site) {
+        float4 *uw = d.u4[cur];
+        reinterpret_cast<float *>(uw + i)[3] = (float)df;
+        d.rho[i] = (float)acc0;
+        for_images(g, s, cx, y, z,
+                   [&](long long idx, double, double, double) { reinterpret_cast<float *>(uw + idx)[3] = (float)df; });
+      } else {
+        d.irho[it] = acc0;
+        d.idf[it] = df;
+      }
+      if (ENERGY) atomicAdd(&d.e_itl[0], F64(P.P, ti, acc0));
+    }
+    return;
+  }
+  fx = warp_sum(fx);
+  fy = warp_sum(fy);
+  fz = warp_sum(fz);
+  if (ENERGY) ep = warp_sum(ep);
+  if (lane != 0) return;
+  double vx, vy, vz;
+  if (is_site) {
+    d.fx[i] = (float)fx;
+    d.fy[i] = (float)fy;
+    d.fz[i] = (float)fz;
+    vx = d.vx[i];
+    vy = d.vy[i];
+    vz = d.vz[i];
+  } else {
+    d.ifx[it] = fx;
+    d.ify[it] = fy;
+    d.ifz[it] = fz;
+    vx = d.ivx[it];
+    vy = d.ivy[it];
+    vz = d.ivz[it];
+  }
+  if (d.primed) {
+    vx += P.h * fx;
+    vy += P.h * fy;
+    vz += P.h * fz;
+  }
+  if (ENERGY) {
+    atomicAdd(&d.e_itl[0], ep);
+    atomicAdd(&d.e_itl[1], 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E);
+  }
+  vx += P.h * fx;
+  vy += P.h * fy;
+  vz += P.h * fz;
+  if (is_site) {
+    d.vx[i] = vx;
+    d.vy[i] = vy;
+    d.vz[i] = vz;
+    const double nx = d.ux[i] + P.dt * vx, ny = d.uy[i] + P.dt * vy, nz = d.uz[i] + P.dt * vz;
+    d.ux[i] = nx;
+    d.uy[i] = ny;
+    d.uz[i] = nz;
+    const float4 nu = make_float4((float)nx, (float)ny, (float)nz, 0.f);
+    float4 *un = d.u4[cur ^ 1];
+    un[i] = nu;
+    for_images(g, s, cx, y, z, [&](long long idx, double, double, double) { un[idx] = nu; });
+  } else {
+    d.ivx[it] = vx;
+    d.ivy[it] = vy;
+    d.ivz[it] = vz;
+    d.ipx[cur ^ 1][it] = xi + P.dt * vx;
+    d.ipy[cur ^ 1][it] = yi + P.dt * vy;
+    d.ipz[cur ^ 1][it] = zi + P.dt * vz;
+  }
+}
+
+template <bool FORCE, bool ENERGY>
+__device__ void itl_items(const EnsParams &P) {
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  for (int q = 0; q < P.n_itl_lats; q++) {
+    const LatDesc &d = P.lats[P.itl_lats[q]];
+    if (!lat_active(d)) continue;
+    const int nflag = min(d.flag_count[d.cur], d.cap_flag);
+    const int n = nflag + d.n_itl;
+    for (int w = gw; w < n; w += warps) itl_item<FORCE, ENERGY>(P, d, w, nflag);
+  }
+}
+
+} // namespace mb

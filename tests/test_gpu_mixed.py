@@ -58,6 +58,48 @@ def test_mixed_forces_within_1e6_of_fp64_oracle(n_itl):
     np.testing.assert_allclose(bg["x"][live], sc.box["x"][live], rtol=0, atol=1e-12)
 
 
+@pytest.mark.parametrize("n_itl", [0, 3])
+def test_split_kernels_forces_within_1e6_of_fp64_oracle(n_itl):
+    # the separate density / force kernels used for one large lattice, forced on a small one
+    sc = make(cells=(9, 8, 10), temperature=900.0, vacancy=0.01, n_itl=n_itl, seed=71, jitter=0.1)
+    bo, io, pe = _oracle_forces(sc, itl=sc.itl)
+    with _ens(sc) as ens:
+        ens.set_mode(2)
+        slot = ens.add(sc.cells, sc.box, sc.itl if n_itl else None, steps=0)
+        ens.run(0)
+        bg, ig = ens.download(slot)
+    live = bo["type"] >= 0
+    fo, fg = bo["f"][live], bg["f"][live]
+    if n_itl:
+        fo = np.concatenate([fo, io["f"]])
+        fg = np.concatenate([fg, ig["f"]])
+    assert rms_rel(fg, fo) < F_RMS_TOL
+    assert rms_rel(bg["rho"][live], bo["rho"][live]) < 1e-6
+
+
+def test_split_kernels_track_persistent_kernel():
+    sc = make(cells=(10, 9, 8), temperature=900.0, vacancy=0.005, n_itl=2, seed=74)
+    out = {}
+    for mode in (1, 2):
+        with _ens(sc) as ens:
+            ens.set_mode(mode)
+            s = ens.add(sc.cells, sc.box, sc.itl, steps=40)
+            ens.advance(100, energy_every=10)
+            out[mode] = (*ens.download(s), ens.energies(s), ens.status(s)[0])
+    (b1, i1, e1, n1), (b2, i2, e2, n2) = out[1], out[2]
+    assert n1 == n2 == 40
+    live = b1["type"] >= 0
+    # same pair arithmetic, different summation order: rounding-level differences only
+    assert np.max(np.abs(b1["x"][live] - b2["x"][live])) < 1e-6
+    assert np.max(np.abs(i1["x"] - i2["x"])) < 1e-6
+    assert np.array_equal(e1[:, 0], e2[:, 0])
+    n = int(live.sum()) + 2
+    assert np.max(np.abs((e1[:, 1] + e1[:, 2]) - (e2[:, 1] + e2[:, 2]))) / n < 1e-7
+    with _ens(sc) as ens:
+        with pytest.raises(mb.MbError):
+            ens.set_mode(3)
+
+
 def test_mixed_sim_tracks_fp64_sim():
     sc = make(cells=(8, 8, 8), temperature=900.0, vacancy=0.005, n_itl=2, seed=72)
     out = {}
