@@ -39,7 +39,8 @@ A0, MASS, RC, SKIN, DT = 2.855, 55.845, 5.6, 0.7, 1.0
 #   force pass reads x, type, df, v, f_old (84), writes x, v, f (72)         = 156 B
 #   flops: 58 pairs x (20 rho + 50 force) + 30 per atom                      = 4090
 BYTES_RHO, BYTES_FORCE = 36, 156
-BYTES_MIXED = 160  # mixed: rho pass 32 B + force/VV pass 128 B per atom-step
+BYTES_MIXED_RHO, BYTES_MIXED_FORCE = 32, 128  # mixed: df and f stored as FP32
+BYTES_MIXED = BYTES_MIXED_RHO + BYTES_MIXED_FORCE
 FLOP_RHO, FLOP_FORCE = 58 * 20, 58 * 50 + 30
 
 WORKLOADS = {
@@ -267,6 +268,11 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
     if precision == mb.MB_PREC_FP64:
         kname, kbytes, kflops, kms = "k_force64 (force + velocity-Verlet)", BYTES_FORCE * n_atoms, FLOP_FORCE, force_ms
         fpeak, fname = f64.value, "fp64"
+    elif rho_ms > 0:
+        # split kernels (one large lattice): density pass, then force + integration
+        kname, kbytes, kflops, kms = ("k_mx_force (mixed force + velocity-Verlet)", BYTES_MIXED_FORCE * n_atoms,
+                                      FLOP_FORCE, force_ms)
+        fpeak, fname = f32.value, "fp32"
     else:
         # one persistent launch holds the rho, force and integration phases
         kname, kbytes, kflops, kms = ("k_ens_step (rho + force + velocity-Verlet, one persistent launch)",
@@ -283,8 +289,10 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
                 "peak_source": "measured FMA-chain probe (mb_measure_fma_peaks)"},
         "fp64_peak_tflops": f64.value, "fp32_peak_tflops": f32.value,
     }
-    if precision == mb.MB_PREC_FP64:
-        roofline["rho_kernel"] = {"launch_ms": rho_ms, "achieved_gbs": BYTES_RHO * n_atoms / (rho_ms * 1e-3) / 1e9,
+    if rho_ms > 0:
+        rb = BYTES_RHO if precision == mb.MB_PREC_FP64 else BYTES_MIXED_RHO
+        roofline["rho_kernel"] = {"kernel": "k_rho64" if precision == mb.MB_PREC_FP64 else "k_mx_rho",
+                                  "launch_ms": rho_ms, "achieved_gbs": rb * n_atoms / (rho_ms * 1e-3) / 1e9,
                                   "achieved_tflops": FLOP_RHO * n_atoms / (rho_ms * 1e-3) / 1e12}
 
     # end to end through the public host-buffer entry point: every step uploads the
@@ -325,6 +333,8 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
     sim.close()
     if precision == mb.MB_PREC_FP64:
         launches_per_step = 5 if itl.shape[0] else 2
+    elif rho_ms > 0:  # split: itl clear, mark, rho, itl rho, force, itl force, bookkeeping
+        launches_per_step = 7 if itl.shape[0] else 3
     else:
         launches_per_step = 1
     if rank == 0:
@@ -366,11 +376,16 @@ def mixed_comparison(args, mb, wl, box, itl, n_atoms, fp64_rate, pg) -> dict:
         ms = s.time_steps(args.steps)
         barrier(pg)
         ms = reduce_max(pg, ms)
+        rho_ms, force_ms = s.kernel_times()
     rate = n_atoms * args.steps / (ms * 1e-3)
+    if rho_ms > 0:
+        kern = {"kernels": "k_mx_rho, k_mx_force (+ interstitial and bookkeeping kernels), one CUDA graph per step",
+                "rho_ms": rho_ms, "force_ms": force_ms}
+    else:
+        kern = {"kernels": "k_ens_step (one persistent launch per step)", "step_ms": force_ms}
     return {"value": rate * (int(os.environ.get("WORLD_SIZE", "1"))), "unit": "atom-steps/s",
             "ms_per_step": ms / args.steps, "speedup_vs_fp64": rate / fp64_rate,
-            "force_rms_rel_err_vs_fp64": err, "dtype": "f32 pairs + two-sum, f64 state",
-            "kernel": "k_ens_step (one persistent launch per step)"}
+            "force_rms_rel_err_vs_fp64": err, "dtype": "f32 pairs + two-sum, f64 state", **kern}
 
 
 def run_ensemble(args, mb, world, rank, local, pg) -> None:

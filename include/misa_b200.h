@@ -193,7 +193,8 @@ int mb_sim_time_steps(mb_sim *sim, int32_t nsteps, float *ms);
  * one velocity-Verlet step on the device, write x, v, f, rho, df back.  The
  * e2e form of the hot path: host<->device copies are part of every call. */
 int mb_sim_step_host(mb_sim *sim, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t n_itl);
-/* Mean kernel milliseconds of the rho and force launches of the last timed run. */
+/* Mean device milliseconds of the rho and force launches over 4 extra steps the sim
+ * takes (mixed precision: as mb_ensemble_kernel_times). */
 int mb_sim_kernel_times(mb_sim *sim, float *rho_ms, float *force_ms);
 int mb_sim_info(mb_sim *sim, int64_t *n_sites, int64_t *n_stencil, int64_t *device_bytes);
 /* CUDA graph capture of the steady-state step (on by default). */
@@ -256,6 +257,11 @@ int mb_ensemble_set_graphs(mb_ensemble *e, int enable);
  * persistent one-launch-per-step kernel; 1 always persistent; 2 always split (one
  * lattice only). */
 int mb_ensemble_set_mode(mb_ensemble *e, int32_t mode);
+/* Device time of one step's kernels, averaged over 4 extra steps every lattice takes
+ * (CUDA events on the ensemble's stream): split kernels report the density pass in
+ * *rho_ms and the force + integration pass in *force_ms; the persistent kernel
+ * reports 0 and its whole launch.  *kernels_per_step: launches one step issues. */
+int mb_ensemble_kernel_times(mb_ensemble *e, float *rho_ms, float *force_ms, int32_t *kernels_per_step);
 
 #ifdef __cplusplus
 }

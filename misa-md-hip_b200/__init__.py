@@ -274,3 +274,9 @@ class Ensemble:
     def set_mode(self, mode: int) -> None:
         """0: split kernels for one large lattice (default), 1: persistent, 2: split."""
         check(lib().mb_ensemble_set_mode(self._h, mode))
+
+    def kernel_times(self) -> tuple[float, float, int]:
+        """(density ms, force ms, kernels per step) of one step; see mb_ensemble_kernel_times."""
+        a, b, n = C.c_float(), C.c_float(), C.c_int32()
+        check(lib().mb_ensemble_kernel_times(self._h, C.byref(a), C.byref(b), C.byref(n)))
+        return a.value, b.value, n.value

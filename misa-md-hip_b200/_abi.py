@@ -125,6 +125,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_ensemble_info": (_I, [_P, _PI64, _PI64, _PI64, C.POINTER(C.c_int32)]),
     "mb_ensemble_set_graphs": (_I, [_P, _I]),
     "mb_ensemble_set_mode": (_I, [_P, C.c_int32]),
+    "mb_ensemble_kernel_times": (_I, [_P, _PF, _PF, C.POINTER(C.c_int32)]),
 }
 
 

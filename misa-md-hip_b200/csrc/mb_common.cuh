@@ -65,6 +65,19 @@ struct DevPot {
   const float4 *f_val32;   // [nt][nr]  {y, s, c2, c3}
   const float2 *force32;   // single type: [nr][3] {f d0, phi d0}, {f d1, phi d1}, {f d2, phi d2}
   const float4 *phi_val32; // single type: [nr]
+  // single type, squared-distance form for the mixed split kernels, on uniform grids in
+  // s = r^2 whose knots carry the FP64 r-spline evaluated exactly; values in between
+  // are interpolated linearly.  Density: per interval {f(s_j), f(s_j+1) - f(s_j)}.
+  // Force: per knot {A, B} = {f'(r) / r, phi'(r) / r} (knot pairs are read, which
+  // halves the table against per-interval storage and allows a finer grid).
+  // n_rs = n_fs = 0 when not built (several types).
+  int n_rs;            // density intervals
+  double ds_r;
+  const float2 *fs32;  // [n_rs]
+  int n_fs;            // force intervals
+  double ds_f;
+  const float2 *ab32;  // [n_fs + 1] knots
+  const float2 *ps32;  // [n_fs] per interval {phi, d phi} (energy steps)
 };
 
 struct PotHost;

@@ -20,7 +20,8 @@ int ens_launch(const EnsParams &P, int grid, cudaStream_t s);
 int ens_max_grid(int nsm);
 int ens_energy_launch(const LatDesc *lats, int n, const int *tile_first, const double *epart, double *out,
                       cudaStream_t s);
-int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s);
+int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s,
+                   cudaEvent_t *ev = nullptr);
 int mx_energy_launch(const LatDesc *lats, int lat, const double *epart, double *out, cudaStream_t s);
 int mx_grid();
 
@@ -171,7 +172,7 @@ struct mb_ensemble {
   mb::EnsParams P{};
   std::vector<mb::LatHost> slots;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev[2] = {};
+  cudaEvent_t ev[6] = {};
   // device work lists (rebuilt when slots change)
   mb::LatDesc *d_lats = nullptr;
   int *d_tile_lat = nullptr, *d_tile_idx = nullptr, *d_tile_first = nullptr, *d_itl_lats = nullptr;
@@ -341,6 +342,8 @@ static void drop_graph(mb_ensemble *e) {
 }
 
 // Rebuild descriptors, tile lists and tensor maps after slots or shapes change.
+static const char *mx_stencil(const mb_ensemble *e, const LatDesc &d, MxStencil &S);
+
 static int rebuild(mb_ensemble *e) {
   MB_TRY(sync_desc(e));
   drop_graph(e);
@@ -453,15 +456,130 @@ static int rebuild(mb_ensemble *e) {
     const long long sites = 2LL * d.bcx * d.by * d.bz;
     e->split = e->mode == 2 || (e->mode == 0 && sites >= kSplitMinSites);
     if (e->split && e->cap_tiles < (size_t)mx_grid()) e->split = false; // one energy partial per CTA
-    if (e->split)
-      for (int s = 0; s < 2; s++)
-        for (int k = 0; k < P.n_st; k++) {
-          const char4 q = P.sd[s][k];
-          e->mxs.off[s][k] = (int)((long long)q.x * d.E + ((long long)q.w * d.ey + q.z) * d.ecx + q.y);
-        }
+    if (e->split) {
+      const char *why = mx_stencil(e, d, e->mxs);
+      if (why) {
+        e->split = false;
+        if (e->mode == 2) return fail(MB_ERR_UNSUPPORTED, why);
+      }
+    }
   }
   e->dirty = false;
   return MB_OK;
+}
+
+// Split-mode stencil of lattice d (see MxStencil); returns why it cannot be built, or
+// nullptr.  Neighbour vectors are enumerated in half-lattice units (hx, hy, hz), all
+// of one parity, and ordered by length.
+static const char *mx_stencil(const mb_ensemble *e, const LatDesc &d, MxStencil &S) {
+  const DevPot &pp = e->P.P;
+  if (pp.n_rs <= 0 || pp.n_fs <= 0) return "split kernels need the single-type squared-distance tables";
+  const double a0 = e->cfg.lattice_const, rc = e->cfg.cutoff, reach = rc + e->cfg.stencil_skin;
+  if (rc * rc > pp.ds_r * pp.n_rs * (1.0 + 1e-12) || rc * rc > pp.ds_f * pp.n_fs * (1.0 + 1e-12))
+    return "cutoff beyond the potential table";
+  const double h = 0.5 * a0;
+  const int lim = (int)ceil(reach / h);
+  struct V {
+    double R;
+    int hx, hy, hz;
+  };
+  std::vector<V> vs;
+  for (int hz = -lim; hz <= lim; hz++)
+    for (int hy = -lim; hy <= lim; hy++)
+      for (int hx = -lim; hx <= lim; hx++) {
+        if (!hx && !hy && !hz) continue;
+        if (((hx ^ hy) & 1) || ((hx ^ hz) & 1)) continue;
+        const double R = h * sqrt((double)(hx * hx + hy * hy + hz * hz));
+        if (R < reach) vs.push_back({R, hx, hy, hz});
+      }
+  if ((int)vs.size() != e->P.n_st) return "split stencil differs from the lattice stencil";
+  std::stable_sort(vs.begin(), vs.end(), [](const V &a, const V &b) { return a.R < b.R; });
+  const long long E = d.E, ecx = d.ecx, ey = d.ey;
+  const long long d_odd = -2 * E + (ey + 1) * ecx + 1;
+  memset(&S, 0, sizeof(S));
+  S.d_odd = (int)d_odd;
+  S.n_rs = pp.n_rs;
+  S.n_fs = pp.n_fs;
+  S.rds = (float)(1.0 / pp.ds_r);
+  S.rds_f = (float)(1.0 / pp.ds_f);
+  const double bf_reach = rc + 0.5 * e->cfg.stencil_skin;
+  for (const V &v : vs) {
+    MxEntry E0;
+    const bool odd = v.hx & 1;
+    long long dcx, dy, dz;
+    if (odd) {
+      dcx = (v.hx - 1) / 2;
+      dy = (v.hy - 1) / 2;
+      dz = (v.hz - 1) / 2;
+    } else {
+      dcx = v.hx / 2;
+      dy = v.hy / 2;
+      dz = v.hz / 2;
+    }
+    // both sublattices' targets must stay inside the 2-cell ghost frame
+    if (llabs(dcx) > 2 || llabs(dy) > 2 || llabs(dz) > 2 || (odd && (dcx + 1 > 2 || dy + 1 > 2 || dz + 1 > 2)))
+      return "stencil reaches beyond the 2-cell ghost frame";
+    E0.off = (int)((odd ? E : 0) + (dz * ey + dy) * ecx + dcx);
+    E0.odd = odd ? 1 : 0;
+    const double cx = -h * v.hx, cy = -h * v.hy, cz = -h * v.hz, R2 = v.R * v.R;
+    E0.c = make_float4((float)cx, (float)cy, (float)cz, (float)(rc * rc - R2));
+    const double x = R2 / pp.ds_r, fl = floor(x), xf = R2 / pp.ds_f, flf = floor(xf);
+    E0.t = make_float4((float)(2 * cx), (float)(2 * cy), (float)(2 * cz), (float)(x - fl));
+    E0.kb = (float)fl;
+    E0.fr_f = (float)(xf - flf);
+    E0.kb_f = (float)flf;
+    E0.pad_[0] = E0.pad_[1] = E0.pad_[2] = 0;
+    if (v.R < bf_reach && odd && S.n_odd < MX_PAR_MAX - 1)
+      S.odd[S.n_odd++] = E0;
+    else if (v.R < bf_reach && !odd && S.n_even < MX_PAR_MAX - 1)
+      S.even[S.n_even++] = E0;
+    else
+      S.far[S.n_far++] = E0;
+  }
+  // pad each branch-free list to even length with an entry that never interacts
+  auto pad = [](MxEntry *list, int &n) {
+    if (n & 1) {
+      list[n] = list[0];
+      list[n].c.w = -3.0e38f;
+      n++;
+    }
+  };
+  if (S.n_odd == 0 || S.n_even == 0) return "split stencil has an empty branch-free class";
+  pad(S.odd, S.n_odd);
+  pad(S.even, S.n_even);
+  // brick walk
+  const unsigned chunks = (unsigned)((d.bcx + 31) / 32), nyb = (unsigned)((d.by + MX_BY - 1) / MX_BY),
+                 nzb = (unsigned)((d.bz + MX_BZ - 1) / MX_BZ);
+  const unsigned long long units = (unsigned long long)chunks * nyb * nzb;
+  if (units * MX_BRICK_ITEMS >= (1ull << 31)) return "lattice too large for the 32-bit brick walk";
+  S.walk.chunks = chunks;
+  S.walk.m_chunks = 0xFFFFFFFFu / chunks;
+  S.walk.nyb = nyb;
+  S.walk.m_nyb = 0xFFFFFFFFu / nyb;
+  S.walk.n_units = (unsigned)units;
+  // built-in shells: the stencil must be exactly BCC shells 1-7 (|h|^2 <= 19 < 20)
+  const double r7 = h * sqrt(19.0), r8 = h * sqrt(20.0);
+  S.fixed = (vs.size() == 88 && r7 < reach && reach <= r8 && (long long)ey * ecx < (1ll << 31)) ? 1 : 0;
+  const int n2s[MX_SHELLS] = {3, 4, 8, 11, 12, 16, 19};
+  MxShells &Q = S.sh;
+  const double grid_ds[2] = {pp.ds_r, pp.ds_f};
+  const int grid_n[2] = {pp.n_rs, pp.n_fs};
+  for (int k = 0; k < MX_SHELLS; k++) Q.w[k] = (float)(rc * rc - h * h * n2s[k]);
+  for (int gi = 0; gi < 2; gi++) {
+    Q.g[gi].rds = (float)(1.0 / grid_ds[gi]);
+    Q.g[gi].mmax = (float)(grid_n[gi] - 1);
+    for (int k = 0; k < MX_SHELLS; k++) {
+      const double x = h * h * n2s[k] / grid_ds[gi], fl = floor(x);
+      Q.g[gi].fr[k] = (float)(x - fl);
+      Q.g[gi].kb[k] = (float)fl;
+    }
+  }
+  Q.a0 = (float)a0;
+  Q.pl = (int)(ey * ecx);
+  Q.rw = (int)ecx;
+  Q.E = E;
+  Q.d_odd = d_odd;
+  return nullptr;
 }
 
 static int check_err(mb_ensemble *e) {
@@ -1007,6 +1125,54 @@ int mb_ensemble_time(mb_ensemble *e, int32_t nsteps, float *ms) {
   MB_CUDA(cudaEventElapsedTime(ms, e->ev[0], e->ev[1]));
   MB_TRY(check_err(e));
   if (n != nsteps) return fail(MB_ERR_STATE, "timed launches ended early");
+  return MB_OK;
+}
+
+int mb_ensemble_kernel_times(mb_ensemble *e, float *rho_ms, float *force_ms, int32_t *kernels_per_step) {
+  if (!e) return fail(MB_ERR_ARG, "null ensemble");
+  std::lock_guard<std::mutex> lk(e->mu);
+  MB_TRY(sync_desc(e));
+  const int reps = 4;
+  for (auto &L : e->slots)
+    if (L.used) L.d.steps_target = L.d.steps_done + reps + 1;
+  if (e->dirty)
+    MB_TRY(rebuild(e));
+  else
+    MB_TRY(push_targets(e));
+  if (e->n_tiles == 0) return fail(MB_ERR_STATE, "no lattices");
+  bool unprimed = false;
+  for (int s : e->order) unprimed |= !e->slots[s].d.primed;
+  if (unprimed) {
+    long long n = 0;
+    MB_TRY(advance(e, 1, 0, &n));
+  }
+  float tr = 0.f, tf = 0.f;
+  e->P.energy = 0;
+  for (int k = 0; k < reps; k++) {
+    if (e->split) {
+      MB_TRY(mx_launch_step(e->P, e->mxs, 0, 0, e->stream, e->ev + 2));
+    } else {
+      MB_CUDA(cudaEventRecord(e->ev[4], e->stream));
+      MB_TRY(ens_launch(e->P, e->grid, e->stream));
+      MB_CUDA(cudaEventRecord(e->ev[5], e->stream));
+    }
+    e->launches++;
+    MB_CUDA(cudaStreamSynchronize(e->stream));
+    float a = 0.f, b = 0.f;
+    if (e->split) {
+      MB_CUDA(cudaEventElapsedTime(&a, e->ev[2], e->ev[3]));
+      MB_CUDA(cudaEventElapsedTime(&b, e->ev[4], e->ev[5]));
+    } else {
+      MB_CUDA(cudaEventElapsedTime(&b, e->ev[4], e->ev[5]));
+    }
+    tr += a;
+    tf += b;
+  }
+  e->synced_desc = false;
+  MB_TRY(check_err(e));
+  if (rho_ms) *rho_ms = tr / reps;
+  if (force_ms) *force_ms = tf / reps;
+  if (kernels_per_step) *kernels_per_step = e->split ? (3 + (e->P.n_itl_lats > 0 ? 4 : 0)) : 1;
   return MB_OK;
 }
 

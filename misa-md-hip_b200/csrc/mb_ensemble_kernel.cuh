@@ -91,9 +91,66 @@ struct EnsParams {
   int energy;
 };
 
-// Split mode: per-lattice linear neighbour offsets in the ghost-extended arrays.
+// Split mode stencil.  BCC is a Bravais lattice: both sublattices see the same ideal
+// neighbour vectors, so the per-entry constants below serve every site.  Only the
+// storage offset differs, and only for vectors that cross to the other sublattice
+// (odd half-lattice components): a sublattice-1 site adds d_odd to their offset.
+// Entries inside the cutoff (plus half the skin) are split by that parity into two
+// lists walked without a per-pair branch, each padded to an even length; the rest
+// are walked with a branch.
+#define MX_PAR_MAX 40
+struct MxEntry {
+  float4 c;    // ideal X_i - X_j (xyz); w = rc^2 - R^2: the pair interacts when num < w
+  float4 t;    // 2 (X_i - X_j) (xyz); w = frac(R^2 / ds) on the density grid
+  float kb;    // floor(R^2 / ds) on the density grid
+  float fr_f;  // frac / floor of R^2 / ds on the force grid
+  float kb_f;
+  int off;     // linear offset from a sublattice-0 site
+  int odd;     // 1: crosses sublattices
+  int pad_[3];
+};
+
+// Walk of the split kernels: the box is cut into bricks of one x chunk (32 sites, one
+// per lane) by MX_BY rows by MX_BZ planes by both sublattices; a block takes whole
+// bricks (brick b, b + grid, ...) so the rows its warps read overlap and stay in L1.
+// Brick index -> (chunk, y brick, z brick) by multiply-high divisions.
+#define MX_BY 8
+#define MX_BZ 8
+#define MX_BRICK_ITEMS (2 * MX_BY * MX_BZ)
+struct MxWalk {
+  unsigned chunks, m_chunks; // x chunks per row and floor((2^32 - 1) / chunks)
+  unsigned nyb, m_nyb;       // y bricks
+  unsigned n_units;          // bricks
+};
+
+// Split-mode stencil built into the kernel: the BCC neighbour shells up to |h|^2 = 19
+// (half-lattice units), which is the stencil whenever cutoff + skin lies between the
+// 7th and 8th shell (a0 = 2.855, rc = 5.6, skin = 0.7 for iron).  Only per-shell and
+// per-lattice scalars are runtime values.
+#define MX_SHELLS 7
+struct MxGrid {
+  float rds, mmax;     // 1 / ds, last interval
+  float fr[MX_SHELLS]; // frac(R^2 / ds)
+  float kb[MX_SHELLS]; // floor(R^2 / ds)
+};
+struct MxShells {
+  float w[MX_SHELLS];  // rc^2 - R^2
+  MxGrid g[2];         // density grid, force grid
+  float a0;
+  int pl, rw;          // plane and row strides of the ghost-extended arrays
+  long long E;         // sites per sublattice array
+  long long d_odd;     // extra offset of odd entries for sublattice-1 sites
+};
+
 struct MxStencil {
-  int off[2][ENS_MAX_ST];
+  int n_odd, n_even, n_far;
+  int d_odd;        // extra offset of odd entries for sublattice-1 sites
+  int n_rs, n_fs;   // density / force table intervals
+  float rds, rds_f; // 1 / ds of the density / force grid
+  MxEntry odd[MX_PAR_MAX], even[MX_PAR_MAX], far[ENS_MAX_ST];
+  MxWalk walk;
+  int fixed;   // 1: the built-in shell stencil applies (see MxShells)
+  MxShells sh;
 };
 
 // ------------------------------------------------------------ primitives

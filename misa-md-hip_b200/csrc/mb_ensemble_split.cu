@@ -11,66 +11,176 @@
 // captured into one CUDA graph by the ensemble host.
 #include "mb_ensemble_kernel.cuh"
 #include "mb_ensemble_pair.cuh"
+#include "mb_ensemble_shells.cuh"
 
 namespace mb {
 
+#ifndef MX_RHO_THREADS
 #define MX_RHO_THREADS 1024
+#endif
+#ifndef MX_FORCE_THREADS
 #define MX_FORCE_THREADS 768
+#endif
+#define MX_SMEM_MAX (220 * 1024)
 
-// Rows of 32 sites along x: item w -> (chunk, y, s, z), as the FP64 kernels walk.
-__device__ __forceinline__ bool mx_site(const LatDesc &d, int chunks, long long w, int lane, int &s, int &cx, int &y,
-                                        int &z, long long &i) {
-  long long t = w;
-  const int chunk = (int)(t % chunks);
-  t /= chunks;
-  y = (int)(t % d.by);
-  t /= d.by;
-  s = (int)(t & 1);
-  z = (int)(t >> 1);
-  cx = chunk * 32 + lane;
-  if (cx >= d.bcx) return false;
+// n / d with m = floor((2^32 - 1) / d): multiply-high under-estimates by at most one.
+__device__ __forceinline__ unsigned fdiv(unsigned n, unsigned d, unsigned m, unsigned &r) {
+  unsigned q = __umulhi(n, m);
+  r = n - q * d;
+  if (r >= d) {
+    q++;
+    r -= d;
+  }
+  return q;
+}
+
+// Item it (0 .. MX_BRICK_ITEMS - 1) of brick `unit`: a row chunk of 32 sites, lane = x.
+__device__ __forceinline__ bool mx_site(const LatDesc &d, const MxWalk &W, unsigned unit, unsigned it, int lane,
+                                        int &s, int &cx, int &y, int &z, long long &i) {
+  unsigned chunk, yb;
+  const unsigned t = fdiv(unit, W.chunks, W.m_chunks, chunk);
+  const unsigned zb = fdiv(t, W.nyb, W.m_nyb, yb);
+  y = (int)(yb * MX_BY + it % MX_BY);
+  s = (int)((it / MX_BY) & 1u);
+  z = (int)(zb * MX_BZ + it / (2 * MX_BY));
+  cx = (int)chunk * 32 + lane;
+  if (cx >= d.bcx || y >= d.by || z >= d.bz) return false;
   i = (long long)s * d.E + ((long long)(z + 2) * d.ey + y + 2) * d.ecx + cx + 2;
   return true;
 }
 
+// ---------------------------------------------------------------- pair terms
+// Geometry of one pair: e = u_i - u_j (displacements), d = C + e the pair vector and
+// num = r^2 - R^2 = e . e + 2 C . e, exact to FP32 rounding of the small quantities.
+// The table index is s / ds = R^2 / ds + num / ds: the large part is split on the
+// host.  Entries are passed by value so that, in the unrolled loops, their fields
+// are constant-bank operands of the arithmetic.
+struct MxPair {
+  float2 exy;
+  float ez;
+  float q;
+  int m;
+  bool in;
+};
+
+__device__ __forceinline__ MxPair mx_pair(const MxEntry E, float fr, float kb, float rds, float mmax,
+                                          const float4 &u, const float4 &nb) {
+  MxPair g;
+  g.exy = __fadd2_rn(make_float2(u.x, u.y), make_float2(-nb.x, -nb.y));
+  g.ez = u.z - nb.z;
+  const float2 ee = __fmul2_rn(g.exy, g.exy);
+  float num = fmaf(g.ez, g.ez, ee.x + ee.y);
+  num = fmaf(E.t.x, g.exy.x, num);
+  num = fmaf(E.t.y, g.exy.y, num);
+  num = fmaf(E.t.z, g.ez, num);
+  g.in = num < E.c.w;
+  const float tt = fmaf(num, rds, fr);
+  const float fl = floorf(tt);
+  g.q = tt - fl;
+  g.m = (int)fminf(fmaxf(fl + kb, 0.f), mmax);
+  return g;
+}
+
+__device__ __forceinline__ float mx_rho_term(const MxEntry E, float rds, float mmax, const float4 &u,
+                                             const float4 *base, const float2 *tab) {
+  const float4 nb = __ldg(base + E.off);
+  const MxPair g = mx_pair(E, E.t.w, E.kb, rds, mmax, u, nb);
+  const float2 c = tab[g.m];
+  const float v = fmaf(c.y, g.q, c.x);
+  return g.in ? v : 0.f;
+}
+
+// Force term of one pair: fpair = -((df_i + df_j) A + B); returns fpair and the pair
+// vector.
 template <bool ENERGY>
+__device__ __forceinline__ float mx_force_term(const MxEntry E, float rds, float mmax, const float4 &u,
+                                               const float4 *base, const float2 *tab, const float2 *ptab,
+                                               float2 &dxy, float &dz, float &e) {
+  const float4 nb = __ldg(base + E.off);
+  const MxPair g = mx_pair(E, E.fr_f, E.kb_f, rds, mmax, u, nb);
+  const float2 ab = mx_ab(tab, g.m, g.q);
+  const float fp = -fmaf(u.w + nb.w, ab.x, ab.y);
+  dxy = make_float2(g.exy.x + E.c.x, g.exy.y + E.c.y);
+  dz = g.ez + E.c.z;
+  if (ENERGY) {
+    const float2 p = __ldg(ptab + g.m);
+    const float v = 0.5f * fmaf(p.y, g.q, p.x);
+    e = g.in ? v : 0.f;
+  }
+  return g.in ? fp : 0.f;
+}
+
+// Density pass.  FIXED: the built-in BCC shells (MxShells); else the runtime stencil.
+template <bool ENERGY, bool FIXED>
 __global__ void __launch_bounds__(MX_RHO_THREADS, 1)
-    k_mx_rho(const __grid_constant__ EnsParams P, const __grid_constant__ MxStencil S, int lat) {
-  extern __shared__ float4 s_fv[];
-  for (int k = threadIdx.x; k < P.nsm; k += blockDim.x) s_fv[k] = P.P.f_val32[P.m_lo + k];
+    k_mx_rho(const __grid_constant__ EnsParams P, const MxStencil S, int lat) {
+  extern __shared__ float2 s_f[];
+  for (int k = threadIdx.x; k < S.n_rs; k += blockDim.x) s_f[k] = P.P.fs32[k];
   __syncthreads();
   const LatDesc &d = P.lats[lat];
   const bool active = lat_active(d);
   const int lane = threadIdx.x & 31;
-  const int chunks = (d.bcx + 31) / 32;
-  const long long n_items = (long long)chunks * d.by * 2 * d.bz;
-  const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+  const unsigned nwarps = blockDim.x >> 5;
   const float4 *u4 = d.u4[d.cur];
   float4 *uw = d.u4[d.cur];
+  const float c[5] = {0.f, -S.sh.a0, -2.f * S.sh.a0, -3.f * S.sh.a0, -4.f * S.sh.a0};
   double e_acc = 0.0;
-  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); active && w < n_items;
-       w += wstride) {
+  for (unsigned k = threadIdx.x >> 5;; k += nwarps) {
+    const unsigned unit = blockIdx.x + (k / MX_BRICK_ITEMS) * gridDim.x;
+    if (!active || unit >= S.walk.n_units) break;
     int s, cx, y, z;
     long long i;
-    if (!mx_site(d, chunks, w, lane, s, cx, y, z, i)) continue;
+    if (!mx_site(d, S.walk, unit, k % MX_BRICK_ITEMS, lane, s, cx, y, z, i)) continue;
     const int code = d.code[i];
     if (code < 0 || (code & MB_FLAG_ITL)) continue;
     const float4 u = __ldg(u4 + i);
-    const int *off = S.off[s];
-    float rs0 = 0.f, rc0 = 0.f, rs1 = 0.f, rc1 = 0.f;
-    const int n = P.n_st, nn = P.n_near;
-    int k = 0;
-    for (; k + 1 < nn; k += 2) {
-      const float4 nb0 = __ldg(u4 + i + off[k]), nb1 = __ldg(u4 + i + off[k + 1]);
-      rho_pair<true>(P, u, nb0, P.ck[s][k], s, k, s_fv, rs0, rc0);
-      rho_pair<true>(P, u, nb1, P.ck[s][k + 1], s, k + 1, s_fv, rs1, rc1);
+    float rs = 0.f, rc = 0.f;
+    if constexpr (FIXED) {
+      const MxShells &Q = S.sh;
+      const MxSite b{u4 + i, u4 + i + Q.E + (s ? Q.d_odd : 0), Q.pl, Q.rw};
+      constexpr int nbf = 64; // shells 1-6, walked without a branch; shell 7 with one
+      static_for<0, nbf / 2>([&](auto pc) {
+        constexpr int k = 2 * decltype(pc)::value;
+        two_sum(rs, rc, mxc_rho<k>(Q, c, b, u, s_f) + mxc_rho<k + 1>(Q, c, b, u, s_f));
+      });
+      static_for<nbf, 88>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        const float4 nb = mxc_load<k>(b);
+        float2 exy;
+        float ez, q;
+        const float num = mxc_num<k>(c, u, nb, exy, ez);
+        if (num < Q.w[HStore<k>::sh]) {
+          const int m = mxc_index<k, 0>(Q, num, q);
+          const float2 t = s_f[m];
+          two_sum(rs, rc, fmaf(t.y, q, t.x));
+        }
+      });
+    } else {
+      const float4 *be = u4 + i, *bo = u4 + i + (s ? S.d_odd : 0);
+      const float rds = S.rds, mmax = (float)(S.n_rs - 1);
+#pragma unroll
+      for (int k = 0; k < MX_PAR_MAX; k += 2) {
+        if (k >= S.n_odd) break;
+        two_sum(rs, rc,
+                mx_rho_term(S.odd[k], rds, mmax, u, bo, s_f) + mx_rho_term(S.odd[k + 1], rds, mmax, u, bo, s_f));
+      }
+#pragma unroll
+      for (int k = 0; k < MX_PAR_MAX; k += 2) {
+        if (k >= S.n_even) break;
+        two_sum(rs, rc,
+                mx_rho_term(S.even[k], rds, mmax, u, be, s_f) + mx_rho_term(S.even[k + 1], rds, mmax, u, be, s_f));
+      }
+      for (int k = 0; k < S.n_far; k++) {
+        const MxEntry E = S.far[k];
+        const float4 *b = (E.odd & s) ? bo : be;
+        const float4 nb = __ldg(b + E.off);
+        const MxPair g = mx_pair(E, E.t.w, E.kb, rds, mmax, u, nb);
+        if (!g.in) continue;
+        const float2 t = s_f[g.m];
+        two_sum(rs, rc, fmaf(t.y, g.q, t.x));
+      }
     }
-    if (k < nn) {
-      rho_pair<true>(P, u, __ldg(u4 + i + off[k]), P.ck[s][k], s, k, s_fv, rs0, rc0);
-      k++;
-    }
-    for (; k < n; k++) rho_pair<false>(P, u, __ldg(u4 + i + off[k]), P.ck[s][k], s, k, s_fv, rs1, rc1);
-    const double rho = ((double)rs0 + (double)rs1) + ((double)rc0 + (double)rc1);
+    const double rho = (double)rs + (double)rc;
     const double df = dF64(P.P, code & 0x3F, rho);
     reinterpret_cast<float *>(uw + i)[3] = (float)df;
     d.rho[i] = (float)rho;
@@ -85,48 +195,105 @@ __global__ void __launch_bounds__(MX_RHO_THREADS, 1)
   }
 }
 
-template <bool ENERGY>
+// Force + velocity-Verlet pass.  Pair terms are added two at a time before one
+// compensated add.
+template <bool ENERGY, bool FIXED>
 __global__ void __launch_bounds__(MX_FORCE_THREADS, 1)
-    k_mx_force(const __grid_constant__ EnsParams P, const __grid_constant__ MxStencil S, int lat) {
-  extern __shared__ float2 s_fd[];
-  for (int k = threadIdx.x; k < 3 * P.nsm; k += blockDim.x) s_fd[k] = P.P.force32[3 * P.m_lo + k];
+    k_mx_force(const __grid_constant__ EnsParams P, const MxStencil S, int lat) {
+  extern __shared__ float2 s_ab[];
+  for (int k = threadIdx.x; k <= S.n_fs; k += blockDim.x) s_ab[k] = P.P.ab32[k];
   __syncthreads();
   const LatDesc &d = P.lats[lat];
   const bool active = lat_active(d);
   const int lane = threadIdx.x & 31;
-  const int chunks = (d.bcx + 31) / 32;
-  const long long n_items = (long long)chunks * d.by * 2 * d.bz;
-  const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+  const unsigned nwarps = blockDim.x >> 5;
   const float4 *u4 = d.u4[d.cur];
   float4 *un = d.u4[d.cur ^ 1];
+  const float2 *ptab = P.P.ps32;
+  const float c[5] = {0.f, -S.sh.a0, -2.f * S.sh.a0, -3.f * S.sh.a0, -4.f * S.sh.a0};
+  const float ha = -0.5f * S.sh.a0;
   double e_pair = 0.0, e_kin = 0.0;
-  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); active && w < n_items;
-       w += wstride) {
+  for (unsigned k = threadIdx.x >> 5;; k += nwarps) {
+    const unsigned unit = blockIdx.x + (k / MX_BRICK_ITEMS) * gridDim.x;
+    if (!active || unit >= S.walk.n_units) break;
     int s, cx, y, z;
     long long i;
-    if (!mx_site(d, chunks, w, lane, s, cx, y, z, i)) continue;
+    if (!mx_site(d, S.walk, unit, k % MX_BRICK_ITEMS, lane, s, cx, y, z, i)) continue;
     const int code = d.code[i];
     if (code < 0 || (code & MB_FLAG_ITL)) continue;
     const float4 u = __ldg(u4 + i);
-    const int *off = S.off[s];
-    float2 fs0 = make_float2(0.f, 0.f), fc0 = fs0, fs1 = fs0, fc1 = fs0;
-    float zs0 = 0.f, zc0 = 0.f, ps0 = 0.f, pc0 = 0.f, zs1 = 0.f, zc1 = 0.f, ps1 = 0.f, pc1 = 0.f;
-    const int n = P.n_st, nn = P.n_near;
-    int k = 0;
-    for (; k + 1 < nn; k += 2) {
-      const float4 nb0 = __ldg(u4 + i + off[k]), nb1 = __ldg(u4 + i + off[k + 1]);
-      force_pair<ENERGY, true>(P, u, nb0, P.ck[s][k], s, k, s_fd, fs0, fc0, zs0, zc0, ps0, pc0);
-      force_pair<ENERGY, true>(P, u, nb1, P.ck[s][k + 1], s, k + 1, s_fd, fs1, fc1, zs1, zc1, ps1, pc1);
+    float2 fs = make_float2(0.f, 0.f), fc = fs;
+    float zs = 0.f, zc = 0.f, ps = 0.f, pc = 0.f;
+    auto add2 = [&](float2 d0, float z0, float f0, float e0, float2 d1, float z1, float f1, float e1) {
+      two_sum2(fs, fc, __ffma2_rn(d1, make_float2(f1, f1), __fmul2_rn(d0, make_float2(f0, f0))));
+      two_sum(zs, zc, fmaf(z1, f1, z0 * f0));
+      if (ENERGY) two_sum(ps, pc, e0 + e1);
+    };
+    auto add1 = [&](float2 d0, float z0, float f0, float e0) {
+      two_sum2(fs, fc, __fmul2_rn(d0, make_float2(f0, f0)));
+      two_sum(zs, zc, z0 * f0);
+      if (ENERGY) two_sum(ps, pc, e0);
+    };
+    if constexpr (FIXED) {
+      const MxShells &Q = S.sh;
+      const MxSite b{u4 + i, u4 + i + Q.E + (s ? Q.d_odd : 0), Q.pl, Q.rw};
+      constexpr int nbf = 64;
+      static_for<0, nbf / 2>([&](auto pc2) {
+        constexpr int k = 2 * decltype(pc2)::value;
+        float2 d0, d1;
+        float z0, z1, e0 = 0.f, e1 = 0.f;
+        const float f0 = mxc_force<k, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d0, z0, e0);
+        const float f1 = mxc_force<k + 1, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d1, z1, e1);
+        add2(d0, z0, f0, e0, d1, z1, f1, e1);
+      });
+      static_for<nbf, 88>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        const float4 nb = mxc_load<k>(b);
+        float2 exy;
+        float ez;
+        const float num = mxc_num<k>(c, u, nb, exy, ez);
+        if (num < Q.w[HStore<k>::sh]) {
+          float2 d0;
+          float z0, e0 = 0.f;
+          const float f0 = mxc_force<k, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d0, z0, e0);
+          add1(d0, z0, f0, e0);
+        }
+      });
+    } else {
+      const float4 *be = u4 + i, *bo = u4 + i + (s ? S.d_odd : 0);
+      const float rds = S.rds_f, mmax = (float)(S.n_fs - 1);
+      auto two = [&](const MxEntry E0, const MxEntry E1, const float4 *bb) {
+        float2 d0, d1;
+        float z0, z1, e0 = 0.f, e1 = 0.f;
+        const float f0 = mx_force_term<ENERGY>(E0, rds, mmax, u, bb, s_ab, ptab, d0, z0, e0);
+        const float f1 = mx_force_term<ENERGY>(E1, rds, mmax, u, bb, s_ab, ptab, d1, z1, e1);
+        add2(d0, z0, f0, e0, d1, z1, f1, e1);
+      };
+#pragma unroll
+      for (int k = 0; k < MX_PAR_MAX; k += 2) {
+        if (k >= S.n_odd) break;
+        two(S.odd[k], S.odd[k + 1], bo);
+      }
+#pragma unroll
+      for (int k = 0; k < MX_PAR_MAX; k += 2) {
+        if (k >= S.n_even) break;
+        two(S.even[k], S.even[k + 1], be);
+      }
+      for (int k = 0; k < S.n_far; k++) {
+        const MxEntry E = S.far[k];
+        const float4 *bb = (E.odd & s) ? bo : be;
+        const float4 nb = __ldg(bb + E.off);
+        const MxPair g = mx_pair(E, E.fr_f, E.kb_f, rds, mmax, u, nb);
+        if (!g.in) continue;
+        float2 d0;
+        float z0, e0 = 0.f;
+        const float f0 = mx_force_term<ENERGY>(E, rds, mmax, u, bb, s_ab, ptab, d0, z0, e0);
+        add1(d0, z0, f0, e0);
+      }
     }
-    if (k < nn) {
-      force_pair<ENERGY, true>(P, u, __ldg(u4 + i + off[k]), P.ck[s][k], s, k, s_fd, fs0, fc0, zs0, zc0, ps0, pc0);
-      k++;
-    }
-    for (; k < n; k++)
-      force_pair<ENERGY, false>(P, u, __ldg(u4 + i + off[k]), P.ck[s][k], s, k, s_fd, fs1, fc1, zs1, zc1, ps1, pc1);
-    const double fx = ((double)fs0.x + (double)fs1.x) + ((double)fc0.x + (double)fc1.x);
-    const double fy = ((double)fs0.y + (double)fs1.y) + ((double)fc0.y + (double)fc1.y);
-    const double fz = ((double)zs0 + (double)zs1) + ((double)zc0 + (double)zc1);
+    const double fx = (double)fs.x + (double)fc.x;
+    const double fy = (double)fs.y + (double)fc.y;
+    const double fz = (double)zs + (double)zc;
     d.fx[i] = (float)fx;
     d.fy[i] = (float)fy;
     d.fz[i] = (float)fz;
@@ -138,7 +305,7 @@ __global__ void __launch_bounds__(MX_FORCE_THREADS, 1)
     }
     if (ENERGY) {
       e_kin += 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E;
-      e_pair += ((double)ps0 + (double)ps1) + ((double)pc0 + (double)pc1);
+      e_pair += (double)ps + (double)pc;
     }
     vx += P.h * fx;
     vy += P.h * fy;
@@ -201,15 +368,43 @@ __global__ void k_mx_bookkeeping(const __grid_constant__ EnsParams P) {
   }
 }
 
-int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s) {
+template <bool FIXED>
+static int mx_set_attrs() {
+  MB_CUDA(cudaFuncSetAttribute(k_mx_rho<false, FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
+  MB_CUDA(cudaFuncSetAttribute(k_mx_rho<true, FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
+  MB_CUDA(cudaFuncSetAttribute(k_mx_force<false, FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
+  MB_CUDA(cudaFuncSetAttribute(k_mx_force<true, FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
+  return MB_OK;
+}
+
+template <bool FIXED>
+static void mx_passes(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s, int which,
+                      size_t smem) {
   const int sms = device_sm_count();
-  const size_t rho_smem = (size_t)P.nsm * sizeof(float4), force_smem = (size_t)P.nsm * 3 * sizeof(float2);
+  if (which == 0) {
+    if (energy)
+      k_mx_rho<true, FIXED><<<sms, MX_RHO_THREADS, smem, s>>>(P, S, lat);
+    else
+      k_mx_rho<false, FIXED><<<sms, MX_RHO_THREADS, smem, s>>>(P, S, lat);
+  } else {
+    if (energy)
+      k_mx_force<true, FIXED><<<sms, MX_FORCE_THREADS, smem, s>>>(P, S, lat);
+    else
+      k_mx_force<false, FIXED><<<sms, MX_FORCE_THREADS, smem, s>>>(P, S, lat);
+  }
+}
+
+// ev (optional): events recorded around the density kernel (ev[0], ev[1]) and the
+// force kernel (ev[2], ev[3]).
+int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s, cudaEvent_t *ev) {
+  const int sms = device_sm_count();
+  const size_t rho_smem = (size_t)S.n_rs * sizeof(float2), force_smem = (size_t)(S.n_fs + 1) * sizeof(float2);
+  if (force_smem > MX_SMEM_MAX || rho_smem > MX_SMEM_MAX)
+    return fail(MB_ERR_ARG, "squared-distance table larger than shared memory");
   static bool attr = false;
   if (!attr) {
-    MB_CUDA(cudaFuncSetAttribute(k_mx_rho<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    MB_CUDA(cudaFuncSetAttribute(k_mx_rho<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    MB_CUDA(cudaFuncSetAttribute(k_mx_force<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    MB_CUDA(cudaFuncSetAttribute(k_mx_force<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    MB_TRY(mx_set_attrs<false>());
+    MB_TRY(mx_set_attrs<true>());
     attr = true;
   }
   const int itl_grid = 2 * sms;
@@ -217,20 +412,24 @@ int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, 
     k_mx_itl_clear<<<itl_grid, 256, 0, s>>>(P);
     k_mx_itl_mark<<<itl_grid, 256, 0, s>>>(P);
   }
-  if (energy)
-    k_mx_rho<true><<<sms, MX_RHO_THREADS, rho_smem, s>>>(P, S, lat);
+  if (ev) MB_CUDA(cudaEventRecord(ev[0], s));
+  if (S.fixed)
+    mx_passes<true>(P, S, lat, energy, s, 0, rho_smem);
   else
-    k_mx_rho<false><<<sms, MX_RHO_THREADS, rho_smem, s>>>(P, S, lat);
+    mx_passes<false>(P, S, lat, energy, s, 0, rho_smem);
+  if (ev) MB_CUDA(cudaEventRecord(ev[1], s));
   if (P.n_itl_lats > 0) {
     if (energy)
       k_mx_itl_items<false, true><<<itl_grid, 256, 0, s>>>(P);
     else
       k_mx_itl_items<false, false><<<itl_grid, 256, 0, s>>>(P);
   }
-  if (energy)
-    k_mx_force<true><<<sms, MX_FORCE_THREADS, force_smem, s>>>(P, S, lat);
+  if (ev) MB_CUDA(cudaEventRecord(ev[2], s));
+  if (S.fixed)
+    mx_passes<true>(P, S, lat, energy, s, 1, force_smem);
   else
-    k_mx_force<false><<<sms, MX_FORCE_THREADS, force_smem, s>>>(P, S, lat);
+    mx_passes<false>(P, S, lat, energy, s, 1, force_smem);
+  if (ev) MB_CUDA(cudaEventRecord(ev[3], s));
   if (P.n_itl_lats > 0) {
     if (energy)
       k_mx_itl_items<true, true><<<itl_grid, 256, 0, s>>>(P);

@@ -9,6 +9,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "mb_common.cuh"
@@ -45,6 +46,69 @@ static void knot_pieces(const double *y, int n, double dx, std::vector<double> &
     k[5] = 2.0 * c2 / dx;
     k[6] = 3.0 * c3 / dx;
   }
+}
+
+// FP64 spline value and derivative at x with the device's locate rule (index clamped to
+// the last interval, local coordinate clamped to [0, 1]).
+static void spl_eval(const std::vector<double> &c7, int n, double dx, double x, double &v, double &d) {
+  const double rdx = 1.0 / dx, pp = x * rdx;
+  int m;
+  double p;
+  if (!(pp < (double)(n - 1))) {
+    m = n - 2;
+    p = 1.0;
+  } else {
+    m = std::min((int)pp, n - 2);
+    p = std::min(pp - (double)m, 1.0);
+  }
+  const double *k = &c7[(size_t)m * 7];
+  v = ((k[3] * p + k[2]) * p + k[1]) * p + k[0];
+  d = (k[6] * p + k[5]) * p + k[4];
+}
+
+// Squared-distance tables of one type (see DevPot::fs32).  Linear interpolation in s
+// between exact knots: the force grid is twice as fine as the density grid (the
+// force sums cancel, so their relative error is amplified), which keeps the
+// interpolation error of a thermally disordered lattice near 1e-7 of the force.
+#ifndef MB_S_RHO_INTERVALS
+#define MB_S_RHO_INTERVALS 12000
+#endif
+#ifndef MB_S_FORCE_INTERVALS
+#define MB_S_FORCE_INTERVALS 24000
+#endif
+struct STables {
+  std::vector<float2> fs, ab, ps;
+  double ds_r = 0.0, ds_f = 0.0;
+};
+static void s_tables(const mb_eam_tables *t, STables &T) {
+  std::vector<double> cf, cp;
+  knot_pieces(t->f, t->nr, t->dr, cf);
+  knot_pieces(t->phi, t->nr, t->dr, cp);
+  const double rmax = std::min((double)(t->nr - 1) * t->dr, t->cutoff), smax = rmax * rmax;
+  const double rfloor = 1e-3 * t->dr; // A and B stay finite at s = 0 (pairs never get there)
+  const int nr_ = MB_S_RHO_INTERVALS, nf = MB_S_FORCE_INTERVALS;
+  T.ds_r = smax / nr_;
+  T.ds_f = smax / nf;
+  std::vector<double> kf(nr_ + 1);
+  for (int j = 0; j <= nr_; j++) {
+    double v, dv;
+    spl_eval(cf, t->nr, t->dr, sqrt((double)j * T.ds_r), v, dv);
+    kf[j] = v;
+  }
+  T.fs.resize(nr_);
+  for (int j = 0; j < nr_; j++) T.fs[j] = make_float2((float)kf[j], (float)(kf[j + 1] - kf[j]));
+  std::vector<double> kp(nf + 1);
+  T.ab.resize(nf + 1);
+  for (int j = 0; j <= nf; j++) {
+    const double r = sqrt((double)j * T.ds_f), rr = std::max(r, rfloor);
+    double f, fd, ph, phd;
+    spl_eval(cf, t->nr, t->dr, r, f, fd);
+    spl_eval(cp, t->nr, t->dr, r, ph, phd);
+    T.ab[j] = make_float2((float)(fd / rr), (float)(phd / rr));
+    kp[j] = ph;
+  }
+  T.ps.resize(nf);
+  for (int j = 0; j < nf; j++) T.ps[j] = make_float2((float)kp[j], (float)(kp[j + 1] - kp[j]));
 }
 
 int pot_build(const mb_eam_tables *t, PotHost **out) {
@@ -95,6 +159,10 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
     f_val32[i] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
   }
 
+  STables st;
+  if (nt == 1) s_tables(t, st);
+  const std::vector<float2> &fs = st.fs, &ab = st.ab, &ps = st.ps;
+
   size_t off = 0;
   auto reserve = [&](size_t bytes) {
     size_t o = off;
@@ -105,7 +173,9 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
                o_Fv = reserve(F_val.size() * sizeof(double4)), o_Fd = reserve(F_der.size() * sizeof(double4)),
                o_pv = reserve(phi_val.size() * sizeof(double4)), o_pd = reserve(phi_der.size() * sizeof(double4)),
                o_f1 = reserve(force1.size() * sizeof(double2)), o_fv32 = reserve(f_val32.size() * sizeof(float4)),
-               o_f32 = reserve(force32.size() * sizeof(float2)), o_pv32 = reserve(phi_val32.size() * sizeof(float4));
+               o_f32 = reserve(force32.size() * sizeof(float2)), o_pv32 = reserve(phi_val32.size() * sizeof(float4)),
+               o_fs = reserve(fs.size() * sizeof(float2)), o_ab = reserve(ab.size() * sizeof(float2)),
+               o_ps = reserve(ps.size() * sizeof(float2));
   PotHost *p = new PotHost();
   cudaError_t e = cudaMalloc(&p->blob, off);
   if (e != cudaSuccess) {
@@ -124,6 +194,11 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
   memcpy(&staging[o_fv32], f_val32.data(), f_val32.size() * sizeof(float4));
   memcpy(&staging[o_f32], force32.data(), force32.size() * sizeof(float2));
   memcpy(&staging[o_pv32], phi_val32.data(), phi_val32.size() * sizeof(float4));
+  if (!fs.empty()) {
+    memcpy(&staging[o_fs], fs.data(), fs.size() * sizeof(float2));
+    memcpy(&staging[o_ab], ab.data(), ab.size() * sizeof(float2));
+    memcpy(&staging[o_ps], ps.data(), ps.size() * sizeof(float2));
+  }
   e = cudaMemcpy(p->blob, staging.data(), off, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     cudaFree(p->blob);
@@ -148,6 +223,13 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
   d.f_val32 = (const float4 *)(b + o_fv32);
   d.force32 = (const float2 *)(b + o_f32);
   d.phi_val32 = (const float4 *)(b + o_pv32);
+  d.n_rs = (int)fs.size();
+  d.ds_r = st.ds_r;
+  d.fs32 = fs.empty() ? nullptr : (const float2 *)(b + o_fs);
+  d.n_fs = (int)ps.size();
+  d.ds_f = st.ds_f;
+  d.ab32 = fs.empty() ? nullptr : (const float2 *)(b + o_ab);
+  d.ps32 = fs.empty() ? nullptr : (const float2 *)(b + o_ps);
   *out = p;
   return MB_OK;
 }

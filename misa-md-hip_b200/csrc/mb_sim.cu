@@ -651,13 +651,9 @@ int mb_sim_time_steps(mb_sim *s, int32_t nsteps, float *ms) {
 }
 
 int mb_sim_kernel_times(mb_sim *s, float *rho_ms, float *force_ms) {
-  if (s && s->ens) { // both passes run inside the one persistent step kernel
+  if (s && s->ens) { // split kernels: each pass timed; persistent kernel: the whole step
     MB_TRY(mixed_need_slot(s));
-    float ms = 0.f;
-    MB_TRY(mb_ensemble_time(s->ens, 4, &ms));
-    if (rho_ms) *rho_ms = 0.f;
-    if (force_ms) *force_ms = ms / 4;
-    return MB_OK;
+    return mb_ensemble_kernel_times(s->ens, rho_ms, force_ms, nullptr);
   }
   if (!s) return fail(MB_ERR_ARG, "null sim");
   if (!s->primed) MB_TRY(prime(s, 0));
