@@ -66,8 +66,8 @@ struct DevPot {
   const float2 *force32;   // single type: [nr][3] {f d0, phi d0}, {f d1, phi d1}, {f d2, phi d2}
   const float4 *phi_val32; // single type: [nr]
   // single type, squared-distance form for the mixed split kernels, on uniform grids in
-  // s = r^2 whose knots carry the FP64 r-spline evaluated exactly; values in between
-  // are interpolated linearly.  Density: per interval {f(s_j), f(s_j+1) - f(s_j)}.
+  // s = r^2, built from the FP64 r-spline and interpolated linearly.  Density: per
+  // interval {value at s_j, rise over the interval}.
   // Force: per knot {A, B} = {f'(r) / r, phi'(r) / r} (knot pairs are read, which
   // halves the table against per-interval storage and allows a finer grid).
   // n_rs = n_fs = 0 when not built (several types).
@@ -77,7 +77,7 @@ struct DevPot {
   int n_fs;            // force intervals
   double ds_f;
   const float2 *ab32;  // [n_fs + 1] knots
-  const float2 *ps32;  // [n_fs] per interval {phi, d phi} (energy steps)
+  const float4 *ps32;  // [n_fs] per interval cubic of phi in p (energy steps)
 };
 
 struct PotHost;

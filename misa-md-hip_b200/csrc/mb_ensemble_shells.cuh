@@ -140,7 +140,7 @@ __device__ __forceinline__ float2 mx_ab(const float2 *tab, int m, float q) {
 // fpair and pair vector d = C + e of vector K (fpair 0 beyond the cutoff).
 template <int K, bool ENERGY>
 __device__ __forceinline__ float mxc_force(const MxShells &Q, const float (&c)[5], float ha, const MxSite &b,
-                                           const float4 &u, const float2 *tab, const float2 *ptab, float2 &dxy,
+                                           const float4 &u, const float2 *tab, const float4 *ptab, float2 &dxy,
                                            float &dz, float &e) {
   using T = HStore<K>;
   const float4 nb = mxc_load<K>(b);
@@ -155,8 +155,8 @@ __device__ __forceinline__ float mxc_force(const MxShells &Q, const float (&c)[5
                     T::h.hy ? fmaf(ha, (float)T::h.hy, exy.y) : exy.y);
   dz = T::h.hz ? fmaf(ha, (float)T::h.hz, ez) : ez;
   if (ENERGY) {
-    const float2 p = __ldg(ptab + m);
-    const float v = 0.5f * fmaf(p.y, q, p.x);
+    const float4 p = __ldg(ptab + m);
+    const float v = 0.5f * fmaf(fmaf(fmaf(p.w, q, p.z), q, p.y), q, p.x);
     e = in ? v : 0.f;
   }
   return in ? fp : 0.f;

@@ -94,7 +94,7 @@ __device__ __forceinline__ float mx_rho_term(const MxEntry E, float rds, float m
 // vector.
 template <bool ENERGY>
 __device__ __forceinline__ float mx_force_term(const MxEntry E, float rds, float mmax, const float4 &u,
-                                               const float4 *base, const float2 *tab, const float2 *ptab,
+                                               const float4 *base, const float2 *tab, const float4 *ptab,
                                                float2 &dxy, float &dz, float &e) {
   const float4 nb = __ldg(base + E.off);
   const MxPair g = mx_pair(E, E.fr_f, E.kb_f, rds, mmax, u, nb);
@@ -103,8 +103,8 @@ __device__ __forceinline__ float mx_force_term(const MxEntry E, float rds, float
   dxy = make_float2(g.exy.x + E.c.x, g.exy.y + E.c.y);
   dz = g.ez + E.c.z;
   if (ENERGY) {
-    const float2 p = __ldg(ptab + g.m);
-    const float v = 0.5f * fmaf(p.y, g.q, p.x);
+    const float4 p = __ldg(ptab + g.m);
+    const float v = 0.5f * fmaf(fmaf(fmaf(p.w, g.q, p.z), g.q, p.y), g.q, p.x);
     e = g.in ? v : 0.f;
   }
   return g.in ? fp : 0.f;
@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(MX_FORCE_THREADS, 1)
   const unsigned nwarps = blockDim.x >> 5;
   const float4 *u4 = d.u4[d.cur];
   float4 *un = d.u4[d.cur ^ 1];
-  const float2 *ptab = P.P.ps32;
+  const float4 *ptab = P.P.ps32;
   const float c[5] = {0.f, -S.sh.a0, -2.f * S.sh.a0, -3.f * S.sh.a0, -4.f * S.sh.a0};
   const float ha = -0.5f * S.sh.a0;
   double e_pair = 0.0, e_kin = 0.0;

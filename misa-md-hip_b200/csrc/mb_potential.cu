@@ -66,18 +66,33 @@ static void spl_eval(const std::vector<double> &c7, int n, double dx, double x, 
   d = (k[6] * p + k[5]) * p + k[4];
 }
 
-// Squared-distance tables of one type (see DevPot::fs32).  Linear interpolation in s
-// between exact knots: the force grid is twice as fine as the density grid (the
-// force sums cancel, so their relative error is amplified), which keeps the
-// interpolation error of a thermally disordered lattice near 1e-7 of the force.
+// Cubic in p through (0, v0), (1/3, v1), (2/3, v2), (1, v3) (forward differences).
+static void fit4(const double v[4], double c[4]) {
+  const double d1 = v[1] - v[0], d2 = v[2] - 2.0 * v[1] + v[0], d3 = v[3] - 3.0 * v[2] + 3.0 * v[1] - v[0];
+  c[0] = v[0];
+  c[1] = 3.0 * (d1 - 0.5 * d2 + d3 / 3.0);
+  c[2] = 4.5 * (d2 - d3);
+  c[3] = 4.5 * d3;
+}
+
+// Squared-distance tables of one type (see DevPot::fs32), from the FP64 r-spline.
+//  * density: one line per interval, the chord lowered by 2/3 of its midpoint gap (the
+//    least-squares line of a locally quadratic function), so that the interpolation
+//    error has zero mean and the density and embedding energy carry no bias;
+//  * force: knot values of f'(r)/r and phi'(r)/r, linear in between, on a grid three
+//    times finer than the density grid (force sums cancel, which amplifies relative
+//    error): about 1e-7 of the force for a thermally disordered lattice;
+//  * pair energy (energy steps only, read from global memory): a cubic per interval
+//    through four exact points.
 #ifndef MB_S_RHO_INTERVALS
-#define MB_S_RHO_INTERVALS 12000
+#define MB_S_RHO_INTERVALS 8000
 #endif
 #ifndef MB_S_FORCE_INTERVALS
 #define MB_S_FORCE_INTERVALS 24000
 #endif
 struct STables {
-  std::vector<float2> fs, ab, ps;
+  std::vector<float2> fs, ab;
+  std::vector<float4> ps;
   double ds_r = 0.0, ds_f = 0.0;
 };
 static void s_tables(const mb_eam_tables *t, STables &T) {
@@ -89,15 +104,17 @@ static void s_tables(const mb_eam_tables *t, STables &T) {
   const int nr_ = MB_S_RHO_INTERVALS, nf = MB_S_FORCE_INTERVALS;
   T.ds_r = smax / nr_;
   T.ds_f = smax / nf;
-  std::vector<double> kf(nr_ + 1);
-  for (int j = 0; j <= nr_; j++) {
+  auto fval = [&](const std::vector<double> &c, double s) {
     double v, dv;
-    spl_eval(cf, t->nr, t->dr, sqrt((double)j * T.ds_r), v, dv);
-    kf[j] = v;
-  }
+    spl_eval(c, t->nr, t->dr, sqrt(s), v, dv);
+    return v;
+  };
   T.fs.resize(nr_);
-  for (int j = 0; j < nr_; j++) T.fs[j] = make_float2((float)kf[j], (float)(kf[j + 1] - kf[j]));
-  std::vector<double> kp(nf + 1);
+  for (int j = 0; j < nr_; j++) {
+    const double a = fval(cf, j * T.ds_r), b = fval(cf, (j + 1) * T.ds_r), mid = fval(cf, (j + 0.5) * T.ds_r);
+    const double lift = (2.0 / 3.0) * (0.5 * (a + b) - mid);
+    T.fs[j] = make_float2((float)(a - lift), (float)(b - a));
+  }
   T.ab.resize(nf + 1);
   for (int j = 0; j <= nf; j++) {
     const double r = sqrt((double)j * T.ds_f), rr = std::max(r, rfloor);
@@ -105,10 +122,14 @@ static void s_tables(const mb_eam_tables *t, STables &T) {
     spl_eval(cf, t->nr, t->dr, r, f, fd);
     spl_eval(cp, t->nr, t->dr, r, ph, phd);
     T.ab[j] = make_float2((float)(fd / rr), (float)(phd / rr));
-    kp[j] = ph;
   }
   T.ps.resize(nf);
-  for (int j = 0; j < nf; j++) T.ps[j] = make_float2((float)kp[j], (float)(kp[j + 1] - kp[j]));
+  for (int j = 0; j < nf; j++) {
+    double v[4], c[4];
+    for (int q = 0; q < 4; q++) v[q] = fval(cp, (j + q / 3.0) * T.ds_f);
+    fit4(v, c);
+    T.ps[j] = make_float4((float)c[0], (float)c[1], (float)c[2], (float)c[3]);
+  }
 }
 
 int pot_build(const mb_eam_tables *t, PotHost **out) {
@@ -161,7 +182,8 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
 
   STables st;
   if (nt == 1) s_tables(t, st);
-  const std::vector<float2> &fs = st.fs, &ab = st.ab, &ps = st.ps;
+  const std::vector<float2> &fs = st.fs, &ab = st.ab;
+  const std::vector<float4> &ps = st.ps;
 
   size_t off = 0;
   auto reserve = [&](size_t bytes) {
@@ -175,7 +197,7 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
                o_f1 = reserve(force1.size() * sizeof(double2)), o_fv32 = reserve(f_val32.size() * sizeof(float4)),
                o_f32 = reserve(force32.size() * sizeof(float2)), o_pv32 = reserve(phi_val32.size() * sizeof(float4)),
                o_fs = reserve(fs.size() * sizeof(float2)), o_ab = reserve(ab.size() * sizeof(float2)),
-               o_ps = reserve(ps.size() * sizeof(float2));
+               o_ps = reserve(ps.size() * sizeof(float4));
   PotHost *p = new PotHost();
   cudaError_t e = cudaMalloc(&p->blob, off);
   if (e != cudaSuccess) {
@@ -197,7 +219,7 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
   if (!fs.empty()) {
     memcpy(&staging[o_fs], fs.data(), fs.size() * sizeof(float2));
     memcpy(&staging[o_ab], ab.data(), ab.size() * sizeof(float2));
-    memcpy(&staging[o_ps], ps.data(), ps.size() * sizeof(float2));
+    memcpy(&staging[o_ps], ps.data(), ps.size() * sizeof(float4));
   }
   e = cudaMemcpy(p->blob, staging.data(), off, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
@@ -229,7 +251,7 @@ int pot_build(const mb_eam_tables *t, PotHost **out) {
   d.n_fs = (int)ps.size();
   d.ds_f = st.ds_f;
   d.ab32 = fs.empty() ? nullptr : (const float2 *)(b + o_ab);
-  d.ps32 = fs.empty() ? nullptr : (const float2 *)(b + o_ps);
+  d.ps32 = fs.empty() ? nullptr : (const float4 *)(b + o_ps);
   *out = p;
   return MB_OK;
 }
