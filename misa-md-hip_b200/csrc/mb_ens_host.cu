@@ -20,13 +20,9 @@ int ens_launch(const EnsParams &P, int grid, cudaStream_t s);
 int ens_max_grid(int nsm);
 int ens_energy_launch(const LatDesc *lats, int n, const int *tile_first, const double *epart, double *out,
                       cudaStream_t s);
-int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s,
-                   cudaEvent_t *ev = nullptr);
-int mx_energy_launch(const LatDesc *lats, int lat, const double *epart, double *out, cudaStream_t s);
-int mx_grid();
+int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s, cudaEvent_t *ev,
+                   double *out);
 
-// Split mode (separate rho / force kernels) pays off for one large lattice.
-static const long long kSplitMinSites = 1LL << 19;
 
 static const int kShapes[ENS_NSHAPE][3] = {{16, 4, 4}, {8, 8, 4}, {8, 4, 8}, {4, 8, 8}};
 
@@ -190,8 +186,11 @@ struct mb_ensemble {
   cudaGraphExec_t graph = nullptr;
   bool graphs_ok = true;
   int policy = -1; // -1: size model per lattice; 0..3: one shape for all
-  int mode = 0;    // 0: split kernels for a single large lattice, else persistent; 1: persistent; 2: split
-  bool split = false;
+  int mode = 0;  // 0: split kernels when the built-in shells apply, else persistent; 1: persistent; 2: split
+  int split = 0; // kernels in use: 0 persistent, 1 split with the brick walk, 2 split with the linear walk
+  unsigned *d_item_first = nullptr; // linear walk: first item of each lattice
+  double *d_epart_items = nullptr;  // split: energy partials per walk item
+  size_t cap_items = 0;
   mb::MxStencil mxs{};
   size_t device_bytes = 0;
   size_t fixed_bytes = 0;
@@ -387,11 +386,12 @@ static int rebuild(mb_ensemble *e) {
   const size_t need_l = std::max(1, nl), need_t = std::max<size_t>(1, tile_lat.size());
   if (need_l > e->cap_lats) {
     const size_t C = std::max<size_t>({need_l, 2 * e->cap_lats, 16});
-    void **arrs[] = {(void **)&e->d_lats, (void **)&e->d_tmaps, (void **)&e->d_itl_lats, (void **)&e->d_tile_first,
-                     (void **)&e->d_eout, (void **)&e->d_eitl};
+    void **arrs[] = {(void **)&e->d_lats, (void **)&e->d_tmaps,     (void **)&e->d_itl_lats,
+                     (void **)&e->d_tile_first, (void **)&e->d_eout, (void **)&e->d_eitl,
+                     (void **)&e->d_item_first};
     const size_t per[] = {sizeof(LatDesc), 2 * sizeof(CUtensorMap), sizeof(int), sizeof(int), 2 * sizeof(double),
-                          2 * sizeof(double)};
-    for (int a = 0; a < 6; a++) {
+                          2 * sizeof(double), sizeof(unsigned)};
+    for (int a = 0; a < 7; a++) {
       if (*arrs[a]) {
         cudaFree(*arrs[a]);
         e->device_bytes -= (e->cap_lats + 1) * per[a];
@@ -449,20 +449,55 @@ static int rebuild(mb_ensemble *e) {
   P.bar = e->d_bar;
   P.err = e->d_err;
   e->grid = std::max(1, std::min(e->max_grid, e->n_tiles));
-  // split mode: one lattice, big enough for separate full-occupancy kernels
-  e->split = false;
-  if (nl == 1) {
-    const LatDesc &d = descs[0];
-    const long long sites = 2LL * d.bcx * d.by * d.bz;
-    e->split = e->mode == 2 || (e->mode == 0 && sites >= kSplitMinSites);
-    if (e->split && e->cap_tiles < (size_t)mx_grid()) e->split = false; // one energy partial per CTA
-    if (e->split) {
-      const char *why = mx_stencil(e, d, e->mxs);
-      if (why) {
-        e->split = false;
-        if (e->mode == 2) return fail(MB_ERR_UNSUPPORTED, why);
-      }
+  // kernel structure: split kernels whenever their stencil applies (unless the
+  // persistent kernel is asked for); one lattice at least a chunk wide walks bricks
+  e->split = 0;
+  if (nl >= 1 && e->mode != 1) {
+    const char *why = mx_stencil(e, descs[0], e->mxs);
+    for (int c = 0; c < nl && !why; c++)
+      if (descs[c].bcx > 2047 || descs[c].by > 2047 || descs[c].bz > 511)
+        why = "split kernels take lattices of at most 2047 x 2047 x 511 cells";
+    if (!why && nl > 1 && !e->mxs.fixed) why = "split kernels over several lattices need the built-in BCC shells";
+    if (why) {
+      if (e->mode == 2) return fail(MB_ERR_UNSUPPORTED, why);
+    } else {
+      e->split = (nl == 1 && (descs[0].bcx >= 32 || !e->mxs.fixed)) ? 1 : 2;
     }
+  }
+  if (e->split) {
+    MxWalk &W = e->mxs.walk;
+    W.linear = e->split == 2;
+    W.n_lats = nl;
+    std::vector<unsigned> first(nl + 1, 0);
+    unsigned long long n_items = 0;
+    if (W.linear) {
+      for (int c = 0; c < nl; c++) {
+        const LatDesc &d = descs[c];
+        first[c] = (unsigned)n_items;
+        n_items += 2ull * d.bz * (((unsigned long long)d.bcx * d.by + 31) / 32);
+      }
+      first[nl] = (unsigned)n_items;
+    } else {
+      n_items = (unsigned long long)W.n_units * MX_BRICK_ITEMS;
+    }
+      if (n_items >= (1ull << 31)) return fail(MB_ERR_ARG, "too many sites for the 32-bit item walk");
+    W.n_items = (unsigned)n_items;
+    if (n_items > e->cap_items) {
+      const size_t C = std::max<size_t>((size_t)n_items, 2 * e->cap_items);
+      if (e->d_epart_items) {
+        cudaFree(e->d_epart_items);
+        e->device_bytes -= e->cap_items * 2 * sizeof(double);
+        e->fixed_bytes -= e->cap_items * 2 * sizeof(double);
+      }
+      e->d_epart_items = nullptr;
+      MB_TRY(edalloc(e, (void **)&e->d_epart_items, C * 2 * sizeof(double)));
+      e->cap_items = C;
+    }
+    MB_CUDA(cudaMemcpyAsync(e->d_item_first, first.data(), sizeof(unsigned) * (nl + 1), cudaMemcpyHostToDevice,
+                            e->stream));
+    MB_CUDA(cudaStreamSynchronize(e->stream));
+    W.item_first = e->d_item_first;
+    P.epart = e->d_epart_items;
   }
   e->dirty = false;
   return MB_OK;
@@ -605,8 +640,7 @@ static int launch_step(mb_ensemble *e, int energy) {
     MB_CUDA(cudaMemsetAsync(e->d_eitl, 0, sizeof(double) * 2 * e->order.size(), e->stream));
     P.energy = 1;
     if (e->split) {
-      MB_TRY(mx_launch_step(P, e->mxs, 0, 1, e->stream));
-      MB_TRY(mx_energy_launch(e->d_lats, 0, e->d_epart, e->d_eout, e->stream));
+      MB_TRY(mx_launch_step(P, e->mxs, 0, 1, e->stream, nullptr, e->d_eout));
     } else {
       MB_TRY(ens_launch(P, e->grid, e->stream));
       MB_TRY(ens_energy_launch(e->d_lats, (int)e->order.size(), e->d_tile_first, e->d_epart, e->d_eout, e->stream));
@@ -621,7 +655,8 @@ static int launch_step(mb_ensemble *e, int energy) {
       cudaGraph_t g = nullptr;
       cudaError_t r = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
       if (r == cudaSuccess) {
-        const int rc = e->split ? mx_launch_step(P, e->mxs, 0, 0, e->stream) : ens_launch(P, e->grid, e->stream);
+        const int rc =
+            e->split ? mx_launch_step(P, e->mxs, 0, 0, e->stream, nullptr, nullptr) : ens_launch(P, e->grid, e->stream);
         r = cudaStreamEndCapture(e->stream, &g);
         if (rc == MB_OK && r == cudaSuccess && g) {
           if (cudaGraphInstantiate(&e->graph, g, 0) != cudaSuccess) e->graph = nullptr;
@@ -638,7 +673,7 @@ static int launch_step(mb_ensemble *e, int energy) {
     }
   }
   if (e->split)
-    MB_TRY(mx_launch_step(P, e->mxs, 0, 0, e->stream));
+    MB_TRY(mx_launch_step(P, e->mxs, 0, 0, e->stream, nullptr, nullptr));
   else
     MB_TRY(ens_launch(P, e->grid, e->stream));
   e->launches++;
@@ -781,7 +816,8 @@ int mb_ensemble_destroy(mb_ensemble *e) {
   drop_graph(e);
   for (auto &L : e->slots) free_slot(e, L);
   void *ptrs[] = {e->d_lats, e->d_tile_lat, e->d_tile_idx, e->d_tile_first, e->d_itl_lats, e->d_tmaps,
-                  e->d_epart, e->d_eout, e->d_eitl, e->d_bar, e->d_err, e->d_bad};
+                  e->d_epart, e->d_eout, e->d_eitl, e->d_bar, e->d_err, e->d_bad, e->d_item_first,
+                  e->d_epart_items};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &ev : e->ev)
@@ -1150,7 +1186,7 @@ int mb_ensemble_kernel_times(mb_ensemble *e, float *rho_ms, float *force_ms, int
   e->P.energy = 0;
   for (int k = 0; k < reps; k++) {
     if (e->split) {
-      MB_TRY(mx_launch_step(e->P, e->mxs, 0, 0, e->stream, e->ev + 2));
+      MB_TRY(mx_launch_step(e->P, e->mxs, 0, 0, e->stream, e->ev + 2, nullptr));
     } else {
       MB_CUDA(cudaEventRecord(e->ev[4], e->stream));
       MB_TRY(ens_launch(e->P, e->grid, e->stream));

@@ -110,17 +110,25 @@ struct MxEntry {
   int pad_[3];
 };
 
-// Walk of the split kernels: the box is cut into bricks of one x chunk (32 sites, one
-// per lane) by MX_BY rows by MX_BZ planes by both sublattices; a block takes whole
-// bricks (brick b, b + grid, ...) so the rows its warps read overlap and stay in L1.
-// Brick index -> (chunk, y brick, z brick) by multiply-high divisions.
+// Walks of the split kernels.  One large lattice: the box is cut into bricks of one x
+// chunk (32 sites, one per lane) by MX_BY rows by MX_BZ planes by both sublattices; a
+// block takes whole bricks (brick b, b + grid, ...) so the rows its warps read overlap
+// and stay in L1.  Many lattices: every lattice's (z, sublattice) planes are cut into
+// items of 32 consecutive sites (rows of small lattices share a warp) and each block
+// walks one contiguous range of the concatenated items.
 #define MX_BY 8
 #define MX_BZ 8
 #define MX_BRICK_ITEMS (2 * MX_BY * MX_BZ)
 struct MxWalk {
+  int linear;                // 0: bricks of lattice `lat`; 1: linear items over every lattice
   unsigned chunks, m_chunks; // x chunks per row and floor((2^32 - 1) / chunks)
   unsigned nyb, m_nyb;       // y bricks
   unsigned n_units;          // bricks
+  // linear walk: item = 32 consecutive sites of one (z, sublattice) plane of a lattice,
+  // planes ordered z-major; lattice l owns items [item_first[l], item_first[l + 1])
+  const unsigned *item_first;
+  unsigned n_items; // every walk: items (energy partials)
+  int n_lats;
 };
 
 // Split-mode stencil built into the kernel: the BCC neighbour shells up to |h|^2 = 19

@@ -1,14 +1,15 @@
-// Mixed-precision step of ONE large lattice as separate kernels (split mode).
+// Mixed-precision step as separate kernels (split mode).
 //
 // The persistent tile kernel (mb_ensemble.cu) keeps both passes, both spline tables
-// and two TMA tile buffers resident, which caps it at 16 warps per SM.  A single
-// large lattice does not need that: here the density pass and the force + velocity-
-// Verlet pass are separate kernels, each holding only its own FP32 table in shared
-// memory and reading neighbour rows through L1 (sublattice rows are contiguous), so
-// each runs with 24-32 warps per SM.  The pair arithmetic (displacement-relative
-// spline index, f32x2 lanes, two-sum accumulation) is the tile kernel's, so results
-// agree with it to rounding of the summation order.  The kernels of one step are
-// captured into one CUDA graph by the ensemble host.
+// and two TMA tile buffers resident, which caps it at 16 warps per SM.  Here the
+// density pass and the force + velocity-Verlet pass are separate kernels, each holding
+// only its own squared-distance table in shared memory and reading neighbour rows
+// through L1, so each runs with 24-32 warps per SM.  Pair terms are FP32 (linear
+// interpolation in s = r^2 of tables built from the FP64 spline, index from the small
+// quantity r^2 - R^2) with two-sum accumulation; state and integration stay FP64.
+// The kernels of one step (interstitial phases included) are captured into one CUDA
+// graph by the ensemble host.  One large lattice is walked by bricks, many lattices by
+// linear items (MxWalk).
 #include "mb_ensemble_kernel.cuh"
 #include "mb_ensemble_pair.cuh"
 #include "mb_ensemble_shells.cuh"
@@ -110,224 +111,334 @@ __device__ __forceinline__ float mx_force_term(const MxEntry E, float rds, float
   return g.in ? fp : 0.f;
 }
 
-// Density pass.  FIXED: the built-in BCC shells (MxShells); else the runtime stencil.
+// Site addressed by walk item `item` of this warp: brick walk (lattice `lat`) or linear
+// walk (lattice found from item_first; `l`, `lo`, `hi` cache the current lattice).
+struct MxAt {
+  int l;
+  unsigned lo, hi;
+};
+
+template <int WALK>
+__device__ __forceinline__ bool mx_locate(const EnsParams &P, const MxWalk &W, int lat, unsigned item, int lane,
+                                          MxAt &at, int &s, int &cx, int &y, int &z, long long &i) {
+  if constexpr (WALK == 0) {
+    at.l = lat;
+    return mx_site(P.lats[lat], W, item / MX_BRICK_ITEMS, item % MX_BRICK_ITEMS, lane, s, cx, y, z, i);
+  } else {
+    if (item < at.lo || item >= at.hi) { // binary search of the owning lattice
+      int a = 0, b = W.n_lats;
+      while (b - a > 1) {
+        const int m = (a + b) >> 1;
+        if (__ldg(W.item_first + m) <= item)
+          a = m;
+        else
+          b = m;
+      }
+      at.l = a;
+      at.lo = __ldg(W.item_first + a);
+      at.hi = __ldg(W.item_first + a + 1);
+    }
+    const LatDesc &d = P.lats[at.l];
+    const unsigned plane_sites = (unsigned)(d.bcx * d.by), cpp = (plane_sites + 31u) / 32u;
+    const unsigned j = item - at.lo, plane = j / cpp, b = (j - plane * cpp) * 32u + (unsigned)lane;
+    if (b >= plane_sites) return false;
+    s = (int)(plane & 1u);
+    z = (int)(plane >> 1);
+    y = (int)(b / (unsigned)d.bcx);
+    cx = (int)(b - (unsigned)y * (unsigned)d.bcx);
+    i = (long long)s * d.E + ((long long)(z + 2) * d.ey + y + 2) * d.ecx + cx + 2;
+    return true;
+  }
+}
+
+// Items of this block: bricks b, b + grid, ... (walk 0) or one contiguous range (walk 1).
+template <int WALK>
+__device__ __forceinline__ void mx_items(const MxWalk &W, unsigned &first, unsigned &count) {
+  if constexpr (WALK == 0) {
+    first = 0;
+    count = 0;
+  } else {
+    const unsigned q = W.n_items / gridDim.x, r = W.n_items % gridDim.x;
+    first = blockIdx.x * q + min(blockIdx.x, r);
+    count = q + (blockIdx.x < r ? 1u : 0u);
+  }
+}
+
+// Brick walk: the k-th item of this block (k = warp, warp + warps, ...) is item it of
+// brick blockIdx.x + (k / MX_BRICK_ITEMS) * grid.  Returns the walk item or ~0u at the end.
+template <int WALK>
+__device__ __forceinline__ unsigned mx_next(const MxWalk &W, unsigned k, unsigned first, unsigned count) {
+  if constexpr (WALK == 0) {
+    const unsigned unit = blockIdx.x + (k / MX_BRICK_ITEMS) * gridDim.x;
+    return unit < W.n_units ? unit * MX_BRICK_ITEMS + k % MX_BRICK_ITEMS : ~0u;
+  } else {
+    return k < count ? first + k : ~0u;
+  }
+}
+
+// Strided views of lattice d for the built-in shells.
+__device__ __forceinline__ MxSite mx_site_bases(const LatDesc &d, const float4 *u4, long long i, int s) {
+  const long long E = d.E, d_odd = -2 * E + (long long)(d.ey + 1) * d.ecx + 1;
+  return MxSite{u4 + i, u4 + i + E + (s ? d_odd : 0), d.ey * d.ecx, d.ecx};
+}
+
+// Density and df of one site; returns F(rho) for the energy.
+// Site coordinates packed into one register across the pair loops: cx (11 bits),
+// y (11), z (9), sublattice (1).
+__device__ __forceinline__ unsigned mx_pack(int s, int cx, int y, int z) {
+  return (unsigned)cx | ((unsigned)y << 11) | ((unsigned)z << 22) | ((unsigned)s << 31);
+}
+__device__ __forceinline__ void mx_unpack(unsigned p, int &s, int &cx, int &y, int &z) {
+  cx = (int)(p & 2047u);
+  y = (int)((p >> 11) & 2047u);
+  z = (int)((p >> 22) & 511u);
+  s = (int)(p >> 31);
+}
+
 template <bool ENERGY, bool FIXED>
+__device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStencil &S, const LatDesc &d,
+                                              const float2 *s_f, const float (&c)[5], long long i, unsigned pos) {
+  const int s = (int)(pos >> 31);
+  const int code = d.code[i];
+  if (code < 0 || (code & MB_FLAG_ITL)) return 0.0;
+  const float4 *u4 = d.u4[d.cur];
+  float4 *uw = d.u4[d.cur];
+  const float4 u = __ldg(u4 + i);
+  float rs = 0.f, rc = 0.f;
+  if constexpr (FIXED) {
+    const MxShells &Q = S.sh;
+    const MxSite b = mx_site_bases(d, u4, i, s);
+    constexpr int nbf = 64; // shells 1-6, walked without a branch; shell 7 with one
+    static_for<0, nbf / 2>([&](auto pc) {
+      constexpr int k = 2 * decltype(pc)::value;
+      two_sum(rs, rc, mxc_rho<k>(Q, c, b, u, s_f) + mxc_rho<k + 1>(Q, c, b, u, s_f));
+    });
+    static_for<nbf, 88>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
+      const float4 nb = mxc_load<k>(b);
+      float2 exy;
+      float ez, q;
+      const float num = mxc_num<k>(c, u, nb, exy, ez);
+      if (num < Q.w[HStore<k>::sh]) {
+        const int m = mxc_index<k, 0>(Q, num, q);
+        const float2 t = s_f[m];
+        two_sum(rs, rc, fmaf(t.y, q, t.x));
+      }
+    });
+  } else {
+    const float4 *be = u4 + i, *bo = u4 + i + (s ? S.d_odd : 0);
+    const float rds = S.rds, mmax = (float)(S.n_rs - 1);
+#pragma unroll
+    for (int k = 0; k < MX_PAR_MAX; k += 2) {
+      if (k >= S.n_odd) break;
+      two_sum(rs, rc,
+              mx_rho_term(S.odd[k], rds, mmax, u, bo, s_f) + mx_rho_term(S.odd[k + 1], rds, mmax, u, bo, s_f));
+    }
+#pragma unroll
+    for (int k = 0; k < MX_PAR_MAX; k += 2) {
+      if (k >= S.n_even) break;
+      two_sum(rs, rc,
+              mx_rho_term(S.even[k], rds, mmax, u, be, s_f) + mx_rho_term(S.even[k + 1], rds, mmax, u, be, s_f));
+    }
+    for (int k = 0; k < S.n_far; k++) {
+      const MxEntry E = S.far[k];
+      const float4 *bb = (E.odd & s) ? bo : be;
+      const float4 nb = __ldg(bb + E.off);
+      const MxPair g = mx_pair(E, E.t.w, E.kb, rds, mmax, u, nb);
+      if (!g.in) continue;
+      const float2 t = s_f[g.m];
+      two_sum(rs, rc, fmaf(t.y, g.q, t.x));
+    }
+  }
+  const double rho = (double)rs + (double)rc;
+  const double df = dF64(P.P, code & 0x3F, rho);
+  reinterpret_cast<float *>(uw + i)[3] = (float)df;
+  d.rho[i] = (float)rho;
+  int sx, cx, y, z;
+  mx_unpack(pos, sx, cx, y, z);
+  const Geom g = lat_geom(d);
+  for_images(g, sx, cx, y, z,
+             [&](long long idx, double, double, double) { reinterpret_cast<float *>(uw + idx)[3] = (float)df; });
+  return ENERGY ? F64(P.P, code & 0x3F, rho) : 0.0;
+}
+
+// Force + velocity-Verlet of one site; adds pair energy and kinetic energy.  Pair terms
+// are added two at a time before one compensated add.
+template <bool ENERGY, bool FIXED>
+__device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStencil &S, const LatDesc &d,
+                                              const float2 *s_ab, const float (&c)[5], long long i, unsigned pos,
+                                              double &e_pair, double &e_kin) {
+  const int s = (int)(pos >> 31);
+  const int code = d.code[i];
+  if (code < 0 || (code & MB_FLAG_ITL)) return;
+  const float4 *u4 = d.u4[d.cur];
+  float4 *un = d.u4[d.cur ^ 1];
+  const float4 *ptab = P.P.ps32;
+  const float4 u = __ldg(u4 + i);
+  float2 fs = make_float2(0.f, 0.f), fc = fs;
+  float zs = 0.f, zc = 0.f, ps = 0.f, pc = 0.f;
+  auto add2 = [&](float2 d0, float z0, float f0, float e0, float2 d1, float z1, float f1, float e1) {
+    two_sum2(fs, fc, __ffma2_rn(d1, make_float2(f1, f1), __fmul2_rn(d0, make_float2(f0, f0))));
+    two_sum(zs, zc, fmaf(z1, f1, z0 * f0));
+    if (ENERGY) two_sum(ps, pc, e0 + e1);
+  };
+  auto add1 = [&](float2 d0, float z0, float f0, float e0) {
+    two_sum2(fs, fc, __fmul2_rn(d0, make_float2(f0, f0)));
+    two_sum(zs, zc, z0 * f0);
+    if (ENERGY) two_sum(ps, pc, e0);
+  };
+  if constexpr (FIXED) {
+    const MxShells &Q = S.sh;
+    const MxSite b = mx_site_bases(d, u4, i, s);
+    const float ha = -0.5f * Q.a0;
+    constexpr int nbf = 64;
+    static_for<0, nbf / 2>([&](auto pc2) {
+      constexpr int k = 2 * decltype(pc2)::value;
+      float2 d0, d1;
+      float z0, z1, e0 = 0.f, e1 = 0.f;
+      const float f0 = mxc_force<k, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d0, z0, e0);
+      const float f1 = mxc_force<k + 1, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d1, z1, e1);
+      add2(d0, z0, f0, e0, d1, z1, f1, e1);
+    });
+    static_for<nbf, 88>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
+      const float4 nb = mxc_load<k>(b);
+      float2 exy;
+      float ez;
+      const float num = mxc_num<k>(c, u, nb, exy, ez);
+      if (num < Q.w[HStore<k>::sh]) {
+        float2 d0;
+        float z0, e0 = 0.f;
+        const float f0 = mxc_force<k, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d0, z0, e0);
+        add1(d0, z0, f0, e0);
+      }
+    });
+  } else {
+    const float4 *be = u4 + i, *bo = u4 + i + (s ? S.d_odd : 0);
+    const float rds = S.rds_f, mmax = (float)(S.n_fs - 1);
+    auto two = [&](const MxEntry E0, const MxEntry E1, const float4 *bb) {
+      float2 d0, d1;
+      float z0, z1, e0 = 0.f, e1 = 0.f;
+      const float f0 = mx_force_term<ENERGY>(E0, rds, mmax, u, bb, s_ab, ptab, d0, z0, e0);
+      const float f1 = mx_force_term<ENERGY>(E1, rds, mmax, u, bb, s_ab, ptab, d1, z1, e1);
+      add2(d0, z0, f0, e0, d1, z1, f1, e1);
+    };
+#pragma unroll
+    for (int k = 0; k < MX_PAR_MAX; k += 2) {
+      if (k >= S.n_odd) break;
+      two(S.odd[k], S.odd[k + 1], bo);
+    }
+#pragma unroll
+    for (int k = 0; k < MX_PAR_MAX; k += 2) {
+      if (k >= S.n_even) break;
+      two(S.even[k], S.even[k + 1], be);
+    }
+    for (int k = 0; k < S.n_far; k++) {
+      const MxEntry E = S.far[k];
+      const float4 *bb = (E.odd & s) ? bo : be;
+      const float4 nb = __ldg(bb + E.off);
+      const MxPair g = mx_pair(E, E.fr_f, E.kb_f, rds, mmax, u, nb);
+      if (!g.in) continue;
+      float2 d0;
+      float z0, e0 = 0.f;
+      const float f0 = mx_force_term<ENERGY>(E, rds, mmax, u, bb, s_ab, ptab, d0, z0, e0);
+      add1(d0, z0, f0, e0);
+    }
+  }
+  const double fx = (double)fs.x + (double)fc.x;
+  const double fy = (double)fs.y + (double)fc.y;
+  const double fz = (double)zs + (double)zc;
+  d.fx[i] = (float)fx;
+  d.fy[i] = (float)fy;
+  d.fz[i] = (float)fz;
+  double vx = d.vx[i], vy = d.vy[i], vz = d.vz[i];
+  if (d.primed) {
+    vx += P.h * fx;
+    vy += P.h * fy;
+    vz += P.h * fz;
+  }
+  if (ENERGY) {
+    e_kin += 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E;
+    e_pair += (double)ps + (double)pc;
+  }
+  vx += P.h * fx;
+  vy += P.h * fy;
+  vz += P.h * fz;
+  const double nx = d.ux[i] + P.dt * vx, ny = d.uy[i] + P.dt * vy, nz = d.uz[i] + P.dt * vz;
+  d.vx[i] = vx;
+  d.vy[i] = vy;
+  d.vz[i] = vz;
+  d.ux[i] = nx;
+  d.uy[i] = ny;
+  d.uz[i] = nz;
+  const float4 nu = make_float4((float)nx, (float)ny, (float)nz, 0.f);
+  un[i] = nu;
+  int sx, cx, y, z;
+  mx_unpack(pos, sx, cx, y, z);
+  const Geom g = lat_geom(d);
+  for_images(g, sx, cx, y, z, [&](long long idx, double, double, double) { un[idx] = nu; });
+}
+
+// Density pass.  FIXED: the built-in BCC shells (MxShells), else the runtime stencil
+// (brick walk only).  Energy steps leave one {F(rho), 0} partial per walk item.
+template <bool ENERGY, bool FIXED, int WALK>
 __global__ void __launch_bounds__(MX_RHO_THREADS, 1)
     k_mx_rho(const __grid_constant__ EnsParams P, const MxStencil S, int lat) {
   extern __shared__ float2 s_f[];
   for (int k = threadIdx.x; k < S.n_rs; k += blockDim.x) s_f[k] = P.P.fs32[k];
   __syncthreads();
-  const LatDesc &d = P.lats[lat];
-  const bool active = lat_active(d);
   const int lane = threadIdx.x & 31;
   const unsigned nwarps = blockDim.x >> 5;
-  const float4 *u4 = d.u4[d.cur];
-  float4 *uw = d.u4[d.cur];
   const float c[5] = {0.f, -S.sh.a0, -2.f * S.sh.a0, -3.f * S.sh.a0, -4.f * S.sh.a0};
-  double e_acc = 0.0;
+  unsigned first, count;
+  mx_items<WALK>(S.walk, first, count);
+  MxAt at{-1, 1u, 0u};
   for (unsigned k = threadIdx.x >> 5;; k += nwarps) {
-    const unsigned unit = blockIdx.x + (k / MX_BRICK_ITEMS) * gridDim.x;
-    if (!active || unit >= S.walk.n_units) break;
-    int s, cx, y, z;
-    long long i;
-    if (!mx_site(d, S.walk, unit, k % MX_BRICK_ITEMS, lane, s, cx, y, z, i)) continue;
-    const int code = d.code[i];
-    if (code < 0 || (code & MB_FLAG_ITL)) continue;
-    const float4 u = __ldg(u4 + i);
-    float rs = 0.f, rc = 0.f;
-    if constexpr (FIXED) {
-      const MxShells &Q = S.sh;
-      const MxSite b{u4 + i, u4 + i + Q.E + (s ? Q.d_odd : 0), Q.pl, Q.rw};
-      constexpr int nbf = 64; // shells 1-6, walked without a branch; shell 7 with one
-      static_for<0, nbf / 2>([&](auto pc) {
-        constexpr int k = 2 * decltype(pc)::value;
-        two_sum(rs, rc, mxc_rho<k>(Q, c, b, u, s_f) + mxc_rho<k + 1>(Q, c, b, u, s_f));
-      });
-      static_for<nbf, 88>([&](auto kc) {
-        constexpr int k = decltype(kc)::value;
-        const float4 nb = mxc_load<k>(b);
-        float2 exy;
-        float ez, q;
-        const float num = mxc_num<k>(c, u, nb, exy, ez);
-        if (num < Q.w[HStore<k>::sh]) {
-          const int m = mxc_index<k, 0>(Q, num, q);
-          const float2 t = s_f[m];
-          two_sum(rs, rc, fmaf(t.y, q, t.x));
-        }
-      });
-    } else {
-      const float4 *be = u4 + i, *bo = u4 + i + (s ? S.d_odd : 0);
-      const float rds = S.rds, mmax = (float)(S.n_rs - 1);
-#pragma unroll
-      for (int k = 0; k < MX_PAR_MAX; k += 2) {
-        if (k >= S.n_odd) break;
-        two_sum(rs, rc,
-                mx_rho_term(S.odd[k], rds, mmax, u, bo, s_f) + mx_rho_term(S.odd[k + 1], rds, mmax, u, bo, s_f));
-      }
-#pragma unroll
-      for (int k = 0; k < MX_PAR_MAX; k += 2) {
-        if (k >= S.n_even) break;
-        two_sum(rs, rc,
-                mx_rho_term(S.even[k], rds, mmax, u, be, s_f) + mx_rho_term(S.even[k + 1], rds, mmax, u, be, s_f));
-      }
-      for (int k = 0; k < S.n_far; k++) {
-        const MxEntry E = S.far[k];
-        const float4 *b = (E.odd & s) ? bo : be;
-        const float4 nb = __ldg(b + E.off);
-        const MxPair g = mx_pair(E, E.t.w, E.kb, rds, mmax, u, nb);
-        if (!g.in) continue;
-        const float2 t = s_f[g.m];
-        two_sum(rs, rc, fmaf(t.y, g.q, t.x));
-      }
+    const unsigned item = mx_next<WALK>(S.walk, k, first, count);
+    if (item == ~0u) break;
+    int s = 0, cx = 0, y = 0, z = 0;
+    long long i = 0;
+    const bool ok = mx_locate<WALK>(P, S.walk, lat, item, lane, at, s, cx, y, z, i);
+    const LatDesc &d = P.lats[at.l];
+    double e = 0.0;
+    if (ok && lat_active(d)) e = mx_rho_site<ENERGY, FIXED>(P, S, d, s_f, c, i, mx_pack(s, cx, y, z));
+    if (ENERGY) {
+      e = warp_sum(e);
+      if (lane == 0) P.epart[2 * (size_t)item] = e;
     }
-    const double rho = (double)rs + (double)rc;
-    const double df = dF64(P.P, code & 0x3F, rho);
-    reinterpret_cast<float *>(uw + i)[3] = (float)df;
-    d.rho[i] = (float)rho;
-    const Geom g = lat_geom(d);
-    for_images(g, s, cx, y, z,
-               [&](long long idx, double, double, double) { reinterpret_cast<float *>(uw + idx)[3] = (float)df; });
-    if (ENERGY) e_acc += F64(P.P, code & 0x3F, rho);
-  }
-  if (ENERGY) {
-    const double t = block_sum(e_acc);
-    if (threadIdx.x == 0) P.epart[2 * blockIdx.x] = t;
   }
 }
 
-// Force + velocity-Verlet pass.  Pair terms are added two at a time before one
-// compensated add.
-template <bool ENERGY, bool FIXED>
+// Force + velocity-Verlet pass; energy steps add the pair energy to the item's partial
+// and store its kinetic energy.
+template <bool ENERGY, bool FIXED, int WALK>
 __global__ void __launch_bounds__(MX_FORCE_THREADS, 1)
     k_mx_force(const __grid_constant__ EnsParams P, const MxStencil S, int lat) {
   extern __shared__ float2 s_ab[];
   for (int k = threadIdx.x; k <= S.n_fs; k += blockDim.x) s_ab[k] = P.P.ab32[k];
   __syncthreads();
-  const LatDesc &d = P.lats[lat];
-  const bool active = lat_active(d);
   const int lane = threadIdx.x & 31;
   const unsigned nwarps = blockDim.x >> 5;
-  const float4 *u4 = d.u4[d.cur];
-  float4 *un = d.u4[d.cur ^ 1];
-  const float4 *ptab = P.P.ps32;
   const float c[5] = {0.f, -S.sh.a0, -2.f * S.sh.a0, -3.f * S.sh.a0, -4.f * S.sh.a0};
-  const float ha = -0.5f * S.sh.a0;
-  double e_pair = 0.0, e_kin = 0.0;
+  unsigned first, count;
+  mx_items<WALK>(S.walk, first, count);
+  MxAt at{-1, 1u, 0u};
   for (unsigned k = threadIdx.x >> 5;; k += nwarps) {
-    const unsigned unit = blockIdx.x + (k / MX_BRICK_ITEMS) * gridDim.x;
-    if (!active || unit >= S.walk.n_units) break;
-    int s, cx, y, z;
-    long long i;
-    if (!mx_site(d, S.walk, unit, k % MX_BRICK_ITEMS, lane, s, cx, y, z, i)) continue;
-    const int code = d.code[i];
-    if (code < 0 || (code & MB_FLAG_ITL)) continue;
-    const float4 u = __ldg(u4 + i);
-    float2 fs = make_float2(0.f, 0.f), fc = fs;
-    float zs = 0.f, zc = 0.f, ps = 0.f, pc = 0.f;
-    auto add2 = [&](float2 d0, float z0, float f0, float e0, float2 d1, float z1, float f1, float e1) {
-      two_sum2(fs, fc, __ffma2_rn(d1, make_float2(f1, f1), __fmul2_rn(d0, make_float2(f0, f0))));
-      two_sum(zs, zc, fmaf(z1, f1, z0 * f0));
-      if (ENERGY) two_sum(ps, pc, e0 + e1);
-    };
-    auto add1 = [&](float2 d0, float z0, float f0, float e0) {
-      two_sum2(fs, fc, __fmul2_rn(d0, make_float2(f0, f0)));
-      two_sum(zs, zc, z0 * f0);
-      if (ENERGY) two_sum(ps, pc, e0);
-    };
-    if constexpr (FIXED) {
-      const MxShells &Q = S.sh;
-      const MxSite b{u4 + i, u4 + i + Q.E + (s ? Q.d_odd : 0), Q.pl, Q.rw};
-      constexpr int nbf = 64;
-      static_for<0, nbf / 2>([&](auto pc2) {
-        constexpr int k = 2 * decltype(pc2)::value;
-        float2 d0, d1;
-        float z0, z1, e0 = 0.f, e1 = 0.f;
-        const float f0 = mxc_force<k, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d0, z0, e0);
-        const float f1 = mxc_force<k + 1, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d1, z1, e1);
-        add2(d0, z0, f0, e0, d1, z1, f1, e1);
-      });
-      static_for<nbf, 88>([&](auto kc) {
-        constexpr int k = decltype(kc)::value;
-        const float4 nb = mxc_load<k>(b);
-        float2 exy;
-        float ez;
-        const float num = mxc_num<k>(c, u, nb, exy, ez);
-        if (num < Q.w[HStore<k>::sh]) {
-          float2 d0;
-          float z0, e0 = 0.f;
-          const float f0 = mxc_force<k, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d0, z0, e0);
-          add1(d0, z0, f0, e0);
-        }
-      });
-    } else {
-      const float4 *be = u4 + i, *bo = u4 + i + (s ? S.d_odd : 0);
-      const float rds = S.rds_f, mmax = (float)(S.n_fs - 1);
-      auto two = [&](const MxEntry E0, const MxEntry E1, const float4 *bb) {
-        float2 d0, d1;
-        float z0, z1, e0 = 0.f, e1 = 0.f;
-        const float f0 = mx_force_term<ENERGY>(E0, rds, mmax, u, bb, s_ab, ptab, d0, z0, e0);
-        const float f1 = mx_force_term<ENERGY>(E1, rds, mmax, u, bb, s_ab, ptab, d1, z1, e1);
-        add2(d0, z0, f0, e0, d1, z1, f1, e1);
-      };
-#pragma unroll
-      for (int k = 0; k < MX_PAR_MAX; k += 2) {
-        if (k >= S.n_odd) break;
-        two(S.odd[k], S.odd[k + 1], bo);
-      }
-#pragma unroll
-      for (int k = 0; k < MX_PAR_MAX; k += 2) {
-        if (k >= S.n_even) break;
-        two(S.even[k], S.even[k + 1], be);
-      }
-      for (int k = 0; k < S.n_far; k++) {
-        const MxEntry E = S.far[k];
-        const float4 *bb = (E.odd & s) ? bo : be;
-        const float4 nb = __ldg(bb + E.off);
-        const MxPair g = mx_pair(E, E.fr_f, E.kb_f, rds, mmax, u, nb);
-        if (!g.in) continue;
-        float2 d0;
-        float z0, e0 = 0.f;
-        const float f0 = mx_force_term<ENERGY>(E, rds, mmax, u, bb, s_ab, ptab, d0, z0, e0);
-        add1(d0, z0, f0, e0);
-      }
-    }
-    const double fx = (double)fs.x + (double)fc.x;
-    const double fy = (double)fs.y + (double)fc.y;
-    const double fz = (double)zs + (double)zc;
-    d.fx[i] = (float)fx;
-    d.fy[i] = (float)fy;
-    d.fz[i] = (float)fz;
-    double vx = d.vx[i], vy = d.vy[i], vz = d.vz[i];
-    if (d.primed) {
-      vx += P.h * fx;
-      vy += P.h * fy;
-      vz += P.h * fz;
-    }
+    const unsigned item = mx_next<WALK>(S.walk, k, first, count);
+    if (item == ~0u) break;
+    int s = 0, cx = 0, y = 0, z = 0;
+    long long i = 0;
+    const bool ok = mx_locate<WALK>(P, S.walk, lat, item, lane, at, s, cx, y, z, i);
+    const LatDesc &d = P.lats[at.l];
+    double ep = 0.0, ek = 0.0;
+    if (ok && lat_active(d)) mx_force_site<ENERGY, FIXED>(P, S, d, s_ab, c, i, mx_pack(s, cx, y, z), ep, ek);
     if (ENERGY) {
-      e_kin += 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E;
-      e_pair += (double)ps + (double)pc;
-    }
-    vx += P.h * fx;
-    vy += P.h * fy;
-    vz += P.h * fz;
-    const double nx = d.ux[i] + P.dt * vx, ny = d.uy[i] + P.dt * vy, nz = d.uz[i] + P.dt * vz;
-    d.vx[i] = vx;
-    d.vy[i] = vy;
-    d.vz[i] = vz;
-    d.ux[i] = nx;
-    d.uy[i] = ny;
-    d.uz[i] = nz;
-    const float4 nu = make_float4((float)nx, (float)ny, (float)nz, 0.f);
-    un[i] = nu;
-    const Geom g = lat_geom(d);
-    for_images(g, s, cx, y, z, [&](long long idx, double, double, double) { un[idx] = nu; });
-  }
-  if (ENERGY) {
-    const double t1 = block_sum(e_pair);
-    const double t2 = block_sum(e_kin);
-    if (threadIdx.x == 0) {
-      P.epart[2 * blockIdx.x] += t1;
-      P.epart[2 * blockIdx.x + 1] = t2;
+      ep = warp_sum(ep);
+      ek = warp_sum(ek);
+      if (lane == 0) {
+        P.epart[2 * (size_t)item] += ep;
+        P.epart[2 * (size_t)item + 1] = ek;
+      }
     }
   }
 }
@@ -368,43 +479,78 @@ __global__ void k_mx_bookkeeping(const __grid_constant__ EnsParams P) {
   }
 }
 
-template <bool FIXED>
+template <bool FIXED, int WALK>
 static int mx_set_attrs() {
-  MB_CUDA(cudaFuncSetAttribute(k_mx_rho<false, FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
-  MB_CUDA(cudaFuncSetAttribute(k_mx_rho<true, FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
-  MB_CUDA(cudaFuncSetAttribute(k_mx_force<false, FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
-  MB_CUDA(cudaFuncSetAttribute(k_mx_force<true, FIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
+  MB_CUDA(cudaFuncSetAttribute(k_mx_rho<false, FIXED, WALK>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
+  MB_CUDA(cudaFuncSetAttribute(k_mx_rho<true, FIXED, WALK>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
+  MB_CUDA(
+      cudaFuncSetAttribute(k_mx_force<false, FIXED, WALK>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
+  MB_CUDA(cudaFuncSetAttribute(k_mx_force<true, FIXED, WALK>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
   return MB_OK;
 }
 
-template <bool FIXED>
-static void mx_passes(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s, int which,
-                      size_t smem) {
+template <bool FIXED, int WALK>
+static void mx_pass(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s, int which,
+                    size_t smem) {
   const int sms = device_sm_count();
   if (which == 0) {
     if (energy)
-      k_mx_rho<true, FIXED><<<sms, MX_RHO_THREADS, smem, s>>>(P, S, lat);
+      k_mx_rho<true, FIXED, WALK><<<sms, MX_RHO_THREADS, smem, s>>>(P, S, lat);
     else
-      k_mx_rho<false, FIXED><<<sms, MX_RHO_THREADS, smem, s>>>(P, S, lat);
+      k_mx_rho<false, FIXED, WALK><<<sms, MX_RHO_THREADS, smem, s>>>(P, S, lat);
   } else {
     if (energy)
-      k_mx_force<true, FIXED><<<sms, MX_FORCE_THREADS, smem, s>>>(P, S, lat);
+      k_mx_force<true, FIXED, WALK><<<sms, MX_FORCE_THREADS, smem, s>>>(P, S, lat);
     else
-      k_mx_force<false, FIXED><<<sms, MX_FORCE_THREADS, smem, s>>>(P, S, lat);
+      k_mx_force<false, FIXED, WALK><<<sms, MX_FORCE_THREADS, smem, s>>>(P, S, lat);
   }
 }
 
-// ev (optional): events recorded around the density kernel (ev[0], ev[1]) and the
-// force kernel (ev[2], ev[3]).
-int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s, cudaEvent_t *ev) {
+static void mx_passes(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s, int which,
+                      size_t smem) {
+  if (S.walk.linear)
+    mx_pass<true, 1>(P, S, lat, energy, s, which, smem);
+  else if (S.fixed)
+    mx_pass<true, 0>(P, S, lat, energy, s, which, smem);
+  else
+    mx_pass<false, 0>(P, S, lat, energy, s, which, smem);
+}
+
+// Per-lattice energies of an energy step: block l sums the partials of lattice l's items
+// and adds its interstitial items.
+__global__ void k_mx_energy(const LatDesc *lats, int n_lats, const unsigned *first, unsigned n_items,
+                            const double *epart, double *out) {
+  const int l = blockIdx.x;
+  if (l >= n_lats) return;
+  const unsigned a = first ? first[l] : 0u, b = first ? first[l + 1] : n_items;
+  double pe = 0.0, ke = 0.0;
+  for (unsigned t = a + threadIdx.x; t < b; t += blockDim.x) {
+    pe += epart[2 * (size_t)t];
+    ke += epart[2 * (size_t)t + 1];
+  }
+  pe = block_sum(pe);
+  ke = block_sum(ke);
+  if (threadIdx.x == 0) {
+    out[2 * l] = pe + lats[l].e_itl[0];
+    out[2 * l + 1] = ke + lats[l].e_itl[1];
+  }
+}
+
+// One step of every active lattice.  ev (optional): events recorded around the density
+// kernel (ev[0], ev[1]) and the force kernel (ev[2], ev[3]).  Energy steps also reduce
+// the item partials into out[2 l], out[2 l + 1].
+int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s, cudaEvent_t *ev,
+                   double *out) {
   const int sms = device_sm_count();
   const size_t rho_smem = (size_t)S.n_rs * sizeof(float2), force_smem = (size_t)(S.n_fs + 1) * sizeof(float2);
   if (force_smem > MX_SMEM_MAX || rho_smem > MX_SMEM_MAX)
     return fail(MB_ERR_ARG, "squared-distance table larger than shared memory");
+  if (S.walk.linear && !S.fixed) return fail(MB_ERR_STATE, "linear walk needs the built-in shells");
   static bool attr = false;
   if (!attr) {
-    MB_TRY(mx_set_attrs<false>());
-    MB_TRY(mx_set_attrs<true>());
+    MB_TRY((mx_set_attrs<false, 0>()));
+    MB_TRY((mx_set_attrs<true, 0>()));
+    MB_TRY((mx_set_attrs<true, 1>()));
     attr = true;
   }
   const int itl_grid = 2 * sms;
@@ -413,10 +559,7 @@ int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, 
     k_mx_itl_mark<<<itl_grid, 256, 0, s>>>(P);
   }
   if (ev) MB_CUDA(cudaEventRecord(ev[0], s));
-  if (S.fixed)
-    mx_passes<true>(P, S, lat, energy, s, 0, rho_smem);
-  else
-    mx_passes<false>(P, S, lat, energy, s, 0, rho_smem);
+  mx_passes(P, S, lat, energy, s, 0, rho_smem);
   if (ev) MB_CUDA(cudaEventRecord(ev[1], s));
   if (P.n_itl_lats > 0) {
     if (energy)
@@ -425,10 +568,7 @@ int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, 
       k_mx_itl_items<false, false><<<itl_grid, 256, 0, s>>>(P);
   }
   if (ev) MB_CUDA(cudaEventRecord(ev[2], s));
-  if (S.fixed)
-    mx_passes<true>(P, S, lat, energy, s, 1, force_smem);
-  else
-    mx_passes<false>(P, S, lat, energy, s, 1, force_smem);
+  mx_passes(P, S, lat, energy, s, 1, force_smem);
   if (ev) MB_CUDA(cudaEventRecord(ev[3], s));
   if (P.n_itl_lats > 0) {
     if (energy)
@@ -436,32 +576,14 @@ int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, 
     else
       k_mx_itl_items<true, false><<<itl_grid, 256, 0, s>>>(P);
   }
+  if (energy) {
+    const int nl = S.walk.linear ? S.walk.n_lats : 1;
+    k_mx_energy<<<nl, 256, 0, s>>>(S.walk.linear ? P.lats : P.lats + lat, nl,
+                                   S.walk.linear ? S.walk.item_first : nullptr, S.walk.n_items, P.epart, out);
+  }
   k_mx_bookkeeping<<<1, 128, 0, s>>>(P);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
-
-// Energies of the split step: the per-CTA partials plus the interstitial items.
-__global__ void k_mx_energy(const LatDesc *lats, int lat, const double *epart, int n_parts, double *out) {
-  double pe = 0.0, ke = 0.0;
-  for (int t = threadIdx.x; t < n_parts; t += blockDim.x) {
-    pe += epart[2 * t];
-    ke += epart[2 * t + 1];
-  }
-  pe = block_sum(pe);
-  ke = block_sum(ke);
-  if (threadIdx.x == 0) {
-    out[0] = pe + lats[lat].e_itl[0];
-    out[1] = ke + lats[lat].e_itl[1];
-  }
-}
-
-int mx_energy_launch(const LatDesc *lats, int lat, const double *epart, double *out, cudaStream_t s) {
-  k_mx_energy<<<1, 256, 0, s>>>(lats, lat, epart, device_sm_count(), out);
-  MB_CUDA(cudaGetLastError());
-  return MB_OK;
-}
-
-int mx_grid() { return device_sm_count(); }
 
 } // namespace mb
