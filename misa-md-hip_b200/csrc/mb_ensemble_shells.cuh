@@ -70,15 +70,21 @@ struct HStore {
   static constexpr int sh = shell_of(K);
 };
 
-// c[|H|] = -a0 |H|: the products 2 C . e = -a0 (h . e) by one FMA per component.
-template <int H>
-__device__ __forceinline__ float hfma(const float (&c)[5], float e, float acc) {
-  if constexpr (H == 0)
-    return acc;
-  else if constexpr (H > 0)
-    return fmaf(c[H], e, acc);
-  else
-    return fmaf(-c[-H], e, acc);
+// h . e with the integer components of h as immediates (zero terms dropped).
+template <int HX, int HY, int HZ>
+__device__ __forceinline__ float hdot(float ex, float ey, float ez) {
+  float acc;
+  if constexpr (HX != 0) {
+    acc = (float)HX * ex;
+    if constexpr (HY != 0) acc = fmaf((float)HY, ey, acc);
+    if constexpr (HZ != 0) acc = fmaf((float)HZ, ez, acc);
+  } else if constexpr (HY != 0) {
+    acc = (float)HY * ey;
+    if constexpr (HZ != 0) acc = fmaf((float)HZ, ez, acc);
+  } else {
+    acc = (float)HZ * ez;
+  }
+  return acc;
 }
 
 struct MxSite {
@@ -93,19 +99,15 @@ __device__ __forceinline__ float4 mxc_load(const MxSite &b) {
   return __ldg(base + (T::dz * b.pl + T::dy * b.rw) + T::dx);
 }
 
-// num = r^2 - R^2 = |e|^2 - a0 (h . e), e = u_i - u_j.
+// num = r^2 - R^2 = |e|^2 - a0 (h . e), e = u_i - u_j (ma0 = -a0).
 template <int K>
-__device__ __forceinline__ float mxc_num(const float (&c)[5], const float4 &u, const float4 &nb, float2 &exy,
-                                         float &ez) {
+__device__ __forceinline__ float mxc_num(float ma0, const float4 &u, const float4 &nb, float2 &exy, float &ez) {
   using T = HStore<K>;
   exy = __fadd2_rn(make_float2(u.x, u.y), make_float2(-nb.x, -nb.y));
   ez = u.z - nb.z;
   const float2 ee = __fmul2_rn(exy, exy);
-  float num = fmaf(ez, ez, ee.x + ee.y);
-  num = hfma<T::h.hx>(c, exy.x, num);
-  num = hfma<T::h.hy>(c, exy.y, num);
-  num = hfma<T::h.hz>(c, ez, num);
-  return num;
+  const float e2 = fmaf(ez, ez, ee.x + ee.y);
+  return fmaf(ma0, hdot<T::h.hx, T::h.hy, T::h.hz>(exy.x, exy.y, ez), e2);
 }
 
 // Table interval and local coordinate of vector K's pair on grid G (0 density, 1 force).
@@ -119,12 +121,12 @@ __device__ __forceinline__ int mxc_index(const MxShells &Q, float num, float &q)
 }
 
 template <int K>
-__device__ __forceinline__ float mxc_rho(const MxShells &Q, const float (&c)[5], const MxSite &b, const float4 &u,
+__device__ __forceinline__ float mxc_rho(const MxShells &Q, float ma0, const MxSite &b, const float4 &u,
                                          const float2 *tab) {
   const float4 nb = mxc_load<K>(b);
   float2 exy;
   float ez, q;
-  const float num = mxc_num<K>(c, u, nb, exy, ez);
+  const float num = mxc_num<K>(ma0, u, nb, exy, ez);
   const int m = mxc_index<K, 0>(Q, num, q);
   const float2 t = tab[m];
   const float v = fmaf(t.y, q, t.x);
@@ -139,14 +141,14 @@ __device__ __forceinline__ float2 mx_ab(const float2 *tab, int m, float q) {
 
 // fpair and pair vector d = C + e of vector K (fpair 0 beyond the cutoff).
 template <int K, bool ENERGY>
-__device__ __forceinline__ float mxc_force(const MxShells &Q, const float (&c)[5], float ha, const MxSite &b,
-                                           const float4 &u, const float2 *tab, const float4 *ptab, float2 &dxy,
-                                           float &dz, float &e) {
+__device__ __forceinline__ float mxc_force(const MxShells &Q, float ma0, const MxSite &b, const float4 &u,
+                                           const float2 *tab, const float4 *ptab, float2 &dxy, float &dz, float &e) {
   using T = HStore<K>;
   const float4 nb = mxc_load<K>(b);
   float2 exy;
   float ez, q;
-  const float num = mxc_num<K>(c, u, nb, exy, ez);
+  const float num = mxc_num<K>(ma0, u, nb, exy, ez);
+  const float ha = 0.5f * ma0;
   const int m = mxc_index<K, 1>(Q, num, q);
   const float2 ab = mx_ab(tab, m, q);
   const float fp = -fmaf(u.w + nb.w, ab.x, ab.y);

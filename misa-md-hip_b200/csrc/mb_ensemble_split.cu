@@ -197,7 +197,7 @@ __device__ __forceinline__ void mx_unpack(unsigned p, int &s, int &cx, int &y, i
 
 template <bool ENERGY, bool FIXED>
 __device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStencil &S, const LatDesc &d,
-                                              const float2 *s_f, const float (&c)[5], long long i, unsigned pos) {
+                                              const float2 *s_f, float ma0, long long i, unsigned pos) {
   const int s = (int)(pos >> 31);
   const int code = d.code[i];
   if (code < 0 || (code & MB_FLAG_ITL)) return 0.0;
@@ -211,14 +211,14 @@ __device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStenci
     constexpr int nbf = 64; // shells 1-6, walked without a branch; shell 7 with one
     static_for<0, nbf / 2>([&](auto pc) {
       constexpr int k = 2 * decltype(pc)::value;
-      two_sum(rs, rc, mxc_rho<k>(Q, c, b, u, s_f) + mxc_rho<k + 1>(Q, c, b, u, s_f));
+      two_sum(rs, rc, mxc_rho<k>(Q, ma0, b, u, s_f) + mxc_rho<k + 1>(Q, ma0, b, u, s_f));
     });
     static_for<nbf, 88>([&](auto kc) {
       constexpr int k = decltype(kc)::value;
       const float4 nb = mxc_load<k>(b);
       float2 exy;
       float ez, q;
-      const float num = mxc_num<k>(c, u, nb, exy, ez);
+      const float num = mxc_num<k>(ma0, u, nb, exy, ez);
       if (num < Q.w[HStore<k>::sh]) {
         const int m = mxc_index<k, 0>(Q, num, q);
         const float2 t = s_f[m];
@@ -266,7 +266,7 @@ __device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStenci
 // are added two at a time before one compensated add.
 template <bool ENERGY, bool FIXED>
 __device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStencil &S, const LatDesc &d,
-                                              const float2 *s_ab, const float (&c)[5], long long i, unsigned pos,
+                                              const float2 *s_ab, float ma0, long long i, unsigned pos,
                                               double &e_pair, double &e_kin) {
   const int s = (int)(pos >> 31);
   const int code = d.code[i];
@@ -290,14 +290,13 @@ __device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStenci
   if constexpr (FIXED) {
     const MxShells &Q = S.sh;
     const MxSite b = mx_site_bases(d, u4, i, s);
-    const float ha = -0.5f * Q.a0;
     constexpr int nbf = 64;
     static_for<0, nbf / 2>([&](auto pc2) {
       constexpr int k = 2 * decltype(pc2)::value;
       float2 d0, d1;
       float z0, z1, e0 = 0.f, e1 = 0.f;
-      const float f0 = mxc_force<k, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d0, z0, e0);
-      const float f1 = mxc_force<k + 1, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d1, z1, e1);
+      const float f0 = mxc_force<k, ENERGY>(Q, ma0, b, u, s_ab, ptab, d0, z0, e0);
+      const float f1 = mxc_force<k + 1, ENERGY>(Q, ma0, b, u, s_ab, ptab, d1, z1, e1);
       add2(d0, z0, f0, e0, d1, z1, f1, e1);
     });
     static_for<nbf, 88>([&](auto kc) {
@@ -305,11 +304,11 @@ __device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStenci
       const float4 nb = mxc_load<k>(b);
       float2 exy;
       float ez;
-      const float num = mxc_num<k>(c, u, nb, exy, ez);
+      const float num = mxc_num<k>(ma0, u, nb, exy, ez);
       if (num < Q.w[HStore<k>::sh]) {
         float2 d0;
         float z0, e0 = 0.f;
-        const float f0 = mxc_force<k, ENERGY>(Q, c, ha, b, u, s_ab, ptab, d0, z0, e0);
+        const float f0 = mxc_force<k, ENERGY>(Q, ma0, b, u, s_ab, ptab, d0, z0, e0);
         add1(d0, z0, f0, e0);
       }
     });
@@ -389,7 +388,7 @@ __global__ void __launch_bounds__(MX_RHO_THREADS, 1)
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned nwarps = blockDim.x >> 5;
-  const float c[5] = {0.f, -S.sh.a0, -2.f * S.sh.a0, -3.f * S.sh.a0, -4.f * S.sh.a0};
+  const float ma0 = -S.sh.a0;
   unsigned first, count;
   mx_items<WALK>(S.walk, first, count);
   MxAt at{-1, 1u, 0u};
@@ -401,7 +400,7 @@ __global__ void __launch_bounds__(MX_RHO_THREADS, 1)
     const bool ok = mx_locate<WALK>(P, S.walk, lat, item, lane, at, s, cx, y, z, i);
     const LatDesc &d = P.lats[at.l];
     double e = 0.0;
-    if (ok && lat_active(d)) e = mx_rho_site<ENERGY, FIXED>(P, S, d, s_f, c, i, mx_pack(s, cx, y, z));
+    if (ok && lat_active(d)) e = mx_rho_site<ENERGY, FIXED>(P, S, d, s_f, ma0, i, mx_pack(s, cx, y, z));
     if (ENERGY) {
       e = warp_sum(e);
       if (lane == 0) P.epart[2 * (size_t)item] = e;
@@ -419,7 +418,7 @@ __global__ void __launch_bounds__(MX_FORCE_THREADS, 1)
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned nwarps = blockDim.x >> 5;
-  const float c[5] = {0.f, -S.sh.a0, -2.f * S.sh.a0, -3.f * S.sh.a0, -4.f * S.sh.a0};
+  const float ma0 = -S.sh.a0;
   unsigned first, count;
   mx_items<WALK>(S.walk, first, count);
   MxAt at{-1, 1u, 0u};
@@ -431,7 +430,7 @@ __global__ void __launch_bounds__(MX_FORCE_THREADS, 1)
     const bool ok = mx_locate<WALK>(P, S.walk, lat, item, lane, at, s, cx, y, z, i);
     const LatDesc &d = P.lats[at.l];
     double ep = 0.0, ek = 0.0;
-    if (ok && lat_active(d)) mx_force_site<ENERGY, FIXED>(P, S, d, s_ab, c, i, mx_pack(s, cx, y, z), ep, ek);
+    if (ok && lat_active(d)) mx_force_site<ENERGY, FIXED>(P, S, d, s_ab, ma0, i, mx_pack(s, cx, y, z), ep, ek);
     if (ENERGY) {
       ep = warp_sum(ep);
       ek = warp_sum(ek);
