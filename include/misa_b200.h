@@ -247,15 +247,18 @@ int mb_ensemble_clear_energies(mb_ensemble *e, int32_t slot);
 int mb_ensemble_time(mb_ensemble *e, int32_t nsteps, float *ms);
 /* Tile-shape policy: -1 picks a shape per lattice from its size, 0..3 one shape for all. */
 int mb_ensemble_set_policy(mb_ensemble *e, int32_t policy);
-/* Times every policy for `steps` launches on a snapshot of the slots (state restored
- * afterwards) and keeps the fastest. */
+/* Times the candidate kernels for `steps` launches each on a snapshot of the slots
+ * (state restored afterwards) and keeps the fastest: the split kernels (reported as
+ * *policy = 4; skipped when their stencil does not apply or mode 1 was set) and every
+ * tile policy -1..3 of the persistent kernel (skipped when mode 2 was set). */
 int mb_ensemble_autotune(mb_ensemble *e, int32_t steps, int32_t *policy, float *best_ms);
 int mb_ensemble_info(mb_ensemble *e, int64_t *n_sites, int64_t *n_tiles, int64_t *device_bytes, int32_t *n_slots);
 int mb_ensemble_set_graphs(mb_ensemble *e, int enable);
-/* Kernel structure: 0 (default) runs a single lattice of >= 2^19 sites as separate
- * density and force kernels (higher occupancy) and everything else with the
- * persistent one-launch-per-step kernel; 1 always persistent; 2 always split (one
- * lattice only). */
+/* Kernel structure: 0 (default) runs the separate density and force kernels ("split":
+ * one CUDA graph of up to 8 launches per step, every lattice in each launch) whenever
+ * their built-in BCC stencil applies and the persistent one-launch-per-step tile
+ * kernel otherwise; 1 always the persistent kernel; 2 always split (MB_ERR_UNSUPPORTED
+ * at the next launch if it cannot apply). */
 int mb_ensemble_set_mode(mb_ensemble *e, int32_t mode);
 /* Device time of one step's kernels, averaged over 4 extra steps every lattice takes
  * (CUDA events on the ensemble's stream): split kernels report the density pass in

@@ -157,8 +157,8 @@ class Sim:
 
 
 class Ensemble:
-    """Many independent periodic lattices advanced together in mixed precision:
-    one persistent kernel launch per timestep (C ABI: mb_ensemble_*)."""
+    """Many independent periodic lattices advanced together in mixed precision: one
+    CUDA graph per timestep advances every lattice (C ABI: mb_ensemble_*)."""
 
     def __init__(self, tables: potential.EamTables, lattice_const: float = 2.855, mass: float = 55.845,
                  dt: float = 1.0, cutoff: float | None = None, stencil_skin: float = 0.7,
@@ -272,7 +272,7 @@ class Ensemble:
         check(lib().mb_ensemble_set_graphs(self._h, int(enable)))
 
     def set_mode(self, mode: int) -> None:
-        """0: split kernels for one large lattice (default), 1: persistent, 2: split."""
+        """0: split kernels where their stencil applies (default), 1: persistent, 2: split."""
         check(lib().mb_ensemble_set_mode(self._h, mode))
 
     def kernel_times(self) -> tuple[float, float, int]:

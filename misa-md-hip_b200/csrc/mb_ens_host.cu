@@ -1247,13 +1247,23 @@ int mb_ensemble_autotune(mb_ensemble *e, int32_t steps, int32_t *policy, float *
       off += L.bytes;
       saved.push_back(L.d);
     }
-  const int old_policy = e->policy;
+  const int old_policy = e->policy, old_mode = e->mode;
   int rc = MB_OK;
-  for (int pol = -1; pol < ENS_NSHAPE && rc == MB_OK; pol++) {
-    rc = mb_ensemble_set_policy(e, pol);
+  // candidates: the split kernels (encoded as policy ENS_NSHAPE), then every tile policy
+  // of the persistent kernel; an explicit mode restricts the search to that kernel
+  std::vector<std::pair<int, int>> cand; // (mode, policy)
+  if (old_mode != 1) cand.push_back({2, old_policy});
+  if (old_mode != 2)
+    for (int pol = -1; pol < ENS_NSHAPE; pol++) cand.push_back({1, pol});
+  for (size_t ci = 0; ci < cand.size() && rc == MB_OK; ci++) {
+    rc = mb_ensemble_set_mode(e, cand[ci].first);
+    if (rc == MB_OK) rc = mb_ensemble_set_policy(e, cand[ci].second);
     float ms = 0.f;
     if (rc == MB_OK) rc = mb_ensemble_time(e, steps, &ms);
-    if (rc == MB_OK) results.push_back({pol, ms});
+    if (rc == MB_OK)
+      results.push_back({cand[ci].first == 2 ? ENS_NSHAPE : cand[ci].second, ms});
+    else if (cand[ci].first == 2 && rc == MB_ERR_UNSUPPORTED && old_mode == 0)
+      rc = MB_OK; // split kernels do not apply here: tune the persistent kernel only
     // restore state for the next candidate
     std::lock_guard<std::mutex> lk(e->mu);
     cudaStreamSynchronize(e->stream);
@@ -1277,15 +1287,23 @@ int mb_ensemble_autotune(mb_ensemble *e, int32_t steps, int32_t *policy, float *
     e->dirty = true;
   }
   cudaFree(snap);
-  if (rc != MB_OK) {
+  if (rc != MB_OK || results.empty()) {
     e->policy = old_policy;
-    return rc;
+    e->mode = old_mode;
+    e->dirty = true;
+    return rc != MB_OK ? rc : fail(MB_ERR_STATE, "no kernel could be timed");
   }
   auto best = std::min_element(results.begin(), results.end(),
                                [](const std::pair<int, float> &a, const std::pair<int, float> &b) {
                                  return a.second < b.second;
                                });
-  MB_TRY(mb_ensemble_set_policy(e, best->first));
+  if (best->first == ENS_NSHAPE) {
+    MB_TRY(mb_ensemble_set_mode(e, old_mode == 0 ? 0 : 2));
+    MB_TRY(mb_ensemble_set_policy(e, old_policy));
+  } else {
+    MB_TRY(mb_ensemble_set_mode(e, 1));
+    MB_TRY(mb_ensemble_set_policy(e, best->first));
+  }
   if (policy) *policy = best->first;
   if (best_ms) *best_ms = best->second;
   return MB_OK;

@@ -38,11 +38,14 @@ def _ens(sc, **kw):
                        stencil_skin=sc.skin, **kw)
 
 
+@pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("n_itl", [0, 3])
-def test_mixed_forces_within_1e6_of_fp64_oracle(n_itl):
+def test_mixed_forces_within_1e6_of_fp64_oracle(n_itl, mode):
+    # mode 1: the persistent tile kernel; mode 2: the split density / force kernels
     sc = make(cells=(9, 8, 10), temperature=900.0, vacancy=0.01, n_itl=n_itl, seed=71, jitter=0.1)
     bo, io, pe = _oracle_forces(sc, itl=sc.itl)
     with _ens(sc) as ens:
+        ens.set_mode(mode)
         slot = ens.add(sc.cells, sc.box, sc.itl if n_itl else None, steps=0)
         ens.run(0)  # priming launch only: forces at the uploaded positions
         bg, ig = ens.download(slot)
@@ -58,21 +61,18 @@ def test_mixed_forces_within_1e6_of_fp64_oracle(n_itl):
     np.testing.assert_allclose(bg["x"][live], sc.box["x"][live], rtol=0, atol=1e-12)
 
 
-@pytest.mark.parametrize("n_itl", [0, 3])
-def test_split_kernels_forces_within_1e6_of_fp64_oracle(n_itl):
-    # the separate density / force kernels used for one large lattice, forced on a small one
-    sc = make(cells=(9, 8, 10), temperature=900.0, vacancy=0.01, n_itl=n_itl, seed=71, jitter=0.1)
+def test_split_brick_walk_forces_within_1e6_of_fp64_oracle():
+    # a lattice 32 cells wide walks bricks (the large-lattice path) instead of linear items
+    sc = make(cells=(32, 9, 10), temperature=900.0, vacancy=0.01, n_itl=2, seed=76, jitter=0.1)
     bo, io, pe = _oracle_forces(sc, itl=sc.itl)
     with _ens(sc) as ens:
         ens.set_mode(2)
-        slot = ens.add(sc.cells, sc.box, sc.itl if n_itl else None, steps=0)
+        slot = ens.add(sc.cells, sc.box, sc.itl, steps=0)
         ens.run(0)
         bg, ig = ens.download(slot)
     live = bo["type"] >= 0
-    fo, fg = bo["f"][live], bg["f"][live]
-    if n_itl:
-        fo = np.concatenate([fo, io["f"]])
-        fg = np.concatenate([fg, ig["f"]])
+    fo = np.concatenate([bo["f"][live], io["f"]])
+    fg = np.concatenate([bg["f"][live], ig["f"]])
     assert rms_rel(fg, fo) < F_RMS_TOL
     assert rms_rel(bg["rho"][live], bo["rho"][live]) < 1e-6
 
@@ -151,17 +151,20 @@ def test_mixed_nve_drift():
     assert np.max(np.abs(tot - (e64[:, 1] + e64[:, 2]))) / n < 1e-6
 
 
-def test_batched_equals_alone():
+@pytest.mark.parametrize("mode", [1, 2])
+def test_batched_equals_alone(mode):
     specs = [((8, 9, 10), 0, 0.01), ((12, 8, 8), 2, 0.0), ((9, 9, 9), 1, 0.005), ((16, 10, 8), 0, 0.0)]
     scs = [make(cells=c, temperature=600.0 + 100 * k, vacancy=v, n_itl=n, seed=80 + k)
            for k, (c, n, v) in enumerate(specs)]
     alone = []
     for sc in scs:
         with _ens(sc) as ens:
+            ens.set_mode(mode)
             s = ens.add(sc.cells, sc.box, sc.itl if sc.itl.shape[0] else None, steps=25)
             ens.advance(100, energy_every=5)
             alone.append((*ens.download(s), ens.energies(s)))
     with _ens(scs[0]) as ens:
+        ens.set_mode(mode)
         slots = [ens.add(sc.cells, sc.box, sc.itl if sc.itl.shape[0] else None, steps=25) for sc in scs]
         ens.advance(100, energy_every=5)
         for k, s in enumerate(slots):
@@ -215,15 +218,37 @@ def test_hbm_budget_and_slot_limit_refuse_admission():
 def test_autotune_keeps_state_and_results():
     specs = [(8, 8, 8), (17, 9, 8), (10, 20, 9)]
     scs = [make(cells=c, temperature=700.0, seed=95 + k) for k, c in enumerate(specs)]
+    with _ens(scs[0]) as ens:
+        slots = [ens.add(sc.cells, sc.box, steps=10) for sc in scs]
+        pol, ms = ens.autotune(3)
+        assert -1 <= pol <= 4 and ms > 0
+        assert all(ens.status(s)[0] == 0 for s in slots)  # tuning took no simulation steps
+        ens.advance(100)
+        tuned = [ens.download(s)[0] for s in slots]
+    with _ens(scs[0]) as ens:  # the chosen kernel, set by hand, from the same start
+        if pol == 4:
+            ens.set_mode(2)
+        else:
+            ens.set_mode(1)
+            ens.set_policy(pol)
+        slots = [ens.add(sc.cells, sc.box, steps=10) for sc in scs]
+        ens.advance(100)
+        plain = [ens.download(s)[0] for s in slots]
+    for a, b in zip(tuned, plain):
+        assert np.array_equal(a["x"], b["x"])
+
+
+def test_persistent_tile_policies_share_arithmetic():
+    specs = [(8, 8, 8), (17, 9, 8), (10, 20, 9)]
+    scs = [make(cells=c, temperature=700.0, seed=95 + k) for k, c in enumerate(specs)]
     res = []
-    for tune in (False, True):
+    for pol in (-1, 0, 3):
         with _ens(scs[0]) as ens:
+            ens.set_mode(1)
+            ens.set_policy(pol)
             slots = [ens.add(sc.cells, sc.box, steps=10) for sc in scs]
-            if tune:
-                pol, ms = ens.autotune(3)
-                assert -1 <= pol <= 3 and ms > 0
-                assert all(ens.status(s)[0] == 0 for s in slots)
             ens.advance(100)
             res.append([ens.download(s)[0] for s in slots])
-    for a, b in zip(*res):  # tile shape changes the schedule, not the per-site arithmetic
-        assert np.array_equal(a["x"], b["x"])
+    for other in res[1:]:  # tile shape changes the schedule, not the per-site arithmetic
+        for a, b in zip(res[0], other):
+            assert np.array_equal(a["x"], b["x"])
