@@ -171,6 +171,27 @@ __device__ __forceinline__ bool window_site(const Geom &g, const Window &w, int 
   return true;
 }
 
+// Same candidate walk, returning the ideal image position relative to the query point
+// (ox, oy, oz) instead of the periodic shift.
+__device__ __forceinline__ bool window_site_rel(const Geom &g, const Window &w, int c, double qx, double qy,
+                                                double qz, double a0, double R, long long &idx, double &ox,
+                                                double &oy, double &oz) {
+  const int ix = c % w.nx;
+  const int rest = c / w.nx;
+  const int iy = rest % w.ny;
+  const int iz = rest / w.ny;
+  const int gx = w.gx0 + ix, gy = w.gy0 + iy, gz = w.gz0 + iz;
+  const double h = 0.5 * (double)(gx & 1);
+  ox = 0.5 * a0 * gx - qx;
+  oy = a0 * (gy + h) - qy;
+  oz = a0 * (gz + h) - qz;
+  if (ox * ox + oy * oy + oz * oz >= R * R) return false;
+  const int bxd = 2 * g.bcx;
+  const int bx = pmod_i(gx, bxd), by = pmod_i(gy, g.by), bz = pmod_i(gz, g.bz);
+  idx = ext_index(g, bx & 1, bx >> 1, by, bz);
+  return true;
+}
+
 __device__ __forceinline__ double min_image(double d, double L, double iL) { return d - L * rint(d * iL); }
 
 } // namespace mb

@@ -131,7 +131,7 @@ __device__ void rho_tiles(const EnsParams &P, TileCtx &T, const float4 *s_fv) {
     double e_site = 0.0;
     int code = -1;
     if (me.valid) code = d.code[me.i];
-    const bool work = me.valid && code >= 0 && !(code & MB_FLAG_ITL);
+    const bool work = me.valid && code >= 0; // flagged sites: lattice part only (see itl_item)
     float rs0 = 0.f, rc0 = 0.f, rs1 = 0.f, rc1 = 0.f;
     if (work) {
       const float4 u = tile[me.o];
@@ -171,7 +171,9 @@ __device__ void rho_tiles(const EnsParams &P, TileCtx &T, const float4 *s_fv) {
     __syncwarp();
     if (lane == 0) mbar_arrive(&T.empty[b]); // tile data no longer needed by this warp
     if (warp == 0) producer_issue(P, T, pr);  // tile i + 2 into this buffer
-    if (work) {
+    if (work && (code & MB_FLAG_ITL)) {
+      d.rho[me.i] = (float)(((double)rs0 + (double)rs1) + ((double)rc0 + (double)rc1));
+    } else if (work) {
       const double rho = ((double)rs0 + (double)rs1) + ((double)rc0 + (double)rc1);
       const double df = dF64(P.P, code & 0x3F, rho);
       float4 *u4 = d.u4[d.cur];
@@ -224,7 +226,7 @@ __device__ void force_tiles(const EnsParams &P, TileCtx &T, const float2 *s_fd) 
       uy = d.uy[me.i];
       uz = d.uz[me.i];
     }
-    const bool work = me.valid && code >= 0 && !(code & MB_FLAG_ITL);
+    const bool work = me.valid && code >= 0; // flagged sites: lattice part only (see itl_item)
     float2 fs0 = make_float2(0.f, 0.f), fc0 = fs0, fs1 = fs0, fc1 = fs0;
     float zs0 = 0.f, zc0 = 0.f, ps0 = 0.f, pc0 = 0.f, zs1 = 0.f, zc1 = 0.f, ps1 = 0.f, pc1 = 0.f;
     if (work) {
@@ -285,15 +287,19 @@ __device__ void force_tiles(const EnsParams &P, TileCtx &T, const float2 *s_fd) 
       d.fx[i] = (float)fx;
       d.fy[i] = (float)fy;
       d.fz[i] = (float)fz;
+      if (ENERGY) e_pair = ((double)ps0 + (double)ps1) + ((double)pc0 + (double)pc1);
+    }
+    if (work && !(code & MB_FLAG_ITL)) { // flagged sites are integrated by the interstitial items
+      const long long i = me.i;
+      const double fx = ((double)fs0.x + (double)fs1.x) + ((double)fc0.x + (double)fc1.x);
+      const double fy = ((double)fs0.y + (double)fs1.y) + ((double)fc0.y + (double)fc1.y);
+      const double fz = ((double)zs0 + (double)zs1) + ((double)zc0 + (double)zc1);
       if (d.primed) {
         vx += P.h * fx;
         vy += P.h * fy;
         vz += P.h * fz;
       }
-      if (ENERGY) {
-        e_kin = 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E;
-        e_pair = ((double)ps0 + (double)ps1) + ((double)pc0 + (double)pc1);
-      }
+      if (ENERGY) e_kin = 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E;
       vx += P.h * fx;
       vy += P.h * fy;
       vz += P.h * fz;
@@ -374,10 +380,14 @@ __global__ void __launch_bounds__(ENS_THREADS, 1) k_ens_step(const __grid_consta
     itl_items<false, ENERGY>(P);
     if (!grid_sync(P.bar, P.err)) return;
   }
-  // D + E: forces and integration
+  // D: forces and integration over lattice tiles (flagged sites: lattice part only)
   force_tiles<ENERGY>(P, T, s_fd);
-  if (P.n_itl_lats > 0) itl_items<true, ENERGY>(P);
   if (!grid_sync(P.bar, P.err)) return;
+  // E: forces and integration of flagged sites and interstitials
+  if (P.n_itl_lats > 0) {
+    itl_items<true, ENERGY>(P);
+    if (!grid_sync(P.bar, P.err)) return;
+  }
   // F: step bookkeeping
   if (blockIdx.x == 0) {
     for (int l = threadIdx.x; l < P.n_lats; l += blockDim.x) {

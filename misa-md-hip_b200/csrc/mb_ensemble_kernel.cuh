@@ -263,24 +263,6 @@ __device__ __forceinline__ Geom lat_geom(const LatDesc &d) {
 
 __device__ __forceinline__ bool lat_active(const LatDesc &d) { return !d.primed || d.steps_done < d.steps_target; }
 
-// Absolute position of ext site j: ideal site + FP32 displacement (ghost sites are
-// periodic images: the ideal position continues past the box, the displacement is the
-// source site's).
-__device__ __forceinline__ void lat_pos(const LatDesc &d, const float4 *u4, long long j, double a0, double &x,
-                                        double &y, double &z) {
-  const int s = (int)(j / d.E);
-  const long long r = j - (long long)s * d.E;
-  const long long row = r / d.ecx;
-  const int cx = (int)(r - row * d.ecx);
-  const int zz = (int)(row / d.ey);
-  const int yy = (int)(row - (long long)zz * d.ey);
-  const float4 u = u4[j];
-  const double h = 0.5 * s;
-  x = 0.5 * a0 * (double)(2 * (cx - 2) + s) + (double)u.x;
-  y = a0 * ((double)(yy - 2) + h) + (double)u.y;
-  z = a0 * ((double)(zz - 2) + h) + (double)u.z;
-}
-
 __device__ __forceinline__ void ideal_pos(int s, int cx, int y, int z, double a0, double &X, double &Y, double &Z) {
   const double h = 0.5 * s;
   X = 0.5 * a0 * (double)(2 * cx + s);

@@ -157,7 +157,10 @@ __device__ __forceinline__ void itl_mark_one(const EnsParams &P, const LatDesc &
 }
 
 // Work of one warp on item w of lattice d: a flagged site (w < nflag) or an
-// interstitial.  FORCE = false: density pass; true: force + integration pass.
+// interstitial.  FORCE = false: density pass; true: force + integration pass.  A
+// flagged site's lattice-pair part comes from the lattice kernels (rho / f of the site);
+// its interstitial pairs, df, integration and ghost images are done here.  An
+// interstitial's pairs (lattice window and other interstitials) are all done here, FP64.
 template <bool FORCE, bool ENERGY>
 __device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag) {
   const int lane = threadIdx.x & 31;
@@ -205,27 +208,28 @@ __device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag)
     }
   };
   if (is_site) {
-    for (int k = lane; k < P.n_st; k += 32) {
-      const char4 e = P.sd[s][k];
-      const long long j = i + (long long)e.x * d.E + ((long long)e.w * d.ey + e.z) * d.ecx + e.y;
-      const int cj = d.code[j];
-      if (cj < 0) continue;
-      double xj, yj, zj;
-      lat_pos(d, u4, j, P.a0, xj, yj, zj);
-      pair(xi - xj, yi - yj, zi - zj, cj & 0x3F, FORCE ? (double)u4[j].w : 0.0);
+    // the lattice kernels summed this site's lattice pairs (FP32, compensated) into
+    // rho / f; only the interstitial pairs are added here
+    if (lane == 0) {
+      if (FORCE) {
+        fx = (double)d.fx[i];
+        fy = (double)d.fy[i];
+        fz = (double)d.fz[i];
+      } else {
+        acc0 = (double)d.rho[i];
+      }
     }
   } else {
     const Window win = make_window(xi, yi, zi, P.a0, P.reach);
     const int ncand = win.nx * win.ny * win.nz;
     for (int c = lane; c < ncand; c += 32) {
       long long j;
-      double sx, sy, sz;
-      if (!window_site(g, win, c, xi, yi, zi, P.a0, P.reach, j, sx, sy, sz)) continue;
+      double ox, oy, oz;
+      if (!window_site_rel(g, win, c, xi, yi, zi, P.a0, P.reach, j, ox, oy, oz)) continue;
       const int cj = d.code[j];
       if (cj < 0) continue;
-      double xj, yj, zj;
-      lat_pos(d, u4, j, P.a0, xj, yj, zj);
-      pair(xi - (xj + sx), yi - (yj + sy), zi - (zj + sz), cj & 0x3F, FORCE ? (double)u4[j].w : 0.0);
+      const float4 uj = u4[j];
+      pair(-(ox + (double)uj.x), -(oy + (double)uj.y), -(oz + (double)uj.z), cj & 0x3F, FORCE ? (double)uj.w : 0.0);
     }
   }
   for (int K = lane; K < d.n_itl; K += 32) {

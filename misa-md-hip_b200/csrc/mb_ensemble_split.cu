@@ -200,7 +200,7 @@ __device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStenci
                                               const float2 *s_f, float ma0, long long i, unsigned pos) {
   const int s = (int)(pos >> 31);
   const int code = d.code[i];
-  if (code < 0 || (code & MB_FLAG_ITL)) return 0.0;
+  if (code < 0) return 0.0;
   const float4 *u4 = d.u4[d.cur];
   float4 *uw = d.u4[d.cur];
   const float4 u = __ldg(u4 + i);
@@ -251,9 +251,10 @@ __device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStenci
     }
   }
   const double rho = (double)rs + (double)rc;
+  d.rho[i] = (float)rho;
+  if (code & MB_FLAG_ITL) return 0.0; // lattice part only: the interstitial items finish the site
   const double df = dF64(P.P, code & 0x3F, rho);
   reinterpret_cast<float *>(uw + i)[3] = (float)df;
-  d.rho[i] = (float)rho;
   int sx, cx, y, z;
   mx_unpack(pos, sx, cx, y, z);
   const Geom g = lat_geom(d);
@@ -270,7 +271,7 @@ __device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStenci
                                               double &e_pair, double &e_kin) {
   const int s = (int)(pos >> 31);
   const int code = d.code[i];
-  if (code < 0 || (code & MB_FLAG_ITL)) return;
+  if (code < 0) return;
   const float4 *u4 = d.u4[d.cur];
   float4 *un = d.u4[d.cur ^ 1];
   const float4 *ptab = P.P.ps32;
@@ -350,16 +351,15 @@ __device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStenci
   d.fx[i] = (float)fx;
   d.fy[i] = (float)fy;
   d.fz[i] = (float)fz;
+  if (ENERGY) e_pair += (double)ps + (double)pc;
+  if (code & MB_FLAG_ITL) return; // lattice part only: the interstitial items integrate the site
   double vx = d.vx[i], vy = d.vy[i], vz = d.vz[i];
   if (d.primed) {
     vx += P.h * fx;
     vy += P.h * fy;
     vz += P.h * fz;
   }
-  if (ENERGY) {
-    e_kin += 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E;
-    e_pair += (double)ps + (double)pc;
-  }
+  if (ENERGY) e_kin += 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E;
   vx += P.h * fx;
   vy += P.h * fy;
   vz += P.h * fz;
