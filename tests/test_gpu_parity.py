@@ -71,6 +71,32 @@ def test_hook_rho_df_force_match_oracle(hooks, n_types, vac, start):
     assert k > 0 and c > 0
 
 
+def test_hook_with_setfl_alloy_matches_oracle(hooks, tmp_path):
+    # a two-element Fe-Cu table written as a setfl file and read back drives both paths
+    t = mb.potential.alloy_analytic(2, nr=3000, nrho=3000)
+    path = tmp_path / "fecu.setfl"
+    mb.potential.write_setfl(path, t, elements=["Fe", "Cu"], numbers=[26, 29])
+    tables, meta = mb.potential.read_setfl(path)
+    assert meta["elements"] == ["Fe", "Cu"]
+    sc = make(cells=(6, 7, 5), temperature=900.0, vacancy=0.01, seed=23, jitter=0.1, tables=tables, n_types=2)
+    dom, odom, even, odd = _hook_setup(hooks, sc)
+    ext_gpu = sc.ext()
+    ext_orc = ext_gpu.copy().view(orc.ATOM)
+    pot = sc.orc_pot()
+    hooks.rho_calc(ext_gpu, sc.cutoff)
+    orc.rho_pass(pot, odom, ext_orc, even, odd, sc.cutoff)
+    L = [sc.cells[0] * A0, sc.cells[1] * A0, sc.cells[2] * A0]
+    orc.ghost_fill(odom, ext_gpu.view(orc.ATOM), L, 2)
+    orc.ghost_fill(odom, ext_orc, L, 2)
+    hooks.force_calc(ext_gpu, sc.cutoff)
+    orc.force_pass(pot, odom, ext_orc, even, odd, sc.cutoff)
+    bg, bo = _box(ext_gpu, sc), _box(ext_orc, sc)
+    live = bg["type"] >= 0
+    assert set(np.unique(bg["type"][live])) == {0, 1}
+    assert rel_err(bg["rho"][live], bo["rho"][live]) < 1e-12
+    assert rel_err(bg["f"][live], bo["f"][live]) < F_TOL
+
+
 def test_hook_df_from_rho_matches_oracle(hooks):
     sc = make(cells=(6, 6, 6), temperature=600.0, vacancy=0.01, seed=4)
     dom, odom, even, odd = _hook_setup(hooks, sc)
