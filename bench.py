@@ -395,6 +395,78 @@ def mixed_comparison(args, mb, wl, box, itl, n_atoms, fp64_rate, pg) -> dict:
             "dtype": "f32 pairs + two-sum, f64 state", **kern}
 
 
+def run_nve(args, mb, world, rank, local, pg) -> None:
+    """The mixed-precision NVE run of the 200^3-cell workload (16 M atoms, 900 K, 0.5%
+    vacancies, 763 interstitials): --nve-steps steps with the total energy recorded and
+    the relative force RMS error against the FP64 path checked every --check-every
+    steps.  At each check the mixed state (positions, velocities, mixed forces at those
+    positions) is read back and the FP64 path evaluates the forces at the same positions;
+    the FP64 path matches the CPU oracle to ~1e-15 (tests/test_gpu_parity.py).  Energy
+    drift is (E(t) - E(0)) / N in eV/atom."""
+    mb.check(mb.lib().mb_env_init(local))
+    wl = dict(WORKLOADS["mixed"])
+    if args.nve_itl is not None:  # interstitial count override (0: vacancies only)
+        wl["n_itl"] = args.nve_itl
+        wl["name"] = wl["name"].replace("itl763", f"itl{args.nve_itl}")
+    if args.nve_precision == "fp64":
+        wl["name"] = wl["name"].replace("mixed", "fp64")
+    box, itl = build_state(mb, wl)
+    n_atoms = int((box["type"] >= 0).sum()) + itl.shape[0]
+    tables = mb.potential.fe_analytic()
+    kw = dict(lattice_const=A0, mass=MASS, dt=DT, cutoff=RC, stencil_skin=SKIN, max_interstitials=max(1, itl.shape[0]))
+    every = max(1, args.check_every)
+    prec = mb.MB_PREC_FP64 if args.nve_precision == "fp64" else mb.MB_PREC_MIXED
+    mixed = mb.Sim(wl["cells"], tables, precision=prec, **kw)
+    ref = mb.Sim(wl["cells"], tables, precision=mb.MB_PREC_FP64, **kw)
+    mixed.upload(box, itl)
+    del box, itl
+    steps_done, rms, rms_steps, e_rec = 0, [], [], []
+    t_md = 0.0
+    mixed.run(0, energy_every=every)  # priming pass: forces and the step-0 energies
+    e_rec.append(mixed.energies())  # each run() keeps only its own energy samples
+    clocks = ClockSampler(local).start()
+    while True:
+        b, i = mixed.download()
+        live = b["type"] >= 0
+        f32 = np.concatenate([b["f"][live], i["f"]])
+        ref.upload(b, i)
+        ref.run(0)
+        rb, ri = ref.download()
+        f64 = np.concatenate([rb["f"][live], ri["f"]])
+        rms.append(float(np.sqrt(np.sum((f32 - f64) ** 2) / np.sum(f64 ** 2))))
+        rms_steps.append(steps_done)
+        del b, i, rb, ri, f32, f64, live
+        if steps_done >= args.nve_steps:
+            break
+        n = min(every, args.nve_steps - steps_done)
+        t0 = time.perf_counter()
+        mixed.run(n, energy_every=every)
+        t_md += time.perf_counter() - t0
+        steps_done += n
+        e_rec.append(mixed.energies())
+    clk = clocks.stop()
+    e = np.concatenate([x for x in e_rec if x.size], axis=0)
+    mixed.close()
+    ref.close()
+    e0 = float(e[0, 1] + e[0, 2])
+    drift = (e[:, 1] + e[:, 2] - e0) / n_atoms
+    if rank == 0:
+        print(json.dumps({
+            "metric": "atom-steps/s", "value": n_atoms * steps_done * world / t_md, "unit": "atom-steps/s",
+            "n_gpus": world, "steps": steps_done, "warmup": 0, "ms_per_step": t_md * 1e3 / max(1, steps_done),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == mb.MB_PREC_FP64 else "f32+f64",
+            "data": "synthetic (seeded lattice, analytic tabulated potential)",
+            "config": {"workload": wl["name"] + "_nve", "cells": list(wl["cells"]), "atoms_per_gpu": n_atoms,
+                       "check_every": every, "timing": "wall clock of the MD segments (energy steps included)"},
+            "force_rms_rel_err_vs_fp64": {"max": max(rms), "mean": float(np.mean(rms)), "final": rms[-1],
+                                          "steps": rms_steps, "values": rms},
+            "energy_drift_ev_per_atom": {"max_abs": float(np.max(np.abs(drift))), "final": float(drift[-1]),
+                                         "steps": e[:, 0].astype(int).tolist(), "values": drift.tolist()},
+            "bars": {"force_rms": 1e-6, "drift": 1e-5}, "clocks": clk, "cpu_baseline": None, "e2e": None,
+            "gpu_launches": None}), flush=True)
+
+
 def run_ensemble(args, mb, world, rank, local, pg) -> None:
     """512 independent lattices (edges uniform in [8, 40] cells, seed 11; temperature
     uniform in [300, 1200] K; 0-1% vacancies), mixed precision, every lattice advanced
@@ -485,10 +557,14 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=sorted(WORKLOADS) + ["ensemble", "serve"], default="scale")
+    ap.add_argument("--config", choices=sorted(WORKLOADS) + ["ensemble", "serve", "nve"], default="scale")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     ap.add_argument("--requests", type=int, default=32, help="requests served by --config serve")
+    ap.add_argument("--nve-steps", type=int, default=10000, help="steps of --config nve")
+    ap.add_argument("--check-every", type=int, default=100, help="force / energy check interval of --config nve")
+    ap.add_argument("--nve-precision", choices=["mixed", "fp64"], default="mixed", help="path run by --config nve")
+    ap.add_argument("--nve-itl", type=int, default=None, help="interstitials of --config nve (default 763)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, pg = dist_setup()
@@ -501,6 +577,8 @@ def main() -> None:
             run_ensemble(args, mb, world, rank, local, pg)
         elif args.config == "serve":
             run_serve(args, mb, world, rank, local, pg)
+        elif args.config == "nve":
+            run_nve(args, mb, world, rank, local, pg)
         else:
             run_ours(args, mb, wl, world, rank, local, pg)
     finally:

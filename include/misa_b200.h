@@ -106,7 +106,8 @@ int mb_pot_init(const mb_eam_tables *tables);
  * ghost-extended AoS array (ghosts already filled); rho and df are written back. */
 int mb_eam_rho_calc(mb_atom_element *atoms, double cutoff_radius);
 /* hip_eam_df_calc (src/hip_arch_acc_imp.cpp:183-205): a no-op in the full-neighbour
- * build, exactly like the reference (df is produced by the rho pass). */
+ * build, exactly like the reference (df is produced by the rho pass); in
+ * half-neighbour mode df = F'(rho) for every box site with type >= 0 (calDf). */
 int mb_eam_df_calc(mb_atom_element *atoms, double cutoff_radius);
 /* hip_eam_force_calc (src/hip_arch_acc_imp.cpp:207-225): f = sum del * fpair over
  * the stencil, overwriting f of every box site with type >= 0 (needs df of the
@@ -127,6 +128,16 @@ int mb_eam_rho_calc_noalloc(mb_atom_element *atoms, double cutoff_radius);
 /* The calDf kernel of the half-neighbour build (src/kernels/hip_kernels.hip.cpp:21-40):
  * df = F'(rho) for every box site with type >= 0. */
 int mb_eam_df_from_rho(mb_atom_element *atoms);
+/* The reference's USE_NEWTONS_THIRD_LOW build (src/md_hip_config.h:12), chosen at
+ * run time: with enable != 0, mb_nei_offset_init takes half stencils (one offset of
+ * each opposite pair, MISA-MD's nei_half_*_offsets, src/hip_arch_acc_imp.cpp:118-130)
+ * and every pair (i, i + o) with i a box site is evaluated once, both atoms receiving
+ * their share (src/kernels/kernel_pairs.hpp:21-32, 39-60).  mb_eam_rho_calc then
+ * rewrites rho of every ext record, box and ghost, with the shares it received (no
+ * df); the host adds ghost shares to their owners and calls mb_eam_df_calc;
+ * mb_eam_force_calc rewrites f of every ext record the same way.  Switching modes
+ * drops the stencil: mb_nei_offset_init must follow.  Default: full neighbour. */
+int mb_set_half_neighbour(int enable);
 /* hip_create_atoms_mem (src/mem.cpp:14-23): page-locked host allocation of
  * size_x*size_y*size_z elements; *allocated = 1 when this library allocated. */
 int mb_create_atoms_mem(void **atoms, size_t data_type_size, int64_t size_x, int64_t size_y, int64_t size_z,

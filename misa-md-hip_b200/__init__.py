@@ -56,6 +56,11 @@ class Hooks:
     def df_from_rho(self, atoms: np.ndarray) -> None:
         check(lib().mb_eam_df_from_rho(ptr(atoms)))
 
+    def set_half_neighbour(self, enable: bool) -> None:
+        """The reference's USE_NEWTONS_THIRD_LOW build at run time (half stencils; rho
+        and f shares written to box and ghost records); nei_offset_init must follow."""
+        check(lib().mb_set_half_neighbour(int(enable)))
+
     def force_calc(self, atoms: np.ndarray, cutoff: float) -> None:
         assert atoms.dtype == ATOM_DTYPE
         check(lib().mb_eam_force_calc(ptr(atoms), cutoff))

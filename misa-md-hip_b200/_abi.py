@@ -86,6 +86,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_eam_df_calc": (_I, [_P, _D]),
     "mb_eam_force_calc": (_I, [_P, _D]),
     "mb_eam_df_from_rho": (_I, [_P]),
+    "mb_set_half_neighbour": (_I, [C.c_int]),
     "mb_create_atoms_mem": (_I, [C.POINTER(_P), C.c_size_t, C.c_int64, C.c_int64, C.c_int64, _PI]),
     "mb_release_atoms_mem": (_I, [_P, _PI]),
     "mb_cli_set_batches": (_I, [C.c_uint]),

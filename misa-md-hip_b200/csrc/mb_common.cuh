@@ -13,6 +13,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/misa_b200.h"
 
@@ -162,19 +163,31 @@ int launch_reduce(const double *partials, int n, double *out, cudaStream_t s);
 int energy_partials_needed();
 
 // AoS conversion (mb_layout.cu)
+// Records whose type has no potential table (type >= n_types) raise *bad_type and
+// are kept out of the passes as vacant sites.
 int launch_unpack_ext(const Geom &g, const mb_atom_element *aos, int ext_x, int ext_y, int ext_z, Lattice64 L,
-                      int with_df, int *bad_type, cudaStream_t s);
+                      int with_df, int *bad_type, int n_types, cudaStream_t s);
 int launch_pack_ext(const Geom &g, mb_atom_element *aos, int ext_x, int ext_y, const Lattice64 &L, int what,
                     cudaStream_t s); // what: 1 rho+df, 2 force, 3 df only
 int launch_unpack_box(const Geom &g, const mb_atom_element *aos, Lattice64 L, int with_f, int *bad_type,
-                      cudaStream_t s);
+                      int n_types, cudaStream_t s);
 int launch_pack_box(const Geom &g, mb_atom_element *aos, const Lattice64 &L, const double *px, const double *py,
                     const double *pz, double h, int unkick, cudaStream_t s);
 int launch_unpack_box_ids(const Geom &g, const mb_atom_element *aos, Lattice64 L, int with_f, int *bad_type,
-                          int64_t *ids, cudaStream_t s);
+                          int64_t *ids, int n_types, cudaStream_t s);
 int launch_pack_box_ids(const Geom &g, mb_atom_element *aos, const Lattice64 &L, const double *px, const double *py,
                         const double *pz, double h, int unkick, const int64_t *ids, cudaStream_t s);
 int launch_df_from_rho(const Geom &g, const DevPot &pot, const Lattice64 &L, cudaStream_t s);
+
+// Half-neighbour hook passes (mb_half.cu): a decoded half-stencil offset.
+struct HalfOff {
+  long long off; // linear offset in the host's ext array
+  int dx, dy, dz, pad_;
+};
+int half_stencil_build(const mb_device_domain &d, const int64_t *even, size_t n_even, const int64_t *odd, size_t n_odd,
+                       std::vector<HalfOff> &out, int &cap);
+int launch_half64(bool force, mb_atom_element *aos, const mb_device_domain &d, const HalfOff *st, int cap,
+                  const int n[2], const DevPot &P, double rc2, int *bad, cudaStream_t s);
 
 // ------------------------------------------------------------ utilities
 int device_sm_count();

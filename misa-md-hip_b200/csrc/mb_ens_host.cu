@@ -57,7 +57,7 @@ static int encode_tile_map(CUtensorMap *m, float4 *u4, int ecx, int ey, int ez, 
 }
 
 // ------------------------------------------------------------ kernels
-__global__ void k_ens_upload(LatDesc d, const mb_atom_element *aos, int64_t *ids, double a0, int *bad) {
+__global__ void k_ens_upload(LatDesc d, const mb_atom_element *aos, int64_t *ids, double a0, int *bad, int n_types) {
   const long long n = 2LL * d.bcx * d.by * d.bz;
   const int bxd = 2 * d.bcx;
   const Geom g = lat_geom(d);
@@ -69,7 +69,7 @@ __global__ void k_ens_upload(LatDesc d, const mb_atom_element *aos, int64_t *ids
     const long long i = (long long)s * d.E + ((long long)(bz + 2) * d.ey + by + 2) * d.ecx + cx + 2;
     const mb_atom_element &a = aos[t];
     int type = a.type;
-    if (type >= 64) {
+    if (type >= n_types) { // no table for it: flagged, and kept out of the pair loops
       *bad = 1;
       type = -1;
     }
@@ -949,7 +949,7 @@ int mb_ensemble_add(mb_ensemble *e, const mb_lattice_spec *spec, const mb_atom_e
   cudaMemsetAsync(e->d_bad, 0, sizeof(int), s);
   cudaMemcpyAsync(stage, box, nb * sizeof(mb_atom_element), cudaMemcpyHostToDevice, s);
   int grid = (int)std::min<size_t>((nb + 255) / 256, 16 * (size_t)device_sm_count());
-  k_ens_upload<<<grid, 256, 0, s>>>(d, stage, L.ids, a0, e->d_bad);
+  k_ens_upload<<<grid, 256, 0, s>>>(d, stage, L.ids, a0, e->d_bad, e->P.P.n_types);
   if (n_itl > 0) {
     std::vector<double> buf(n_itl);
     std::vector<int8_t> t(n_itl, 0);
@@ -973,7 +973,7 @@ int mb_ensemble_add(mb_ensemble *e, const mb_lattice_spec *spec, const mb_atom_e
   cudaError_t er = cudaStreamSynchronize(s);
   cudaFree(stage);
   if (er != cudaSuccess) return undo(cuda_fail(er, "lattice upload"));
-  if (bad) return undo(fail(MB_ERR_ARG, "atom type >= 64 is not supported"));
+  if (bad) return undo(fail(MB_ERR_ARG, "atom type without a potential table"));
   d.cur = 0;
   d.primed = 0;
   d.steps_done = 0;

@@ -38,6 +38,10 @@ struct HookCtx {
   int8_t *code = nullptr;
   int *bad = nullptr;
   float kernel_ms = 0.f, copy_ms = 0.f;
+  // half-neighbour mode (the reference's USE_NEWTONS_THIRD_LOW build)
+  bool half = false;
+  HalfOff *d_half = nullptr;
+  int half_cap = 0, half_n[2] = {0, 0};
 };
 
 static HookCtx g_ctx;
@@ -81,6 +85,13 @@ static Lattice64 lattice_view(HookCtx &c) {
   return L;
 }
 
+static void free_half(HookCtx &c) {
+  if (c.d_half) cudaFree(c.d_half);
+  c.d_half = nullptr;
+  c.half_cap = 0;
+  c.half_n[0] = c.half_n[1] = 0;
+}
+
 static int require_ready(const HookCtx &c) {
   if (!c.env) return fail(MB_ERR_STATE, "mb_env_init has not been called");
   if (!c.domain) return fail(MB_ERR_STATE, "mb_domain_init has not been called");
@@ -107,7 +118,8 @@ static int run_hook(HookCtx &c, mb_atom_element *atoms, int with_df, int pack_wh
   MB_CUDA(cudaMemcpyAsync(c.aos, atoms, n * sizeof(mb_atom_element), cudaMemcpyHostToDevice, s));
   MB_CUDA(cudaEventRecord(c.ev[1], s));
   Lattice64 L = lattice_view(c);
-  MB_TRY(launch_unpack_ext(c.g, c.aos, d.ext_size_x, d.ext_size_y, d.ext_size_z, L, with_df, c.bad, s));
+  MB_TRY(launch_unpack_ext(c.g, c.aos, d.ext_size_x, d.ext_size_y, d.ext_size_z, L, with_df, c.bad,
+                           pot_dev(c.potp).n_types, s));
   MB_TRY(body(L, s));
   MB_TRY(launch_pack_ext(c.g, c.aos, d.ext_size_x, d.ext_size_y, L, pack_what, s));
   MB_CUDA(cudaEventRecord(c.ev[2], s));
@@ -123,7 +135,37 @@ static int run_hook(HookCtx &c, mb_atom_element *atoms, int with_df, int pack_wh
   cudaEventElapsedTime(&b, c.ev[2], c.ev[3]);
   c.kernel_ms = k;
   c.copy_ms = a + b;
-  if (bad) return fail(MB_ERR_ARG, "atom type >= 64 is not supported (treated as vacant)");
+  if (bad) return fail(MB_ERR_ARG, "atom type without a potential table (treated as vacant)");
+  return MB_OK;
+}
+
+// Half-neighbour pass: the whole ext array goes in, every record's rho (or f) is
+// rewritten with the shares it received, and the whole array comes back (ghost
+// records carry the shares owed to atoms owned elsewhere).
+static int run_half(HookCtx &c, mb_atom_element *atoms, bool force, double rc2) {
+  if (!atoms) return fail(MB_ERR_ARG, "null atoms array");
+  MB_TRY(require_ready(c));
+  MB_TRY(ensure_buffers(c));
+  const size_t n = c.n_ext;
+  cudaStream_t s = c.stream;
+  MB_CUDA(cudaMemsetAsync(c.bad, 0, sizeof(int), s));
+  MB_CUDA(cudaEventRecord(c.ev[0], s));
+  MB_CUDA(cudaMemcpyAsync(c.aos, atoms, n * sizeof(mb_atom_element), cudaMemcpyHostToDevice, s));
+  MB_CUDA(cudaEventRecord(c.ev[1], s));
+  MB_TRY(launch_half64(force, c.aos, c.dom, c.d_half, c.half_cap, c.half_n, pot_dev(c.potp), rc2, c.bad, s));
+  MB_CUDA(cudaEventRecord(c.ev[2], s));
+  MB_CUDA(cudaMemcpyAsync(atoms, c.aos, n * sizeof(mb_atom_element), cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaEventRecord(c.ev[3], s));
+  int bad = 0;
+  MB_CUDA(cudaMemcpyAsync(&bad, c.bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  float a = 0, b = 0, k = 0;
+  cudaEventElapsedTime(&a, c.ev[0], c.ev[1]);
+  cudaEventElapsedTime(&k, c.ev[1], c.ev[2]);
+  cudaEventElapsedTime(&b, c.ev[2], c.ev[3]);
+  c.kernel_ms = k;
+  c.copy_ms = a + b;
+  if (bad) return fail(MB_ERR_ARG, "atom type without a potential table (treated as vacant)");
   return MB_OK;
 }
 
@@ -154,6 +196,8 @@ int mb_env_clean(void) {
   HookCtx &c = g_ctx;
   if (c.stream) cudaStreamSynchronize(c.stream);
   free_buffers(c);
+  free_half(c);
+  c.half = false;
   if (c.potp) pot_free(c.potp);
   c.potp = nullptr;
   for (auto &e : c.ev)
@@ -198,6 +242,24 @@ int mb_domain_init(const mb_device_domain *d) {
   c.stencil = false;
   c.even.clear();
   c.odd.clear();
+  free_half(c);
+  return MB_OK;
+}
+
+int mb_set_half_neighbour(int enable) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  HookCtx &c = g_ctx;
+  if (!c.env) return fail(MB_ERR_STATE, "mb_env_init has not been called");
+  const bool h = enable != 0;
+  if (h != c.half) {
+    // full and half stencils are different offset sets: the next pass needs
+    // mb_nei_offset_init with the kind this mode takes
+    c.half = h;
+    c.stencil = false;
+    c.even.clear();
+    c.odd.clear();
+    free_half(c);
+  }
   return MB_OK;
 }
 
@@ -210,6 +272,21 @@ int mb_nei_offset_init(const int64_t *nei_even, size_t n_even, const int64_t *ne
   // even ghost the global parity of its sites is (s + box_index_start_x) & 1
   // (the reference selects the stencil by (x + box_index_start_x) % 2,
   // src/kernels/kernel_itl.hpp:82).
+  if (c.half) {
+    std::vector<HalfOff> h;
+    int cap = 0;
+    MB_TRY(half_stencil_build(c.dom, nei_even, n_even, nei_odd, n_odd, h, cap));
+    free_half(c);
+    MB_CUDA(cudaMalloc(&c.d_half, h.size() * sizeof(HalfOff)));
+    MB_CUDA(cudaMemcpy(c.d_half, h.data(), h.size() * sizeof(HalfOff), cudaMemcpyHostToDevice));
+    c.half_cap = cap;
+    c.half_n[0] = (int)n_even;
+    c.half_n[1] = (int)n_odd;
+    c.even.assign(nei_even, nei_even + n_even);
+    c.odd.assign(nei_odd, nei_odd + n_odd);
+    c.stencil = true;
+    return MB_OK;
+  }
   const int par[2] = {(int)(c.dom.box_index_start_x & 1), (int)((1 + c.dom.box_index_start_x) & 1)};
   StencilSet st;
   MB_TRY(stencil_from_linear(nei_even, n_even, nei_odd, n_odd, c.dom.ext_size_x, c.dom.ext_size_y, c.g, par, &st));
@@ -236,18 +313,23 @@ int mb_eam_rho_calc(mb_atom_element *atoms, double cutoff_radius) {
   std::lock_guard<std::mutex> lk(g_mu);
   HookCtx &c = g_ctx;
   if (!(cutoff_radius > 0)) return fail(MB_ERR_ARG, "cutoff must be > 0");
+  if (c.half) return run_half(c, atoms, false, cutoff_radius * cutoff_radius);
   return run_hook(c, atoms, 0, 1, [&](Lattice64 &L, cudaStream_t s) {
     return launch_rho64(c.g, c.st, pot_dev(c.potp), L, cutoff_radius * cutoff_radius, nullptr, 0, 0, s);
   });
 }
 
 int mb_eam_df_calc(mb_atom_element *atoms, double cutoff_radius) {
-  // Full-neighbour build: df already came out of the rho pass
-  // (src/hip_arch_acc_imp.cpp:184-186 returns at once).
-  (void)atoms;
+  // Full-neighbour mode: df already came out of the rho pass
+  // (src/hip_arch_acc_imp.cpp:184-186 returns at once).  Half-neighbour mode: the
+  // host has added the ghost shares of rho to their owners; df = F'(rho) of the box
+  // sites (calDf, src/kernels/hip_kernels.hip.cpp:21-40).
   (void)cutoff_radius;
   std::lock_guard<std::mutex> lk(g_mu);
-  return require_ready(g_ctx);
+  HookCtx &c = g_ctx;
+  if (!c.half) return require_ready(c);
+  return run_hook(c, atoms, 2, 3,
+                  [&](Lattice64 &L, cudaStream_t s) { return launch_df_from_rho(c.g, pot_dev(c.potp), L, s); });
 }
 
 int mb_eam_df_from_rho(mb_atom_element *atoms) {
@@ -261,6 +343,7 @@ int mb_eam_force_calc(mb_atom_element *atoms, double cutoff_radius) {
   std::lock_guard<std::mutex> lk(g_mu);
   HookCtx &c = g_ctx;
   if (!(cutoff_radius > 0)) return fail(MB_ERR_ARG, "cutoff must be > 0");
+  if (c.half) return run_half(c, atoms, true, cutoff_radius * cutoff_radius);
   return run_hook(c, atoms, 1, 2, [&](Lattice64 &L, cudaStream_t s) {
     StepParams sp{};
     sp.rc2 = cutoff_radius * cutoff_radius;
@@ -361,6 +444,7 @@ extern "C" int mb_eam_rho_calc_noalloc(mb_atom_element *atoms, double cutoff_rad
   if (!atoms) return fail(MB_ERR_ARG, "null atoms array");
   if (!(cutoff_radius > 0)) return fail(MB_ERR_ARG, "cutoff must be > 0");
   MB_TRY(require_ready(c));
+  if (c.half) return fail(MB_ERR_UNSUPPORTED, "mb_eam_rho_calc_noalloc runs the full-neighbour pass only");
   const mb_device_domain &d = c.dom;
   const size_t n = (size_t)d.ext_size_x * d.ext_size_y * d.ext_size_z;
   if (noalloc_bytes(n) > MB_NOALLOC_SCRATCH_BYTES)
@@ -400,7 +484,7 @@ extern "C" int mb_eam_rho_calc_noalloc(mb_atom_element *atoms, double cutoff_rad
   cudaStream_t s = c.stream;
   MB_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s)); // the flag must start at zero on every call
   MB_CUDA(cudaMemcpyAsync(aos, atoms, n * sizeof(mb_atom_element), cudaMemcpyHostToDevice, s));
-  MB_TRY(launch_unpack_ext(c.g, aos, d.ext_size_x, d.ext_size_y, d.ext_size_z, L, 0, bad, s));
+  MB_TRY(launch_unpack_ext(c.g, aos, d.ext_size_x, d.ext_size_y, d.ext_size_z, L, 0, bad, pot_dev(c.potp).n_types, s));
   MB_TRY(launch_rho64(c.g, c.st, pot_dev(c.potp), L, cutoff_radius * cutoff_radius, nullptr, 0, 0, s));
   MB_TRY(launch_pack_ext(c.g, aos, d.ext_size_x, d.ext_size_y, L, 1, s));
   MB_CUDA(cudaMemcpyAsync(atoms + first, aos + first, (last - first + 1) * sizeof(mb_atom_element),

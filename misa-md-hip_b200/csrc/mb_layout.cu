@@ -11,7 +11,7 @@ __device__ __forceinline__ long long split_index(const Geom &g, int ex, int ey, 
 }
 
 __global__ void k_unpack_ext(const Geom g, const mb_atom_element *aos, int ext_x, int ext_y, int ext_z, Lattice64 L,
-                             int with_df, int *bad_type) {
+                             int with_df, int *bad_type, int n_types) {
   const long long n = (long long)ext_x * ext_y * ext_z;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int ex = (int)(t % ext_x);
@@ -20,7 +20,7 @@ __global__ void k_unpack_ext(const Geom g, const mb_atom_element *aos, int ext_x
     const long long i = split_index(g, ex, ey, ez);
     const mb_atom_element &a = aos[t];
     int type = a.type;
-    if (type >= 64) {
+    if (type >= n_types) { // no table for it: flagged, and kept out of the pair loops
       *bad_type = 1;
       type = -1;
     }
@@ -62,7 +62,7 @@ __global__ void k_pack_ext(const Geom g, mb_atom_element *aos, int ext_x, int ex
 }
 
 __global__ void k_unpack_box(const Geom g, const mb_atom_element *aos, Lattice64 L, int with_f, int *bad_type,
-                             int64_t *ids) {
+                             int64_t *ids, int n_types) {
   const long long n = 2LL * g.bcx * g.by * g.bz;
   const int bxd = 2 * g.bcx;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
@@ -73,7 +73,7 @@ __global__ void k_unpack_box(const Geom g, const mb_atom_element *aos, Lattice64
                         (bx >> 1) + g.gcx;
     const mb_atom_element &a = aos[t];
     int type = a.type;
-    if (type >= 64) {
+    if (type >= n_types) { // no table for it: flagged, and kept out of the pair loops
       *bad_type = 1;
       type = -1;
     }
@@ -171,9 +171,9 @@ static int flat_grid(long long n) {
 }
 
 int launch_unpack_ext(const Geom &g, const mb_atom_element *aos, int ext_x, int ext_y, int ext_z, Lattice64 L,
-                      int with_df, int *bad_type, cudaStream_t s) {
+                      int with_df, int *bad_type, int n_types, cudaStream_t s) {
   k_unpack_ext<<<flat_grid((long long)ext_x * ext_y * ext_z), 256, 0, s>>>(g, aos, ext_x, ext_y, ext_z, L, with_df,
-                                                                          bad_type);
+                                                                          bad_type, n_types);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
@@ -186,15 +186,15 @@ int launch_pack_ext(const Geom &g, mb_atom_element *aos, int ext_x, int ext_y, c
 }
 
 int launch_unpack_box_ids(const Geom &g, const mb_atom_element *aos, Lattice64 L, int with_f, int *bad_type,
-                          int64_t *ids, cudaStream_t s) {
-  k_unpack_box<<<flat_grid(2LL * g.bcx * g.by * g.bz), 256, 0, s>>>(g, aos, L, with_f, bad_type, ids);
+                          int64_t *ids, int n_types, cudaStream_t s) {
+  k_unpack_box<<<flat_grid(2LL * g.bcx * g.by * g.bz), 256, 0, s>>>(g, aos, L, with_f, bad_type, ids, n_types);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
 
 int launch_unpack_box(const Geom &g, const mb_atom_element *aos, Lattice64 L, int with_f, int *bad_type,
-                      cudaStream_t s) {
-  return launch_unpack_box_ids(g, aos, L, with_f, bad_type, nullptr, s);
+                      int n_types, cudaStream_t s) {
+  return launch_unpack_box_ids(g, aos, L, with_f, bad_type, nullptr, n_types, s);
 }
 
 int launch_pack_box_ids(const Geom &g, mb_atom_element *aos, const Lattice64 &L, const double *px, const double *py,

@@ -477,7 +477,8 @@ static int upload_itl(mb_sim *s, const mb_atom_element *itl, int32_t n_itl, int 
   std::vector<int8_t> t((size_t)n_itl);
   std::vector<int64_t> ids((size_t)n_itl);
   for (int k = 0; k < n_itl; k++) {
-    if (itl[k].type < 0 || itl[k].type >= 64) return fail(MB_ERR_ARG, "interstitial type must be 0..63");
+    if (itl[k].type < 0 || itl[k].type >= pot_dev(s->pot).n_types)
+      return fail(MB_ERR_ARG, "interstitial type without a potential table");
     t[k] = (int8_t)itl[k].type;
     ids[k] = itl[k].id;
   }
@@ -553,13 +554,13 @@ int mb_sim_upload(mb_sim *s, const mb_atom_element *box_atoms, const mb_atom_ele
   MB_CUDA(cudaMemsetAsync(s->flag_count, 0, 2 * sizeof(int), s->stream));
   for (int b = 0; b < 2; b++) {
     Lattice64 L = sim_lattice(s, b);
-    MB_TRY(launch_unpack_box_ids(s->g, s->stage, L, 1, s->bad, s->id, s->stream));
+    MB_TRY(launch_unpack_box_ids(s->g, s->stage, L, 1, s->bad, s->id, pot_dev(s->pot).n_types, s->stream));
     MB_TRY(launch_images64(s->g, L, 1, s->stream));
   }
   int bad = 0;
   MB_CUDA(cudaMemcpyAsync(&bad, s->bad, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   MB_CUDA(cudaStreamSynchronize(s->stream));
-  if (bad) return fail(MB_ERR_ARG, "atom type >= 64 is not supported");
+  if (bad) return fail(MB_ERR_ARG, "atom type without a potential table");
   MB_TRY(upload_itl(s, itl, n_itl, 1));
   return MB_OK;
 }
@@ -688,7 +689,7 @@ int mb_sim_step_host(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl
                           s->stream));
   Lattice64 L = sim_lattice(s, 0);
   L.nx = L.ny = L.nz = nullptr;
-  MB_TRY(launch_unpack_box_ids(s->g, s->stage, L, 1, s->bad, s->id, s->stream));
+  MB_TRY(launch_unpack_box_ids(s->g, s->stage, L, 1, s->bad, s->id, pot_dev(s->pot).n_types, s->stream));
   MB_TRY(launch_images64(s->g, L, 1, s->stream));
   MB_TRY(upload_itl(s, itl, n_itl, 1));
   Itl64 I = sim_itl(s, 0);

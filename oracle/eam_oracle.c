@@ -293,6 +293,76 @@ void orc_force_pass(const orc_pot *p, const orc_domain *d, orc_atom *atoms, cons
       }
 }
 
+/* ------------------------------------------- half-neighbour (Newton) passes */
+
+/* The reference's USE_NEWTONS_THIRD_LOW build (src/md_hip_config.h:12): the stencil
+ * holds one offset of each opposite pair (src/hip_arch_acc_imp.cpp:118-130 takes
+ * MISA-MD's nei_half_*_offsets), every pair (i, i + o) with i a box site is evaluated
+ * once, and both atoms receive their share (src/kernels/kernel_pairs.hpp:21-32 for
+ * rho, :39-60 for force).  Ghost records receive the shares of pairs whose partner is
+ * owned elsewhere; the host adds them to their owners.  Every ext record's rho (or f)
+ * starts from zero (the reference overwrites the current atom's sum at the end of its
+ * loop, kernel_itl.hpp:90-97, which drops shares written to it earlier by other
+ * threads; the sum here keeps every share).  Sequential on purpose: the scatter has
+ * no races, and the order of the sum is fixed. */
+void orc_rho_pass_half(const orc_pot *p, const orc_domain *d, orc_atom *atoms, const int64_t *even, size_t n_even,
+                       const int64_t *odd, size_t n_odd, double cutoff) {
+  const double rc2 = cutoff * cutoff;
+  const int64_t n = (int64_t)d->ext_size_x * d->ext_size_y * d->ext_size_z;
+  for (int64_t i = 0; i < n; i++) atoms[i].rho = 0.0;
+  for (int64_t z = 0; z < d->box_size_z; z++)
+    for (int64_t y = 0; y < d->box_size_y; y++)
+      for (int64_t x = 0; x < d->box_size_x; x++) {
+        const int64_t i = site_linear(d, x, y, z);
+        orc_atom *a = atoms + i;
+        if (a->type < 0) continue;
+        const int ev = ((x + d->box_index_start_x) % 2) == 0;
+        const int64_t *st = ev ? even : odd;
+        const size_t ns = ev ? n_even : n_odd;
+        for (size_t k = 0; k < ns; k++) {
+          orc_atom *b = atoms + i + st[k];
+          if (b->type < 0) continue;
+          const double dx = a->x[0] - b->x[0], dy = a->x[1] - b->x[1], dz = a->x[2] - b->x[2];
+          const double d2 = dx * dx + dy * dy + dz * dz;
+          if (d2 >= rc2) continue;
+          const double r = sqrt(d2);
+          a->rho += orc_rho_of_r(p, b->type, r);
+          b->rho += orc_rho_of_r(p, a->type, r);
+        }
+      }
+}
+
+void orc_force_pass_half(const orc_pot *p, const orc_domain *d, orc_atom *atoms, const int64_t *even, size_t n_even,
+                         const int64_t *odd, size_t n_odd, double cutoff) {
+  const double rc2 = cutoff * cutoff;
+  const int64_t n = (int64_t)d->ext_size_x * d->ext_size_y * d->ext_size_z;
+  for (int64_t i = 0; i < n; i++) atoms[i].f[0] = atoms[i].f[1] = atoms[i].f[2] = 0.0;
+  for (int64_t z = 0; z < d->box_size_z; z++)
+    for (int64_t y = 0; y < d->box_size_y; y++)
+      for (int64_t x = 0; x < d->box_size_x; x++) {
+        const int64_t i = site_linear(d, x, y, z);
+        orc_atom *a = atoms + i;
+        if (a->type < 0) continue;
+        const int ev = ((x + d->box_index_start_x) % 2) == 0;
+        const int64_t *st = ev ? even : odd;
+        const size_t ns = ev ? n_even : n_odd;
+        for (size_t k = 0; k < ns; k++) {
+          orc_atom *b = atoms + i + st[k];
+          if (b->type < 0) continue;
+          const double dx = a->x[0] - b->x[0], dy = a->x[1] - b->x[1], dz = a->x[2] - b->x[2];
+          const double d2 = dx * dx + dy * dy + dz * dz;
+          if (d2 >= rc2) continue;
+          const double fp = pair_fpair(p, a->type, b->type, sqrt(d2), a->df, b->df);
+          a->f[0] += dx * fp;
+          a->f[1] += dy * fp;
+          a->f[2] += dz * fp;
+          b->f[0] -= dx * fp;
+          b->f[1] -= dy * fp;
+          b->f[2] -= dz * fp;
+        }
+      }
+}
+
 /* ------------------------------------------------------------ ghost fill */
 
 static inline int64_t pmod(int64_t a, int64_t b) {

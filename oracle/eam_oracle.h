@@ -73,6 +73,14 @@ void orc_df_pass(const orc_pot *p, const orc_domain *d, orc_atom *atoms);
 void orc_force_pass(const orc_pot *p, const orc_domain *d, orc_atom *atoms, const int64_t *even, size_t n_even,
                     const int64_t *odd, size_t n_odd, double cutoff);
 
+/* Half-neighbour (Newton's third law) passes of the reference's USE_NEWTONS_THIRD_LOW
+ * build: each pair (i, i + o), i a box site and o from the half stencil, once; rho (f)
+ * of every ext record, box and ghost, is the sum of the shares it received. */
+void orc_rho_pass_half(const orc_pot *p, const orc_domain *d, orc_atom *atoms, const int64_t *even, size_t n_even,
+                       const int64_t *odd, size_t n_odd, double cutoff);
+void orc_force_pass_half(const orc_pot *p, const orc_domain *d, orc_atom *atoms, const int64_t *even, size_t n_even,
+                         const int64_t *odd, size_t n_odd, double cutoff);
+
 /* Single-rank periodic ghost fill.  mask bit 0: type+x, bit 1: df. */
 void orc_ghost_fill(const orc_domain *d, orc_atom *atoms, const double box_len[3], int mask);
 

@@ -79,6 +79,10 @@ def lib() -> C.CDLL:
             "orc_rho_pass": (None, [_P, C.POINTER(Domain), _P, _PI64, C.c_size_t, _PI64, C.c_size_t, C.c_double]),
             "orc_df_pass": (None, [_P, C.POINTER(Domain), _P]),
             "orc_force_pass": (None, [_P, C.POINTER(Domain), _P, _PI64, C.c_size_t, _PI64, C.c_size_t, C.c_double]),
+            "orc_rho_pass_half": (None, [_P, C.POINTER(Domain), _P, _PI64, C.c_size_t, _PI64, C.c_size_t,
+                                         C.c_double]),
+            "orc_force_pass_half": (None, [_P, C.POINTER(Domain), _P, _PI64, C.c_size_t, _PI64, C.c_size_t,
+                                           C.c_double]),
             "orc_ghost_fill": (None, [C.POINTER(Domain), _P, _PD, C.c_int]),
             "orc_compute_forces": (None, [_P, C.POINTER(Domain), _P, _P, C.c_int, _PI64, C.c_size_t, _PI64,
                                           C.c_size_t, C.POINTER(MdParams), C.POINTER(Energy)]),
@@ -180,6 +184,38 @@ def df_pass(pot: Pot, dom: Domain, ext: np.ndarray) -> None:
 
 def force_pass(pot: Pot, dom: Domain, ext: np.ndarray, even, odd, cutoff: float) -> None:
     lib().orc_force_pass(pot.h, C.byref(dom), _a(ext), _i(even), even.size, _i(odd), odd.size, cutoff)
+
+
+def half_stencil(st: np.ndarray) -> np.ndarray:
+    """One offset of each opposite pair: the offsets that are positive as linear
+    indices (lexicographically positive (dz, dy, dx)), in their original order."""
+    return np.ascontiguousarray(st[st > 0])
+
+
+def rho_pass_half(pot: Pot, dom: Domain, ext: np.ndarray, even, odd, cutoff: float) -> None:
+    """Newton's-third-law rho pass (orc_rho_pass_half): shares to box and ghost records."""
+    lib().orc_rho_pass_half(pot.h, C.byref(dom), _a(ext), _i(even), even.size, _i(odd), odd.size, cutoff)
+
+
+def force_pass_half(pot: Pot, dom: Domain, ext: np.ndarray, even, odd, cutoff: float) -> None:
+    """Newton's-third-law force pass (orc_force_pass_half)."""
+    lib().orc_force_pass_half(pot.h, C.byref(dom), _a(ext), _i(even), even.size, _i(odd), odd.size, cutoff)
+
+
+def fold_ghosts(dom: Domain, ext: np.ndarray, field: str) -> np.ndarray:
+    """Box-order copy of `field` with every ghost record's value added to the box site
+    it images under the periodic wrap: what the host's reverse ghost communication
+    does on a single periodic rank."""
+    ex, ey, ez = dom.ext_size_x, dom.ext_size_y, dom.ext_size_z
+    gx, gy, gz = dom.ghost_size_x, dom.ghost_size_y, dom.ghost_size_z
+    bx, by, bz = dom.box_size_x, dom.box_size_y, dom.box_size_z
+    a = ext[field].reshape((ez, ey, ex) + ext[field].shape[1:])
+    out = np.zeros((bz, by, bx) + ext[field].shape[1:])
+    zi = (np.arange(ez) - gz) % bz
+    yi = (np.arange(ey) - gy) % by
+    xi = (np.arange(ex) - gx) % bx
+    np.add.at(out, (zi[:, None, None], yi[None, :, None], xi[None, None, :]), a)
+    return out.reshape((bz * by * bx,) + ext[field].shape[1:])
 
 
 def ghost_fill(dom: Domain, ext: np.ndarray, box_len, mask: int) -> None:

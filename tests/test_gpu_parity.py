@@ -97,6 +97,68 @@ def test_hook_with_setfl_alloy_matches_oracle(hooks, tmp_path):
     assert rel_err(bg["f"][live], bo["f"][live]) < F_TOL
 
 
+@pytest.mark.parametrize("n_types,start", [(1, (0, 0, 0)), (3, (1, 0, 0))])
+def test_half_neighbour_hooks_match_oracle(hooks, n_types, start):
+    # the reference's USE_NEWTONS_THIRD_LOW build: half stencils, shares to box and ghost
+    # records; the host folds ghost shares into their owners between the passes
+    sc = make(cells=(6, 7, 5), temperature=900.0, vacancy=0.02, n_types=n_types, seed=27, jitter=0.1)
+    dom = mb.lattice.domain(sc.cells, sc.ghost, start)
+    odom = orc.make_domain(sc.cells, sc.ghost, start)
+    hooks.domain_init(dom)
+    even, odd = mb.lattice.stencil_linear(A0, sc.reach, dom.ext_size_x, dom.ext_size_y)
+    he, ho = orc.half_stencil(even), orc.half_stencil(odd)
+    hooks.pot_init(sc.tables)
+    hooks.set_half_neighbour(True)
+    try:
+        with pytest.raises(mb.MbError, match="half stencil"):
+            hooks.nei_offset_init(even, odd)  # a full stencil holds every pair twice
+        hooks.nei_offset_init(he, ho)
+        pot = sc.orc_pot()
+        L = [sc.cells[0] * A0, sc.cells[1] * A0, sc.cells[2] * A0]
+        ext_gpu = sc.ext()
+        ext_orc = ext_gpu.copy().view(orc.ATOM)
+        hooks.rho_calc(ext_gpu, sc.cutoff)
+        orc.rho_pass_half(pot, odom, ext_orc, he, ho, sc.cutoff)
+        # every ext record, ghosts included, against the oracle's shares
+        assert rel_err(ext_gpu["rho"], ext_orc["rho"]) < 1e-12
+        assert np.array_equal(ext_gpu["x"], ext_orc["x"])
+        # host: fold ghost shares into owners, df pass, refresh ghost df
+        for e in (ext_gpu, ext_orc.view(mb.ATOM_DTYPE)):
+            folded = orc.fold_ghosts(odom, e, "rho")
+            b = mb.lattice.ext_to_box(e, sc.cells, sc.ghost)
+            b["rho"] = folded
+            e[:] = mb.lattice.box_to_ext(b, sc.cells, sc.ghost, A0)
+        hooks.df_calc(ext_gpu, sc.cutoff)
+        orc.df_pass(pot, odom, ext_orc)
+        live = _box(ext_gpu, sc)["type"] >= 0
+        assert rel_err(_box(ext_gpu, sc)["df"][live], _box(ext_orc, sc)["df"][live]) < 1e-12
+        orc.ghost_fill(odom, ext_gpu.view(orc.ATOM), L, 2)
+        orc.ghost_fill(odom, ext_orc, L, 2)
+        hooks.force_calc(ext_gpu, sc.cutoff)
+        orc.force_pass_half(pot, odom, ext_orc, he, ho, sc.cutoff)
+        assert rel_err(ext_gpu["f"], ext_orc["f"]) < F_TOL
+        # after the fold the forces are the full-neighbour forces
+        full = sc.ext().view(orc.ATOM)
+        orc.rho_pass(pot, odom, full, even, odd, sc.cutoff)
+        orc.ghost_fill(odom, full, L, 2)
+        orc.force_pass(pot, odom, full, even, odd, sc.cutoff)
+        fg = orc.fold_ghosts(odom, ext_gpu, "f")
+        assert rel_err(fg[live], _box(full.view(mb.ATOM_DTYPE), sc)["f"][live]) < F_TOL
+        with pytest.raises(mb.MbError, match="full-neighbour"):
+            mb.check(mb.lib().mb_eam_rho_calc_noalloc(mb.ptr(ext_gpu), sc.cutoff))
+    finally:
+        hooks.set_half_neighbour(False)
+
+
+def test_hook_rejects_types_without_a_potential_table(hooks):
+    sc = make(cells=(6, 6, 6), seed=5)
+    _hook_setup(hooks, sc)
+    ext = sc.ext()
+    ext["type"][len(ext) // 2] = 2  # the one-type potential has a table for type 0 only
+    with pytest.raises(mb.MbError, match="potential table"):
+        hooks.rho_calc(ext, sc.cutoff)
+
+
 def test_hook_df_from_rho_matches_oracle(hooks):
     sc = make(cells=(6, 6, 6), temperature=600.0, vacancy=0.01, seed=4)
     dom, odom, even, odd = _hook_setup(hooks, sc)
@@ -252,3 +314,11 @@ def test_bad_inputs_are_rejected_on_device():
         bad["type"][3] = 99
         with pytest.raises(mb.MbError):
             sim.upload(bad)
+        # a type the potential has no table for (one-type potential: only type 0)
+        bad["type"][3] = 1
+        with pytest.raises(mb.MbError, match="potential table"):
+            sim.upload(bad)
+        itl = mb.lattice.octahedral_interstitials(1, sc.cells, A0, 2)
+        itl["type"] = 2
+        with pytest.raises(mb.MbError, match="potential table"):
+            sim.upload(sc.box, itl)
