@@ -397,12 +397,18 @@ def mixed_comparison(args, mb, wl, box, itl, n_atoms, fp64_rate, pg) -> dict:
 
 def run_nve(args, mb, world, rank, local, pg) -> None:
     """The mixed-precision NVE run of the 200^3-cell workload (16 M atoms, 900 K, 0.5%
-    vacancies, 763 interstitials): --nve-steps steps with the total energy recorded and
-    the relative force RMS error against the FP64 path checked every --check-every
-    steps.  At each check the mixed state (positions, velocities, mixed forces at those
-    positions) is read back and the FP64 path evaluates the forces at the same positions;
-    the FP64 path matches the CPU oracle to ~1e-15 (tests/test_gpu_parity.py).  Energy
-    drift is (E(t) - E(0)) / N in eV/atom."""
+    vacancies, 763 interstitials): --nve-equil + --nve-steps steps with the total energy
+    recorded and the relative force RMS error against the FP64 path checked every
+    --check-every steps.  At each check the mixed state (positions, velocities, mixed
+    forces at those positions) is read back and the FP64 path evaluates the forces at the
+    same positions; the FP64 path matches the CPU oracle to ~1e-15
+    (tests/test_gpu_parity.py).  Atoms that leave their lattice site move to the
+    interstitial list and back (mb_sim_set_conversion, on unless --no-conversion).
+    Energy drift is reported over the --nve-steps production steps after the
+    equilibration (E(t) - E(t_eq)) / N in eV/atom, plus the offset from step 0: a run
+    started from a perfect lattice moves about 1e-5 eV/atom within its first few hundred
+    steps while kinetic and potential energy equilibrate (the O(dt^2) velocity-Verlet
+    energy error, the same in the FP64 path)."""
     mb.check(mb.lib().mb_env_init(local))
     wl = dict(WORKLOADS["mixed"])
     if args.nve_itl is not None:  # interstitial count override (0: vacancies only)
@@ -413,12 +419,17 @@ def run_nve(args, mb, world, rank, local, pg) -> None:
     box, itl = build_state(mb, wl)
     n_atoms = int((box["type"] >= 0).sum()) + itl.shape[0]
     tables = mb.potential.fe_analytic()
-    kw = dict(lattice_const=A0, mass=MASS, dt=DT, cutoff=RC, stencil_skin=SKIN, max_interstitials=max(1, itl.shape[0]))
+    conversion = not args.no_conversion
+    cap = itl.shape[0] + (4096 if conversion else 0)
+    kw = dict(lattice_const=A0, mass=MASS, dt=DT, cutoff=RC, stencil_skin=SKIN, max_interstitials=max(1, cap))
     every = max(1, args.check_every)
+    total = args.nve_equil + args.nve_steps
     prec = mb.MB_PREC_FP64 if args.nve_precision == "fp64" else mb.MB_PREC_MIXED
     mixed = mb.Sim(wl["cells"], tables, precision=prec, **kw)
     ref = mb.Sim(wl["cells"], tables, precision=mb.MB_PREC_FP64, **kw)
     mixed.upload(box, itl)
+    if conversion:
+        mixed.set_conversion(SKIN, 0.5 * SKIN)
     del box, itl
     steps_done, rms, rms_steps, e_rec = 0, [], [], []
     t_md = 0.0
@@ -436,9 +447,9 @@ def run_nve(args, mb, world, rank, local, pg) -> None:
         rms.append(float(np.sqrt(np.sum((f32 - f64) ** 2) / np.sum(f64 ** 2))))
         rms_steps.append(steps_done)
         del b, i, rb, ri, f32, f64, live
-        if steps_done >= args.nve_steps:
+        if steps_done >= total:
             break
-        n = min(every, args.nve_steps - steps_done)
+        n = min(every, total - steps_done)
         t0 = time.perf_counter()
         mixed.run(n, energy_every=every)
         t_md += time.perf_counter() - t0
@@ -446,10 +457,16 @@ def run_nve(args, mb, world, rank, local, pg) -> None:
         e_rec.append(mixed.energies())
     clk = clocks.stop()
     e = np.concatenate([x for x in e_rec if x.size], axis=0)
+    conv = mixed.conversion_stats() if conversion else None
     mixed.close()
     ref.close()
-    e0 = float(e[0, 1] + e[0, 2])
-    drift = (e[:, 1] + e[:, 2] - e0) / n_atoms
+    etot = e[:, 1] + e[:, 2]
+    e0 = float(etot[0])
+    drift = (etot - e0) / n_atoms
+    prod = e[:, 0] >= args.nve_equil
+    eq = float(etot[prod][0]) if prod.any() else e0
+    drift_prod = (etot[prod] - eq) / n_atoms if prod.any() else np.zeros(1)
+    slope = float(np.polyfit(e[prod, 0], etot[prod] / n_atoms, 1)[0]) if prod.sum() > 2 else 0.0
     if rank == 0:
         print(json.dumps({
             "metric": "atom-steps/s", "value": n_atoms * steps_done * world / t_md, "unit": "atom-steps/s",
@@ -461,8 +478,13 @@ def run_nve(args, mb, world, rank, local, pg) -> None:
                        "check_every": every, "timing": "wall clock of the MD segments (energy steps included)"},
             "force_rms_rel_err_vs_fp64": {"max": max(rms), "mean": float(np.mean(rms)), "final": rms[-1],
                                           "steps": rms_steps, "values": rms},
-            "energy_drift_ev_per_atom": {"max_abs": float(np.max(np.abs(drift))), "final": float(drift[-1]),
-                                         "steps": e[:, 0].astype(int).tolist(), "values": drift.tolist()},
+            "energy_drift_ev_per_atom": {
+                "production_steps": args.nve_steps, "equilibration_steps": args.nve_equil,
+                "production_max_abs": float(np.max(np.abs(drift_prod))), "production_final": float(drift_prod[-1]),
+                "production_fit_slope_x_steps": slope * args.nve_steps,
+                "offset_from_step0_max_abs": float(np.max(np.abs(drift))), "final_from_step0": float(drift[-1]),
+                "steps": e[:, 0].astype(int).tolist(), "values_from_step0": drift.tolist()},
+            "conversion": conv,
             "bars": {"force_rms": 1e-6, "drift": 1e-5}, "clocks": clk, "cpu_baseline": None, "e2e": None,
             "gpu_launches": None}), flush=True)
 
@@ -565,6 +587,8 @@ def main() -> None:
     ap.add_argument("--check-every", type=int, default=100, help="force / energy check interval of --config nve")
     ap.add_argument("--nve-precision", choices=["mixed", "fp64"], default="mixed", help="path run by --config nve")
     ap.add_argument("--nve-itl", type=int, default=None, help="interstitials of --config nve (default 763)")
+    ap.add_argument("--nve-equil", type=int, default=1000, help="equilibration steps before the drift window")
+    ap.add_argument("--no-conversion", action="store_true", help="--config nve without lattice <-> interstitial moves")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, pg = dist_setup()

@@ -210,6 +210,19 @@ int mb_sim_kernel_times(mb_sim *sim, float *rho_ms, float *force_ms);
 int mb_sim_info(mb_sim *sim, int64_t *n_sites, int64_t *n_stencil, int64_t *device_bytes);
 /* CUDA graph capture of the steady-state step (on by default). */
 int mb_sim_set_graphs(mb_sim *sim, int enable);
+/* Lattice <-> interstitial bookkeeping of the device-resident run.  MISA-MD keeps atoms
+ * that have left their lattice site in its interstitial list (the plugin only sees
+ * type < 0 for such sites, src/kernels/kernel_itl.hpp:44).  With convert_distance > 0,
+ * after every step an atom farther than convert_distance (A) from its lattice site
+ * joins the end of the interstitial list (sites in box order) and its site becomes
+ * vacant; then an interstitial (list order) within recombine_distance of a vacant site
+ * takes that site and leaves the list.  0 switches it off (the default).  Needs
+ * 0 < max_interstitials <= 65536; a conversion beyond the capacity is refused (the atom
+ * stays on its site) and counted. */
+int mb_sim_set_conversion(mb_sim *sim, double convert_distance, double recombine_distance);
+/* counters[4]: conversions, recombinations, conversions refused (list full), candidates
+ * dropped (more than 2048 in one step); *n_itl: the current interstitial count. */
+int mb_sim_conversion_stats(mb_sim *sim, int64_t *counters, int32_t *n_itl);
 
 /* ------------------------------------------- 3. ensembles and serving */
 
@@ -271,6 +284,10 @@ int mb_ensemble_set_graphs(mb_ensemble *e, int enable);
  * kernel otherwise; 1 always the persistent kernel; 2 always split (MB_ERR_UNSUPPORTED
  * at the next launch if it cannot apply). */
 int mb_ensemble_set_mode(mb_ensemble *e, int32_t mode);
+/* mb_sim_set_conversion for every lattice of the ensemble (each within its own
+ * max_interstitials). */
+int mb_ensemble_set_conversion(mb_ensemble *e, double convert_distance, double recombine_distance);
+int mb_ensemble_conversion_stats(mb_ensemble *e, int32_t slot, int64_t *counters, int32_t *n_itl);
 /* Device time of one step's kernels, averaged over 4 extra steps every lattice takes
  * (CUDA events on the ensemble's stream): split kernels report the density pass in
  * *rho_ms and the force + integration pass in *force_ms; the persistent kernel

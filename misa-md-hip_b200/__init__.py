@@ -160,6 +160,19 @@ class Sim:
     def set_graphs(self, enable: bool) -> None:
         check(lib().mb_sim_set_graphs(self._h, int(enable)))
 
+    def set_conversion(self, convert_distance: float, recombine_distance: float) -> None:
+        """Atoms farther than convert_distance from their site join the interstitial
+        list after each step; interstitials within recombine_distance of a vacant site
+        take it (mb_sim_set_conversion).  convert_distance 0 switches it off."""
+        check(lib().mb_sim_set_conversion(self._h, convert_distance, recombine_distance))
+
+    def conversion_stats(self) -> dict:
+        c = np.zeros(4, dtype=np.int64)
+        n = C.c_int32(0)
+        check(lib().mb_sim_conversion_stats(self._h, _abi.i64ptr(c), C.byref(n)))
+        return {"converted": int(c[0]), "recombined": int(c[1]), "refused": int(c[2]), "dropped": int(c[3]),
+                "n_itl": n.value}
+
 
 class Ensemble:
     """Many independent periodic lattices advanced together in mixed precision: one
@@ -233,6 +246,17 @@ class Ensemble:
 
     def sync(self) -> None:
         check(lib().mb_ensemble_sync(self._h))
+
+    def set_conversion(self, convert_distance: float, recombine_distance: float) -> None:
+        """mb_sim_set_conversion for every lattice (mb_ensemble_set_conversion)."""
+        check(lib().mb_ensemble_set_conversion(self._h, convert_distance, recombine_distance))
+
+    def conversion_stats(self, slot: int) -> dict:
+        c = np.zeros(4, dtype=np.int64)
+        n = C.c_int32(0)
+        check(lib().mb_ensemble_conversion_stats(self._h, slot, _abi.i64ptr(c), C.byref(n)))
+        return {"converted": int(c[0]), "recombined": int(c[1]), "refused": int(c[2]), "dropped": int(c[3]),
+                "n_itl": n.value}
 
     def download(self, slot: int) -> tuple[np.ndarray, np.ndarray]:
         cells, cap = self._cells[slot]

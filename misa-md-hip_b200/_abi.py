@@ -107,6 +107,10 @@ SIGNATURES: dict[str, tuple] = {
     "mb_sim_kernel_times": (_I, [_P, _PF, _PF]),
     "mb_sim_info": (_I, [_P, _PI64, _PI64, _PI64]),
     "mb_sim_set_graphs": (_I, [_P, _I]),
+    "mb_sim_set_conversion": (_I, [_P, _D, _D]),
+    "mb_sim_conversion_stats": (_I, [_P, _PI64, C.POINTER(C.c_int32)]),
+    "mb_ensemble_set_conversion": (_I, [_P, _D, _D]),
+    "mb_ensemble_conversion_stats": (_I, [_P, C.c_int32, _PI64, C.POINTER(C.c_int32)]),
     "mb_ensemble_create": (_I, [C.c_void_p, C.POINTER(MbEamTables), C.POINTER(_P)]),
     "mb_ensemble_destroy": (_I, [_P]),
     "mb_ensemble_lattice_bytes": (_I, [C.c_void_p, _PI64]),

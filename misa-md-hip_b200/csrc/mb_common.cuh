@@ -127,12 +127,15 @@ struct Lattice64 {
 };
 
 struct Itl64 {
-  int n;
+  int n;                   // count, when nd is null (lists fixed by the host)
+  const int *nd;           // device-resident count (lists that change on the device), or null
+  int cap;                 // capacity of the list
   int cap_flag;
   double *px, *py, *pz;    // current positions
   double *nx, *ny, *nz;    // next positions
   double *vx, *vy, *vz, *fx, *fy, *fz, *rho, *df;
   int8_t *type;
+  int64_t *id;
   int *flag_list;          // flagged box sites (ext index)
   int *flag_count;         // [0] this step, [1] overflow marker
   double a0, reach;        // window radius in A (cutoff + skin)
@@ -145,7 +148,23 @@ struct StepParams {
   double mass;
   int kick_pre;  // 1: v += h f before the energy sample (closes the previous step)
   int drift;     // 1: v += h f ; x_next = x + dt v
+  // lattice -> interstitial conversion (conv2 > 0): sites whose drifted atom lies
+  // farther than sqrt(conv2) from the ideal site are listed in cand (box index)
+  double a0, conv2;
+  long long *cand;
+  int *cand_n;
 };
+#define MB_CAND_CAP 2048     // conversion candidates handled per step
+#define MB_CONV_ITL_MAX 65536 // interstitial capacity with conversion on
+
+// Ideal position of box site (s, cx, y, z): x doubled = 2 cx + s.
+__host__ __device__ __forceinline__ void site_ideal(int s, int cx, int y, int z, double a0, double &X, double &Y,
+                                                    double &Z) {
+  const double h = 0.5 * s;
+  X = 0.5 * a0 * (double)(2 * cx + s);
+  Y = a0 * ((double)y + h);
+  Z = a0 * ((double)z + h);
+}
 
 // kernels (mb_kernels64.cu)
 int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, double rc2,
@@ -158,6 +177,12 @@ int launch_itl_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, con
 int launch_itl_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const Itl64 &I,
                        const StepParams &sp, double *e_partial, int energy, cudaStream_t s);
 int launch_images64(const Geom &g, const Lattice64 &L, int what, cudaStream_t s); // what: 1 pos+code, 2 df
+// Lattice <-> interstitial bookkeeping after a drift (one CTA): candidates of
+// sp.cand become interstitials (box order), then interstitials within sqrt(rec2) of a
+// vacant site take it (list order, first claim wins).  counters: [0] conversions,
+// [1] recombinations, [2] refused conversions (list full), [3] dropped candidates.
+int launch_convert64(const Geom &g, const Lattice64 &L, const Itl64 &I, const StepParams &sp, double rec2,
+                     int64_t *site_id, int *nd, long long *counters, cudaStream_t s);
 int launch_kick_drift64(const Geom &g, const Lattice64 &L, const Itl64 &I, const StepParams &sp, cudaStream_t s);
 int launch_reduce(const double *partials, int n, double *out, cudaStream_t s);
 int energy_partials_needed();

@@ -194,4 +194,39 @@ __device__ __forceinline__ bool window_site_rel(const Geom &g, const Window &w, 
 
 __device__ __forceinline__ double min_image(double d, double L, double iL) { return d - L * rint(d * iL); }
 
+// ------------------------------------------------- conversion helpers
+// In-place ascending bitonic sort of n2 (a power of two) keys by the whole block.
+__device__ __forceinline__ void bitonic_sort(long long *key, int n2) {
+  for (int k = 2; k <= n2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = threadIdx.x; t < n2; t += blockDim.x) {
+        const int p = t ^ j;
+        if (p > t) {
+          const bool up = (t & k) == 0;
+          const long long a = key[t], b = key[p];
+          if ((a > b) == up) {
+            key[t] = b;
+            key[p] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void decode_box(const Geom &g, long long t, int &s, int &cx, int &y, int &z) {
+  const long long bx = 2LL * g.bcx;
+  const int xd = (int)(t % bx);
+  const long long r = t / bx;
+  y = (int)(r % g.by);
+  z = (int)(r / g.by);
+  s = xd & 1;
+  cx = xd >> 1;
+}
+
+__device__ __forceinline__ int pmod_int(long long a, int b) {
+  long long r = a % b;
+  return (int)(r < 0 ? r + b : r);
+}
+
 } // namespace mb

@@ -187,6 +187,7 @@ struct mb_ensemble {
   bool graphs_ok = true;
   int policy = -1; // -1: size model per lattice; 0..3: one shape for all
   int mode = 0;  // 0: split kernels when the built-in shells apply, else persistent; 1: persistent; 2: split
+  double conv_d = 0.0, rec_d = 0.0; // lattice <-> interstitial conversion (off while conv_d == 0)
   int split = 0; // kernels in use: 0 persistent, 1 split with the brick walk, 2 split with the linear walk
   unsigned *d_item_first = nullptr; // linear walk: first item of each lattice
   double *d_epart_items = nullptr;  // split: energy partials per walk item
@@ -313,7 +314,7 @@ static size_t lattice_bytes(int cx, int cy, int cz, int cap_itl) {
   const int per = 2 * 4 * 64 + 64; // flagged sites per interstitial (upper bound of the window sphere)
   const size_t ci = (size_t)std::max(1, cap_itl);
   return 2 * a(n * 16) + 6 * a(n * 8) + 4 * a(n * 4) + a(n) + a(nb * 8) + a(ci * 8) * 16 + a(ci) +
-         a((size_t)std::max(1, cap_itl * per) * 4) + a(16) + a(ci * 8);
+         a((size_t)std::max(1, cap_itl * per) * 4) + a(16) + a(ci * 8) + a(MB_CAND_CAP * 8) + a(16) + a(32);
 }
 
 static int sync_desc(mb_ensemble *e) {
@@ -330,6 +331,7 @@ static int sync_desc(mb_ensemble *e) {
     d.cur = tmp[c].cur;
     d.primed = tmp[c].primed;
     d.steps_done = tmp[c].steps_done;
+    d.n_itl = tmp[c].n_itl; // conversions change it on the device
   }
   e->synced_desc = true;
   return MB_OK;
@@ -378,7 +380,7 @@ static int rebuild(mb_ensemble *e) {
                              ((unsigned)(tz * kShapes[shape][2]) << 22));
         }
     (void)nt;
-    if (L.d.n_itl > 0) itl_lats.push_back(c);
+    if (L.d.n_itl > 0 || (e->conv_d > 0.0 && L.d.cap_itl > 0)) itl_lats.push_back(c);
     descs[c] = L.d;
   }
   tile_first[nl] = (int)tile_lat.size();
@@ -634,6 +636,8 @@ static int check_err(mb_ensemble *e) {
 static int launch_step(mb_ensemble *e, int energy) {
   if (e->dirty) MB_TRY(rebuild(e));
   if (e->n_tiles == 0) return MB_OK;
+  if (e->conv_d > 0.0 && !e->split)
+    return fail(MB_ERR_UNSUPPORTED, "lattice <-> interstitial conversion runs with the split kernels only");
   e->synced_desc = false;
   EnsParams &P = e->P;
   if (energy) {
@@ -731,13 +735,17 @@ static int advance(mb_ensemble *e, long long max_launches, int energy_every, lon
     }
     n++;
   }
-  e->synced_desc = true; // the mirror now matches what the device will hold
+  // the mirror now matches what the device will hold, except the interstitial counts,
+  // which conversions change on the device: then the next sync pulls them
+  e->synced_desc = !(e->conv_d > 0.0);
   if (done) *done = n;
   return MB_OK;
 }
 
 static int push_targets(mb_ensemble *e) {
-  // descriptors are small: re-upload after host-side changes of targets
+  // descriptors are small: re-upload after host-side changes of targets, with the
+  // device-owned fields (parity, counters, interstitial counts) pulled back first
+  MB_TRY(sync_desc(e));
   std::vector<LatDesc> descs;
   for (int s : e->order) descs.push_back(e->slots[s].d);
   if (!descs.empty())
@@ -935,6 +943,12 @@ int mb_ensemble_add(mb_ensemble *e, const mb_lattice_spec *spec, const mb_atom_e
   d.itype = (int8_t *)take(ci);
   d.flag_list = (int *)take((size_t)d.cap_flag * 4);
   d.flag_count = (int *)take(16); // [count parity 0, count parity 1, overflow, -]
+  d.cand = (long long *)take(MB_CAND_CAP * 8);
+  d.cand_n = (int *)take(16);
+  d.conv_counters = (long long *)take(32);
+  d.cap_itl = L.cap_itl;
+  d.ids = L.ids;
+  d.iids = L.iids;
   if ((size_t)(p - (char *)block) > bytes) return fail(MB_ERR_STATE, "lattice layout overflows its block");
   cudaStream_t s = e->stream;
   auto undo = [&](int code) {
@@ -967,6 +981,8 @@ int mb_ensemble_add(mb_ensemble *e, const mb_lattice_spec *spec, const mb_atom_e
     put(d.ivy, 1, 1);
     put(d.ivz, 2, 1);
     cudaMemcpyAsync(d.itype, t.data(), n_itl, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(L.iids, L.host_iids.data(), sizeof(int64_t) * n_itl, cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
   }
   int bad = 0;
   cudaMemcpyAsync(&bad, e->d_bad, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -1078,10 +1094,14 @@ int mb_ensemble_download(mb_ensemble *e, int32_t slot, mb_atom_element *box, mb_
     }
     MB_CUDA(cudaMemcpy(rho.data(), d.irho, sizeof(double) * n, cudaMemcpyDeviceToHost));
     MB_CUDA(cudaMemcpy(df.data(), d.idf, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    std::vector<int64_t> ids(n);
+    std::vector<int8_t> types(n);
+    MB_CUDA(cudaMemcpy(ids.data(), d.iids, sizeof(int64_t) * n, cudaMemcpyDeviceToHost));
+    MB_CUDA(cudaMemcpy(types.data(), d.itype, n, cudaMemcpyDeviceToHost));
     for (int q = 0; q < n; q++) {
       mb_atom_element &a = itl[q];
-      a.id = L.host_iids.empty() ? q : L.host_iids[q];
-      a.type = 0;
+      a.id = ids[q];
+      a.type = types[q];
       a.pad_ = 0;
       for (int k = 0; k < 3; k++) {
         a.x[k] = x[k][q];
@@ -1208,7 +1228,9 @@ int mb_ensemble_kernel_times(mb_ensemble *e, float *rho_ms, float *force_ms, int
   MB_TRY(check_err(e));
   if (rho_ms) *rho_ms = tr / reps;
   if (force_ms) *force_ms = tf / reps;
-  if (kernels_per_step) *kernels_per_step = e->split ? (3 + (e->P.n_itl_lats > 0 ? 4 : 0)) : 1;
+  if (kernels_per_step)
+    *kernels_per_step =
+        e->split ? (3 + (e->P.n_itl_lats > 0 ? 4 + (e->P.conv2 > 0.0 ? 1 : 0) : 0)) : 1;
   return MB_OK;
 }
 
@@ -1278,6 +1300,7 @@ int mb_ensemble_autotune(mb_ensemble *e, int32_t steps, int32_t *policy, float *
         L.d.primed = sd.primed;
         L.d.steps_done = sd.steps_done;
         L.d.steps_target = sd.steps_target;
+        L.d.n_itl = sd.n_itl; // the block copy restored the list itself
         L.e_step.clear();
         L.e_pe.clear();
         L.e_ke.clear();
@@ -1341,6 +1364,38 @@ int mb_ensemble_set_graphs(mb_ensemble *e, int enable) {
   std::lock_guard<std::mutex> lk(e->mu);
   e->graphs_ok = enable != 0;
   drop_graph(e);
+  return MB_OK;
+}
+
+int mb_ensemble_set_conversion(mb_ensemble *e, double convert_distance, double recombine_distance) {
+  if (!e) return fail(MB_ERR_ARG, "null ensemble");
+  if (convert_distance < 0 || recombine_distance < 0 || (convert_distance > 0 && recombine_distance >= convert_distance))
+    return fail(MB_ERR_ARG, "need 0 <= recombine_distance < convert_distance (0 switches conversion off)");
+  std::lock_guard<std::mutex> lk(e->mu);
+  for (auto &L : e->slots)
+    if (L.used && convert_distance > 0 && L.cap_itl > MB_CONV_ITL_MAX)
+      return fail(MB_ERR_ARG, "max_interstitials above the conversion limit (65536)");
+  MB_TRY(sync_desc(e));
+  e->conv_d = convert_distance;
+  e->rec_d = convert_distance > 0 ? recombine_distance : 0.0;
+  e->P.conv2 = e->conv_d * e->conv_d;
+  e->P.rec2 = e->rec_d * e->rec_d;
+  e->dirty = true; // the interstitial lattice list and the captured step change
+  return MB_OK;
+}
+
+int mb_ensemble_conversion_stats(mb_ensemble *e, int32_t slot, int64_t *counters, int32_t *n_itl) {
+  if (!e) return fail(MB_ERR_ARG, "null ensemble");
+  std::lock_guard<std::mutex> lk(e->mu);
+  if (slot < 0 || slot >= (int)e->slots.size() || !e->slots[slot].used) return fail(MB_ERR_ARG, "no such slot");
+  MB_CUDA(cudaStreamSynchronize(e->stream));
+  MB_TRY(sync_desc(e));
+  const LatHost &L = e->slots[slot];
+  long long c[4] = {0, 0, 0, 0};
+  MB_CUDA(cudaMemcpy(c, L.d.conv_counters, sizeof(c), cudaMemcpyDeviceToHost));
+  if (counters)
+    for (int k = 0; k < 4; k++) counters[k] = (int64_t)c[k];
+  if (n_itl) *n_itl = L.d.n_itl;
   return MB_OK;
 }
 

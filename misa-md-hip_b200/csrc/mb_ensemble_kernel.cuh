@@ -62,6 +62,12 @@ struct LatDesc {
   double *ivx, *ivy, *ivz, *ifx, *ify, *ifz, *irho, *idf;
   int8_t *itype;
   double *e_itl; // [2] interstitial-item energy (pe, ke), accumulated atomically
+  // lattice <-> interstitial conversion
+  int cap_itl;
+  int64_t *ids, *iids;   // atom ids of the box sites (box order) and of the interstitials
+  long long *cand;       // [MB_CAND_CAP] box index of sites whose atom left them this step
+  int *cand_n;
+  long long *conv_counters; // [4] conversions, recombinations, refused, dropped
 };
 
 struct EnsParams {
@@ -89,6 +95,7 @@ struct EnsParams {
   const int *itl_lats;
   int n_itl_lats;
   int energy;
+  double conv2, rec2; // conversion / recombination distances squared (conv2 = 0: off)
 };
 
 // Split mode stencil.  BCC is a Bravais lattice: both sublattices see the same ideal
@@ -262,6 +269,16 @@ __device__ __forceinline__ Geom lat_geom(const LatDesc &d) {
 }
 
 __device__ __forceinline__ bool lat_active(const LatDesc &d) { return !d.primed || d.steps_done < d.steps_target; }
+
+// Lists box site (s, cx, y, z) of lattice d when its drifted atom (displacement u from
+// the ideal site) lies farther than sqrt(conv2) from it (conversion on).
+__device__ __forceinline__ void ens_conv_check(const EnsParams &P, const LatDesc &d, int s, int cx, int y, int z,
+                                               double ux, double uy, double uz) {
+  if (!(P.conv2 > 0.0) || !d.cand) return;
+  if (ux * ux + uy * uy + uz * uz <= P.conv2) return;
+  const int slot = atomicAdd(d.cand_n, 1);
+  if (slot < MB_CAND_CAP) d.cand[slot] = ((long long)z * d.by + y) * (2LL * d.bcx) + 2LL * cx + s;
+}
 
 __device__ __forceinline__ void ideal_pos(int s, int cx, int y, int z, double a0, double &X, double &Y, double &Z) {
   const double h = 0.5 * s;

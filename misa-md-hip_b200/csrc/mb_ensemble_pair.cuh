@@ -299,6 +299,7 @@ __device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag)
     const float4 nu = make_float4((float)nx, (float)ny, (float)nz, 0.f);
     float4 *un = d.u4[cur ^ 1];
     un[i] = nu;
+    ens_conv_check(P, d, s, cx, y, z, nx, ny, nz);
     for_images(g, s, cx, y, z, [&](long long idx, double, double, double) { un[idx] = nu; });
   } else {
     d.ivx[it] = vx;

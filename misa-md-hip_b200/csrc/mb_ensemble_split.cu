@@ -10,6 +10,8 @@
 // The kernels of one step (interstitial phases included) are captured into one CUDA
 // graph by the ensemble host.  One large lattice is walked by bricks, many lattices by
 // linear items (MxWalk).
+#include <limits.h>
+
 #include "mb_ensemble_kernel.cuh"
 #include "mb_ensemble_pair.cuh"
 #include "mb_ensemble_shells.cuh"
@@ -374,6 +376,7 @@ __device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStenci
   un[i] = nu;
   int sx, cx, y, z;
   mx_unpack(pos, sx, cx, y, z);
+  ens_conv_check(P, d, sx, cx, y, z, nx, ny, nz);
   const Geom g = lat_geom(d);
   for_images(g, sx, cx, y, z, [&](long long idx, double, double, double) { un[idx] = nu; });
 }
@@ -464,6 +467,199 @@ __global__ void k_mx_itl_mark(const __grid_constant__ EnsParams P) {
 template <bool FORCE, bool ENERGY>
 __global__ void k_mx_itl_items(const __grid_constant__ EnsParams P) {
   itl_items<FORCE, ENERGY>(P);
+}
+
+// Lattice <-> interstitial bookkeeping after the drift, one CTA per lattice that can
+// hold interstitials (the FP64 path's k_convert64 does the same; see there): this
+// step's candidates (box order) join the interstitial list and their sites become
+// vacant in both float4 buffers; then interstitials within the recombination distance
+// of a vacant site take it (lowest list index first) and the list is compacted in order.
+#define MX_CONV_THREADS 1024
+__global__ void __launch_bounds__(MX_CONV_THREADS, 1) k_mx_convert(const __grid_constant__ EnsParams P) {
+  __shared__ long long key[MB_CAND_CAP];
+  __shared__ unsigned removed[MB_CONV_ITL_MAX / 32];
+  __shared__ int s_scan[MX_CONV_THREADS / 32];
+  __shared__ int s_nclaim, s_base;
+  LatDesc &d = const_cast<LatDesc &>(P.lats[P.itl_lats[blockIdx.x]]);
+  if (!lat_active(d) || !d.cand) return; // uniform per block
+  const int tid = threadIdx.x;
+  const Geom g = lat_geom(d);
+  const int c0 = d.cur, c1 = c0 ^ 1; // this step's buffer and the drifted one
+  const int n0 = d.n_itl;
+  const int nraw = *d.cand_n;
+  const int nc = min(nraw, MB_CAND_CAP);
+  int n2 = 1;
+  while (n2 < nc) n2 <<= 1;
+  for (int k = tid; k < n2; k += blockDim.x) key[k] = k < nc ? d.cand[k] : LLONG_MAX;
+  __syncthreads();
+  if (nc > 1) bitonic_sort(key, n2);
+  const int nconv = min(nc, max(0, d.cap_itl - n0));
+  const float4 vac = make_float4(ENS_VACANT, ENS_VACANT, ENS_VACANT, 0.f);
+  for (int r = tid; r < nconv; r += blockDim.x) {
+    const long long t = key[r];
+    int s, cx, y, z;
+    decode_box(g, t, s, cx, y, z);
+    const long long i = ext_index(g, s, cx, y, z);
+    const int k = n0 + r;
+    double X, Y, Z;
+    ideal_pos(s, cx, y, z, P.a0, X, Y, Z);
+    const double ux = d.ux[i], uy = d.uy[i], uz = d.uz[i], vx = d.vx[i], vy = d.vy[i], vz = d.vz[i];
+    d.ipx[c1][k] = X + ux;
+    d.ipy[c1][k] = Y + uy;
+    d.ipz[c1][k] = Z + uz;
+    d.ipx[c0][k] = X + (ux - P.dt * vx); // the step's start (what a download reports)
+    d.ipy[c0][k] = Y + (uy - P.dt * vy);
+    d.ipz[c0][k] = Z + (uz - P.dt * vz);
+    d.ivx[k] = vx;
+    d.ivy[k] = vy;
+    d.ivz[k] = vz;
+    d.ifx[k] = (double)d.fx[i];
+    d.ify[k] = (double)d.fy[i];
+    d.ifz[k] = (double)d.fz[i];
+    d.irho[k] = (double)d.rho[i];
+    d.idf[k] = (double)d.u4[c0][i].w;
+    d.itype[k] = (int8_t)(d.code[i] & 0x3F);
+    d.iids[k] = d.ids[t];
+    // vacant: far away in both float4 buffers (the pair loops reject vacancies by position)
+    d.code[i] = -1;
+    d.u4[c0][i] = vac;
+    d.u4[c1][i] = vac;
+    d.ux[i] = d.uy[i] = d.uz[i] = 0.0;
+    d.vx[i] = d.vy[i] = d.vz[i] = 0.0;
+    d.fx[i] = d.fy[i] = d.fz[i] = 0.f;
+    for_images(g, s, cx, y, z, [&](long long idx, double, double, double) {
+      d.code[idx] = -1;
+      d.u4[c0][idx] = vac;
+      d.u4[c1][idx] = vac;
+    });
+  }
+  const int n1 = n0 + nconv;
+  if (tid == 0) {
+    d.conv_counters[0] += nconv;
+    d.conv_counters[2] += nc - nconv;
+    d.conv_counters[3] += nraw - nc;
+    *d.cand_n = 0;
+    s_nclaim = 0;
+  }
+  for (int w = tid; w < MB_CONV_ITL_MAX / 32; w += blockDim.x) removed[w] = 0u;
+  __syncthreads();
+  for (int k = tid; k < n1; k += blockDim.x) {
+    const double qx = d.ipx[c1][k], qy = d.ipy[c1][k], qz = d.ipz[c1][k];
+    double best = 1e300;
+    long long gx = 0, gy = 0, gz = 0;
+    int bs = 0;
+    for (int sl = 0; sl < 2; sl++) {
+      const double o = 0.5 * P.a0 * sl;
+      const long long ax = llrint((qx - o) / P.a0), ay = llrint((qy - o) / P.a0), az = llrint((qz - o) / P.a0);
+      const double X = 0.5 * P.a0 * (double)(2 * ax + sl), Y = P.a0 * ((double)ay + 0.5 * sl),
+                   Z = P.a0 * ((double)az + 0.5 * sl);
+      const double dd = (qx - X) * (qx - X) + (qy - Y) * (qy - Y) + (qz - Z) * (qz - Z);
+      if (dd < best) {
+        best = dd;
+        gx = ax;
+        gy = ay;
+        gz = az;
+        bs = sl;
+      }
+    }
+    if (!(best < P.rec2)) continue;
+    const int cx = pmod_int(gx, d.bcx), y = pmod_int(gy, d.by), z = pmod_int(gz, d.bz);
+    if (d.code[ext_index(g, bs, cx, y, z)] >= 0) continue;
+    const long long t = ((long long)z * d.by + y) * (2LL * d.bcx) + 2LL * cx + bs;
+    const int slot = atomicAdd(&s_nclaim, 1);
+    if (slot < MB_CAND_CAP) key[slot] = (t << 17) | (long long)k;
+  }
+  __syncthreads();
+  const int ncl = min(s_nclaim, MB_CAND_CAP);
+  n2 = 1;
+  while (n2 < ncl) n2 <<= 1;
+  for (int k = ncl + tid; k < n2; k += blockDim.x) key[k] = LLONG_MAX;
+  __syncthreads();
+  if (ncl > 1) bitonic_sort(key, n2);
+  int nrec = 0;
+  for (int r = tid; r < ncl; r += blockDim.x) {
+    const long long t = key[r] >> 17;
+    if (r > 0 && (key[r - 1] >> 17) == t) continue; // a lower list index took the site
+    const int k = (int)(key[r] & 0x1FFFF);
+    int s, cx, y, z;
+    decode_box(g, t, s, cx, y, z);
+    const long long i = ext_index(g, s, cx, y, z);
+    double X, Y, Z;
+    ideal_pos(s, cx, y, z, P.a0, X, Y, Z);
+    const double ux = min_image(d.ipx[c1][k] - X, g.Lx, g.iLx), uy = min_image(d.ipy[c1][k] - Y, g.Ly, g.iLy),
+                 uz = min_image(d.ipz[c1][k] - Z, g.Lz, g.iLz);
+    const double pux = ux + (d.ipx[c0][k] - d.ipx[c1][k]), puy = uy + (d.ipy[c0][k] - d.ipy[c1][k]),
+                 puz = uz + (d.ipz[c0][k] - d.ipz[c1][k]);
+    const int8_t ty = d.itype[k];
+    const float4 nu = make_float4((float)ux, (float)uy, (float)uz, 0.f);
+    const float4 pu = make_float4((float)pux, (float)puy, (float)puz, (float)d.idf[k]);
+    d.code[i] = ty;
+    d.ux[i] = ux;
+    d.uy[i] = uy;
+    d.uz[i] = uz;
+    d.vx[i] = d.ivx[k];
+    d.vy[i] = d.ivy[k];
+    d.vz[i] = d.ivz[k];
+    d.fx[i] = (float)d.ifx[k];
+    d.fy[i] = (float)d.ify[k];
+    d.fz[i] = (float)d.ifz[k];
+    d.rho[i] = (float)d.irho[k];
+    d.u4[c1][i] = nu;
+    d.u4[c0][i] = pu;
+    d.ids[t] = d.iids[k];
+    for_images(g, s, cx, y, z, [&](long long idx, double, double, double) {
+      d.code[idx] = ty;
+      d.u4[c1][idx] = nu;
+      d.u4[c0][idx] = pu;
+    });
+    atomicOr(&removed[k >> 5], 1u << (k & 31));
+    nrec++;
+  }
+  const double nrec_all = block_sum((double)nrec);
+  if (tid == 0) {
+    d.conv_counters[1] += (long long)nrec_all;
+    s_base = 0;
+  }
+  __syncthreads();
+  for (int q0 = 0; q0 < n1; q0 += blockDim.x) {
+    const int k = q0 + tid;
+    const bool keep = k < n1 && !((removed[k >> 5] >> (k & 31)) & 1u);
+    const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+    const int lane = tid & 31, wid = tid >> 5;
+    if (lane == 0) s_scan[wid] = __popc(ballot);
+    __syncthreads();
+    if (tid == 0) {
+      int acc = s_base;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+        const int c = s_scan[w];
+        s_scan[w] = acc;
+        acc += c;
+      }
+      s_base = acc;
+    }
+    __syncthreads();
+    const int dst = s_scan[wid] + __popc(ballot & ((1u << lane) - 1u));
+    double v[14];
+    int8_t ty = 0;
+    int64_t id = 0;
+    if (keep) {
+      v[0] = d.ipx[0][k], v[1] = d.ipy[0][k], v[2] = d.ipz[0][k], v[3] = d.ipx[1][k], v[4] = d.ipy[1][k];
+      v[5] = d.ipz[1][k], v[6] = d.ivx[k], v[7] = d.ivy[k], v[8] = d.ivz[k], v[9] = d.ifx[k], v[10] = d.ify[k];
+      v[11] = d.ifz[k], v[12] = d.irho[k], v[13] = d.idf[k];
+      ty = d.itype[k];
+      id = d.iids[k];
+    }
+    __syncthreads();
+    if (keep && dst != k) {
+      d.ipx[0][dst] = v[0], d.ipy[0][dst] = v[1], d.ipz[0][dst] = v[2], d.ipx[1][dst] = v[3], d.ipy[1][dst] = v[4];
+      d.ipz[1][dst] = v[5], d.ivx[dst] = v[6], d.ivy[dst] = v[7], d.ivz[dst] = v[8], d.ifx[dst] = v[9];
+      d.ify[dst] = v[10], d.ifz[dst] = v[11], d.irho[dst] = v[12], d.idf[dst] = v[13];
+      d.itype[dst] = ty;
+      d.iids[dst] = id;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) d.n_itl = s_base;
 }
 
 __global__ void k_mx_bookkeeping(const __grid_constant__ EnsParams P) {
@@ -574,6 +770,7 @@ int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, 
       k_mx_itl_items<true, true><<<itl_grid, 256, 0, s>>>(P);
     else
       k_mx_itl_items<true, false><<<itl_grid, 256, 0, s>>>(P);
+    if (P.conv2 > 0.0) k_mx_convert<<<P.n_itl_lats, MX_CONV_THREADS, 0, s>>>(P);
   }
   if (energy) {
     const int nl = S.walk.linear ? S.walk.n_lats : 1;

@@ -21,12 +21,28 @@
 //  * sites near the domain faces write their periodic ghost images themselves
 //    (no separate ghost-exchange pass), and the force pass closes the previous
 //    velocity-Verlet step and drifts to the next positions (double-buffered).
+#include <limits.h>
 #include <stdio.h>
 
 #include "mb_common.cuh"
 #include "mb_device.cuh"
 
 namespace mb {
+
+__device__ __forceinline__ int itl_n(const Itl64 &I) { return I.nd ? *I.nd : I.n; }
+
+// Lists the box site of a drifted lattice atom that left its site (conversion on).
+__device__ __forceinline__ void conv_check(const Geom &g, const StepParams &sp, int s, int cx, int y, int z, double nx,
+                                           double ny, double nz) {
+  if (!(sp.conv2 > 0.0)) return;
+  double X, Y, Z;
+  site_ideal(s, cx, y, z, sp.a0, X, Y, Z);
+  const double ux = nx - X, uy = ny - Y, uz = nz - Z;
+  if (ux * ux + uy * uy + uz * uz <= sp.conv2) return;
+  const int slot = atomicAdd(sp.cand_n, 1);
+  if (slot < MB_CAND_CAP) sp.cand[slot] = ((long long)z * g.by + y) * (2LL * g.bcx) + 2LL * cx + s;
+}
+
 
 #define MB_EPART_CAP 4096 // CTA partial sums per energy region
 #define MB_RHO_THREADS 1024  // 52 registers: a full SM of warps
@@ -281,6 +297,7 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
         L.nx[i] = nx;
         L.ny[i] = ny;
         L.nz[i] = nz;
+        conv_check(g, sp, s, cx, y, z, nx, ny, nz);
         if (g.images)
           for_images(g, s, cx, y, z, [&](long long idx, double ox, double oy, double oz) {
             L.nx[idx] = nx + ox;
@@ -423,7 +440,7 @@ __global__ void k_itl_clear(const Lattice64 L, const Itl64 I) {
 __global__ void k_itl_mark(const Geom g, const Lattice64 L, const Itl64 I) {
   const int lane = threadIdx.x & 31;
   const int it = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-  if (it >= I.n) return;
+  if (it >= itl_n(I)) return;
   const double qx = I.px[it], qy = I.py[it], qz = I.pz[it];
   const Window w = make_window(qx, qy, qz, I.a0, I.reach);
   const int ncand = w.nx * w.ny * w.nz;
@@ -452,7 +469,8 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
                 double rc2, double *e_partial) {
   const int lane = threadIdx.x & 31;
   const int nflag = min(I.flag_count[0], I.cap_flag);
-  const long long n_items = (long long)nflag + I.n;
+  const int n_itl = itl_n(I);
+  const long long n_items = (long long)nflag + n_itl;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
   double e_acc = 0.0;
   for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_items; w += wstride) {
@@ -469,7 +487,7 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
         const double d2 = dx * dx + dy * dy + dz * dz;
         if (d2 < rc2) rho += rho_of_r(P, L.code[j] & 0x3F, d2 * rsqrt(d2));
       }
-      for (int K = lane; K < I.n; K += 32) {
+      for (int K = lane; K < n_itl; K += 32) {
         const double dx = min_image(xi - I.px[K], g.Lx, g.iLx), dy = min_image(yi - I.py[K], g.Ly, g.iLy),
                      dz = min_image(zi - I.pz[K], g.Lz, g.iLz);
         const double d2 = dx * dx + dy * dy + dz * dz;
@@ -499,7 +517,7 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
         const double d2 = dx * dx + dy * dy + dz * dz;
         if (d2 < rc2) rho += rho_of_r(P, cj & 0x3F, d2 * rsqrt(d2));
       }
-      for (int K = lane; K < I.n; K += 32) {
+      for (int K = lane; K < n_itl; K += 32) {
         if (K == it) continue;
         const double dx = min_image(qx - I.px[K], g.Lx, g.iLx), dy = min_image(qy - I.py[K], g.Ly, g.iLy),
                      dz = min_image(qz - I.pz[K], g.Lz, g.iLz);
@@ -527,7 +545,8 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
                   const Itl64 I, const StepParams sp, double *e_pair, double *e_kin) {
   const int lane = threadIdx.x & 31;
   const int nflag = min(I.flag_count[0], I.cap_flag);
-  const long long n_items = (long long)nflag + I.n;
+  const int n_itl = itl_n(I);
+  const long long n_items = (long long)nflag + n_itl;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
   double ep_acc = 0.0, ek_acc = 0.0;
   for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_items; w += wstride) {
@@ -583,7 +602,7 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
         add_pair(xi - (L.px[j] + sx), yi - (L.py[j] + sy), zi - (L.pz[j] + sz), cj & 0x3F, L.df[j]);
       }
     }
-    for (int K = lane; K < I.n; K += 32) {
+    for (int K = lane; K < n_itl; K += 32) {
       if (!is_site && K == it) continue;
       add_pair(min_image(xi - I.px[K], g.Lx, g.iLx), min_image(yi - I.py[K], g.Ly, g.iLy), min_image(zi - I.pz[K], g.Lz, g.iLz),
                I.type[K], I.df[K]);
@@ -624,6 +643,7 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
             L.nx[i] = nx;
             L.ny[i] = ny;
             L.nz[i] = nz;
+            conv_check(g, sp, s, cx, y, z, nx, ny, nz);
             if (g.images)
               for_images(g, s, cx, y, z, [&](long long idx, double ox, double oy, double oz) {
                 L.nx[idx] = nx + ox;
@@ -657,13 +677,14 @@ int launch_itl_mark64(const Geom &g, const Lattice64 &L, const Itl64 &I, cudaStr
   k_itl_clear<<<grid, 256, 0, s>>>(L, I);
   MB_CUDA(cudaGetLastError());
   MB_CUDA(cudaMemsetAsync(I.flag_count, 0, sizeof(int), s));
-  k_itl_mark<<<(I.n * 32 + 255) / 256, 256, 0, s>>>(g, L, I);
+  const int nmax = I.nd ? I.cap : I.n;
+  if (nmax > 0) k_itl_mark<<<(nmax * 32 + 255) / 256, 256, 0, s>>>(g, L, I);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
 
 static int itl_grid(const Itl64 &I) {
-  const long long warps = (long long)I.cap_flag + I.n;
+  const long long warps = (long long)I.cap_flag + (I.nd ? I.cap : I.n);
   long long ctas = (warps * 32 + MB_ITL_THREADS - 1) / MB_ITL_THREADS;
   const long long cap = 4LL * device_sm_count();
   if (ctas > cap) ctas = cap;
@@ -673,7 +694,7 @@ static int itl_grid(const Itl64 &I) {
 
 int launch_itl_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const Itl64 &I,
                      double rc2, double *e_partial, int energy, cudaStream_t s) {
-  if (I.n == 0) return MB_OK;
+  if (!I.nd && I.n == 0) return MB_OK;
   const int grid = itl_grid(I);
   if (energy)
     k_itl_rho64<true><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, rc2, e_partial + 3 * MB_EPART_CAP);
@@ -685,13 +706,228 @@ int launch_itl_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, con
 
 int launch_itl_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const Itl64 &I,
                        const StepParams &sp, double *e_partial, int energy, cudaStream_t s) {
-  if (I.n == 0) return MB_OK;
+  if (!I.nd && I.n == 0) return MB_OK;
   const int grid = itl_grid(I);
   if (energy)
     k_itl_force64<true><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, sp, e_partial + 4 * MB_EPART_CAP,
                                                          e_partial + 5 * MB_EPART_CAP);
   else
     k_itl_force64<false><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, sp, nullptr, nullptr);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+// ------------------------------------------ lattice <-> interstitial bookkeeping
+// MISA-MD keeps atoms that have left their lattice site in its interstitial list (the
+// plugin only sees type < 0 for such sites, src/kernels/kernel_itl.hpp:44).  After the
+// drift of a step, one CTA
+//   1. sorts this step's candidates (box index of sites whose atom is farther than the
+//      conversion distance from the site) and appends their atoms to the interstitial
+//      list in that order, vacating the sites (and their ghost images);
+//   2. finds, for every interstitial, the nearest ideal site; one within the
+//      recombination distance of a vacant site claims it, the lowest list index
+//      winning a contested site;
+//   3. moves each winner onto its site and compacts the list, keeping its order.
+// Fixed orders (box index, list index) keep the result independent of thread timing.
+#define MB_CONV_THREADS 1024
+
+__global__ void __launch_bounds__(MB_CONV_THREADS, 1)
+    k_convert64(const Geom g, const Lattice64 L, const Itl64 I, const StepParams sp, double rec2,
+                int64_t *site_id, int *nd, long long *counters) {
+  __shared__ long long key[MB_CAND_CAP];
+  __shared__ unsigned removed[MB_CONV_ITL_MAX / 32];
+  __shared__ int s_scan[MB_CONV_THREADS / 32];
+  __shared__ int s_nclaim, s_base;
+  const int tid = threadIdx.x;
+  const int n0 = *nd;
+  // 1. conversions in box order
+  const int nraw = *sp.cand_n;
+  const int nc = min(nraw, MB_CAND_CAP);
+  int n2 = 1;
+  while (n2 < nc) n2 <<= 1;
+  for (int k = tid; k < n2; k += blockDim.x) key[k] = k < nc ? sp.cand[k] : LLONG_MAX;
+  __syncthreads();
+  if (nc > 1) bitonic_sort(key, n2);
+  const int room = max(0, I.cap - n0);
+  const int nconv = min(nc, room);
+  for (int r = tid; r < nconv; r += blockDim.x) {
+    const long long t = key[r];
+    int s, cx, y, z;
+    decode_box(g, t, s, cx, y, z);
+    const long long i = ext_index(g, s, cx, y, z);
+    const int k = n0 + r;
+    I.nx[k] = L.nx[i];
+    I.ny[k] = L.ny[i];
+    I.nz[k] = L.nz[i];
+    I.px[k] = L.px[i];
+    I.py[k] = L.py[i];
+    I.pz[k] = L.pz[i];
+    I.vx[k] = L.vx[i];
+    I.vy[k] = L.vy[i];
+    I.vz[k] = L.vz[i];
+    I.fx[k] = L.fx[i];
+    I.fy[k] = L.fy[i];
+    I.fz[k] = L.fz[i];
+    I.rho[k] = L.rho ? L.rho[i] : 0.0;
+    I.df[k] = L.df[i];
+    I.type[k] = (int8_t)(L.code[i] & 0x3F);
+    I.id[k] = site_id[t];
+    // vacant: both position buffers far away (the pair loops reject vacancies by
+    // position, and the buffer of this step comes back as the next step's drift target)
+    L.code[i] = -1;
+    L.nx[i] = L.ny[i] = L.nz[i] = MB_VACANT_POS;
+    L.px[i] = L.py[i] = L.pz[i] = MB_VACANT_POS;
+    L.vx[i] = L.vy[i] = L.vz[i] = 0.0;
+    L.fx[i] = L.fy[i] = L.fz[i] = 0.0;
+    for_images(g, s, cx, y, z, [&](long long idx, double, double, double) {
+      L.code[idx] = -1;
+      L.nx[idx] = L.ny[idx] = L.nz[idx] = MB_VACANT_POS;
+      L.px[idx] = L.py[idx] = L.pz[idx] = MB_VACANT_POS;
+    });
+  }
+  const int n1 = n0 + nconv;
+  if (tid == 0) {
+    counters[0] += nconv;
+    counters[2] += nc - nconv;
+    counters[3] += nraw - nc;
+    *sp.cand_n = 0;
+    s_nclaim = 0;
+  }
+  for (int w = tid; w < MB_CONV_ITL_MAX / 32; w += blockDim.x) removed[w] = 0u;
+  __syncthreads(); // vacated sites visible to the claims below
+  // 2. claims: nearest ideal site of every interstitial, when vacant and close enough
+  for (int k = tid; k < n1; k += blockDim.x) {
+    const double qx = I.nx[k], qy = I.ny[k], qz = I.nz[k];
+    double best = 1e300;
+    long long gx = 0, gy = 0, gz = 0;
+    int bs = 0;
+    for (int sl = 0; sl < 2; sl++) {
+      const double o = 0.5 * sp.a0 * sl;
+      const long long cx = llrint((qx - o) / sp.a0), cy = llrint((qy - o) / sp.a0), cz = llrint((qz - o) / sp.a0);
+      const double X = 0.5 * sp.a0 * (double)(2 * cx + sl), Y = sp.a0 * ((double)cy + 0.5 * sl),
+                   Z = sp.a0 * ((double)cz + 0.5 * sl);
+      const double dd = (qx - X) * (qx - X) + (qy - Y) * (qy - Y) + (qz - Z) * (qz - Z);
+      if (dd < best) {
+        best = dd;
+        gx = cx;
+        gy = cy;
+        gz = cz;
+        bs = sl;
+      }
+    }
+    if (!(best < rec2)) continue;
+    const int cx = pmod_int(gx, g.bcx), y = pmod_int(gy, g.by), z = pmod_int(gz, g.bz);
+    if (L.code[ext_index(g, bs, cx, y, z)] >= 0) continue;
+    const long long t = ((long long)z * g.by + y) * (2LL * g.bcx) + 2LL * cx + bs;
+    const int slot = atomicAdd(&s_nclaim, 1);
+    if (slot < MB_CAND_CAP) key[slot] = (t << 17) | (long long)k; // k < 2^16 (MB_CONV_ITL_MAX)
+  }
+  __syncthreads();
+  const int ncl = min(s_nclaim, MB_CAND_CAP);
+  n2 = 1;
+  while (n2 < ncl) n2 <<= 1;
+  for (int k = ncl + tid; k < n2; k += blockDim.x) key[k] = LLONG_MAX;
+  __syncthreads();
+  if (ncl > 1) bitonic_sort(key, n2);
+  // 3. winners move onto their sites
+  int nrec = 0;
+  for (int r = tid; r < ncl; r += blockDim.x) {
+    const long long t = key[r] >> 17;
+    if (r > 0 && (key[r - 1] >> 17) == t) continue; // a lower list index took the site
+    const int k = (int)(key[r] & 0x1FFFF);
+    int s, cx, y, z;
+    decode_box(g, t, s, cx, y, z);
+    const long long i = ext_index(g, s, cx, y, z);
+    double X, Y, Z;
+    site_ideal(s, cx, y, z, sp.a0, X, Y, Z);
+    // displacement of the interstitial from the nearest image of the site
+    const double ux = min_image(I.nx[k] - X, g.Lx, g.iLx), uy = min_image(I.ny[k] - Y, g.Ly, g.iLy),
+                 uz = min_image(I.nz[k] - Z, g.Lz, g.iLz);
+    const double nx = X + ux, ny = Y + uy, nz = Z + uz;
+    // the previous positions too (the buffer a download reads), on the same image
+    const double px = nx + (I.px[k] - I.nx[k]), py = ny + (I.py[k] - I.ny[k]), pz = nz + (I.pz[k] - I.nz[k]);
+    const int8_t ty = I.type[k];
+    L.code[i] = ty;
+    L.nx[i] = nx;
+    L.ny[i] = ny;
+    L.nz[i] = nz;
+    L.px[i] = px;
+    L.py[i] = py;
+    L.pz[i] = pz;
+    L.vx[i] = I.vx[k];
+    L.vy[i] = I.vy[k];
+    L.vz[i] = I.vz[k];
+    L.fx[i] = I.fx[k];
+    L.fy[i] = I.fy[k];
+    L.fz[i] = I.fz[k];
+    L.df[i] = I.df[k];
+    for_images(g, s, cx, y, z, [&](long long idx, double ox, double oy, double oz) {
+      L.code[idx] = ty;
+      L.nx[idx] = nx + ox;
+      L.ny[idx] = ny + oy;
+      L.nz[idx] = nz + oz;
+      L.px[idx] = px + ox;
+      L.py[idx] = py + oy;
+      L.pz[idx] = pz + oz;
+    });
+    site_id[t] = I.id[k];
+    atomicOr(&removed[k >> 5], 1u << (k & 31));
+    nrec++;
+  }
+  const double nrec_all = block_sum((double)nrec); // exact for integer counts
+  if (tid == 0) {
+    counters[1] += (long long)nrec_all;
+    s_base = 0;
+  }
+  __syncthreads();
+  // 4. stable compaction of the list
+  for (int c0 = 0; c0 < n1; c0 += blockDim.x) {
+    const int k = c0 + tid;
+    const bool keep = k < n1 && !((removed[k >> 5] >> (k & 31)) & 1u);
+    // block exclusive scan of keep
+    const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+    const int lane = tid & 31, wid = tid >> 5;
+    if (lane == 0) s_scan[wid] = __popc(ballot);
+    __syncthreads();
+    if (tid == 0) {
+      int acc = s_base;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+        const int c = s_scan[w];
+        s_scan[w] = acc;
+        acc += c;
+      }
+      s_base = acc;
+    }
+    __syncthreads();
+    const int dst = s_scan[wid] + __popc(ballot & ((1u << lane) - 1u));
+    double v[14];
+    int8_t ty = 0;
+    int64_t id = 0;
+    if (keep) {
+      v[0] = I.px[k], v[1] = I.py[k], v[2] = I.pz[k], v[3] = I.nx[k], v[4] = I.ny[k], v[5] = I.nz[k];
+      v[6] = I.vx[k], v[7] = I.vy[k], v[8] = I.vz[k], v[9] = I.fx[k], v[10] = I.fy[k], v[11] = I.fz[k];
+      v[12] = I.rho[k], v[13] = I.df[k];
+      ty = I.type[k];
+      id = I.id[k];
+    }
+    __syncthreads(); // every read of this chunk before any write (dst <= k)
+    if (keep && dst != k) {
+      I.px[dst] = v[0], I.py[dst] = v[1], I.pz[dst] = v[2], I.nx[dst] = v[3], I.ny[dst] = v[4], I.nz[dst] = v[5];
+      I.vx[dst] = v[6], I.vy[dst] = v[7], I.vz[dst] = v[8], I.fx[dst] = v[9], I.fy[dst] = v[10], I.fz[dst] = v[11];
+      I.rho[dst] = v[12], I.df[dst] = v[13];
+      I.type[dst] = ty;
+      I.id[dst] = id;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) *nd = s_base;
+}
+
+int launch_convert64(const Geom &g, const Lattice64 &L, const Itl64 &I, const StepParams &sp, double rec2,
+                     int64_t *site_id, int *nd, long long *counters, cudaStream_t s) {
+  if (!(sp.conv2 > 0.0)) return MB_OK;
+  if (I.cap > MB_CONV_ITL_MAX) return fail(MB_ERR_ARG, "interstitial capacity above the conversion limit (65536)");
+  k_convert64<<<1, MB_CONV_THREADS, 0, s>>>(g, L, I, sp, rec2, site_id, nd, counters);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
@@ -737,7 +973,8 @@ int launch_images64(const Geom &g, const Lattice64 &L, int what, cudaStream_t s)
 // from the host each step): v += h f ; x += dt v, then refresh ghost images.
 __global__ void k_kick_drift64(const Geom g, const Lattice64 L, const Itl64 I, const StepParams sp) {
   const long long n = 2LL * g.bcx * g.by * g.bz;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n + I.n;
+  const int n_itl = itl_n(I);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n + n_itl;
        t += (long long)gridDim.x * blockDim.x) {
     if (t >= n) {
       const int it = (int)(t - n);
@@ -774,7 +1011,7 @@ __global__ void k_kick_drift64(const Geom g, const Lattice64 L, const Itl64 I, c
 }
 
 int launch_kick_drift64(const Geom &g, const Lattice64 &L, const Itl64 &I, const StepParams &sp, cudaStream_t s) {
-  const long long n = 2LL * g.bcx * g.by * g.bz + I.n;
+  const long long n = 2LL * g.bcx * g.by * g.bz + (I.nd ? I.cap : I.n);
   int grid = (int)((n + 255) / 256);
   if (grid > 8 * device_sm_count()) grid = 8 * device_sm_count();
   k_kick_drift64<<<grid, 256, 0, s>>>(g, L, I, sp);

@@ -37,6 +37,11 @@ struct mb_sim {
   int8_t *itype = nullptr;
   int64_t *iid = nullptr;
   int *flag_list = nullptr, *flag_count = nullptr;
+  int *d_nitl = nullptr; // device-resident interstitial count (conversions change it)
+  // lattice <-> interstitial conversion (off while conv_d == 0)
+  double conv_d = 0.0, rec_d = 0.0;
+  long long *d_cand = nullptr, *d_conv_counters = nullptr; // counters[4]
+  int *d_cand_n = nullptr;
   // energies
   double *epart = nullptr;
   double *eout = nullptr; // [cap_e][2]
@@ -95,6 +100,8 @@ Lattice64 sim_lattice(mb_sim *s, int which) {
 Itl64 sim_itl(mb_sim *s, int which) {
   Itl64 I{};
   I.n = s->n_itl;
+  I.nd = s->d_nitl;
+  I.cap = s->cap_itl;
   I.cap_flag = s->cap_flag;
   I.px = s->ipos[which][0];
   I.py = s->ipos[which][1];
@@ -111,6 +118,7 @@ Itl64 sim_itl(mb_sim *s, int which) {
   I.rho = s->irho;
   I.df = s->idf;
   I.type = s->itype;
+  I.id = s->iid;
   I.flag_list = s->flag_list;
   I.flag_count = s->flag_count;
   I.a0 = s->cfg.lattice_const;
@@ -126,8 +134,18 @@ StepParams sim_params(const mb_sim *s, int kick_pre, int drift) {
   sp.mass = s->cfg.mass;
   sp.kick_pre = kick_pre;
   sp.drift = drift;
+  sp.a0 = s->cfg.lattice_const;
+  if (drift && s->conv_d > 0.0) {
+    sp.conv2 = s->conv_d * s->conv_d;
+    sp.cand = s->d_cand;
+    sp.cand_n = s->d_cand_n;
+  }
   return sp;
 }
+
+// Interstitial passes run when the host placed interstitials or conversions may create
+// them (the count itself lives on the device).
+static bool itl_active(const mb_sim *s) { return s->n_itl > 0 || s->conv_d > 0.0; }
 
 // One FP64 step at positions pos[cur] (forces, closing kick, drift to pos[cur^1]).
 static int step64(mb_sim *s, int energy, int kick_pre, int drift, int timed) {
@@ -137,7 +155,7 @@ static int step64(mb_sim *s, int energy, int kick_pre, int drift, int timed) {
   StepParams sp = sim_params(s, kick_pre, drift);
   double *ep = energy ? s->epart : nullptr;
   if (energy) MB_CUDA(cudaMemsetAsync(s->epart, 0, sizeof(double) * energy_partials_needed(), s->stream));
-  const int itl = s->n_itl > 0;
+  const int itl = itl_active(s);
   if (itl) MB_TRY(launch_itl_mark64(s->g, L, I, s->stream));
   if (timed) MB_CUDA(cudaEventRecord(s->ev[4], s->stream));
   MB_TRY(launch_rho64(s->g, s->st, P, L, sp.rc2, ep, energy, itl, s->stream));
@@ -147,6 +165,8 @@ static int step64(mb_sim *s, int energy, int kick_pre, int drift, int timed) {
   MB_TRY(launch_force64(s->g, s->st, P, L, sp, ep, energy, itl, s->stream));
   if (timed) MB_CUDA(cudaEventRecord(s->ev[7], s->stream));
   if (itl) MB_TRY(launch_itl_force64(s->g, s->st, P, L, I, sp, ep, energy, s->stream));
+  if (sp.conv2 > 0.0)
+    MB_TRY(launch_convert64(s->g, L, I, sp, s->rec_d * s->rec_d, s->id, s->d_nitl, s->d_conv_counters, s->stream));
   return MB_OK;
 }
 
@@ -412,6 +432,14 @@ int mb_sim_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **o
   s->cap_flag = std::max(1, s->cap_itl * per);
   if ((rc = dalloc(s, (void **)&s->flag_list, (size_t)s->cap_flag * sizeof(int))) != MB_OK) return cleanup(rc);
   if ((rc = dalloc(s, (void **)&s->flag_count, 2 * sizeof(int))) != MB_OK) return cleanup(rc);
+  if ((rc = dalloc(s, (void **)&s->d_nitl, sizeof(int))) != MB_OK) return cleanup(rc);
+  if ((rc = dalloc(s, (void **)&s->d_cand, MB_CAND_CAP * sizeof(long long))) != MB_OK) return cleanup(rc);
+  if ((rc = dalloc(s, (void **)&s->d_cand_n, sizeof(int))) != MB_OK) return cleanup(rc);
+  if ((rc = dalloc(s, (void **)&s->d_conv_counters, 4 * sizeof(long long))) != MB_OK) return cleanup(rc);
+  if (cudaMemsetAsync(s->d_nitl, 0, sizeof(int), s->stream) != cudaSuccess ||
+      cudaMemsetAsync(s->d_cand_n, 0, sizeof(int), s->stream) != cudaSuccess ||
+      cudaMemsetAsync(s->d_conv_counters, 0, 4 * sizeof(long long), s->stream) != cudaSuccess)
+    return cleanup(fail(MB_ERR_CUDA, "memset failed"));
   if (cudaMemsetAsync(s->flag_count, 0, 2 * sizeof(int), s->stream) != cudaSuccess)
     return cleanup(fail(MB_ERR_CUDA, "memset failed"));
   // vacant everywhere until an upload
@@ -433,7 +461,7 @@ int mb_sim_destroy(mb_sim *s) {
   drop_graph(s);
   if (s->ens) mb_ensemble_destroy(s->ens);
   void *ptrs[] = {s->code, s->df, s->rho, s->id, s->epart, s->eout, s->stage, s->bad, s->irho, s->idf, s->itype,
-                  s->iid, s->flag_list, s->flag_count};
+                  s->iid, s->flag_list, s->flag_count, s->d_nitl, s->d_cand, s->d_cand_n, s->d_conv_counters};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int b = 0; b < 2; b++)
@@ -472,6 +500,9 @@ static int upload_itl(mb_sim *s, const mb_atom_element *itl, int32_t n_itl, int 
   if (n_itl < 0 || n_itl > s->cap_itl) return fail(MB_ERR_ARG, "n_itl exceeds max_interstitials");
   if (n_itl > 0 && !itl) return fail(MB_ERR_ARG, "null interstitial array");
   s->n_itl = n_itl;
+  MB_CUDA(cudaStreamSynchronize(s->stream));
+  MB_CUDA(cudaMemcpy(s->d_nitl, &s->n_itl, sizeof(int), cudaMemcpyHostToDevice));
+  MB_CUDA(cudaMemsetAsync(s->d_cand_n, 0, sizeof(int), s->stream));
   if (n_itl == 0) return MB_OK;
   std::vector<double> buf((size_t)n_itl);
   std::vector<int8_t> t((size_t)n_itl);
@@ -580,6 +611,7 @@ int mb_sim_download(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl,
   MB_CUDA(cudaMemcpyAsync(box_atoms, s->stage, (size_t)s->n_box * sizeof(mb_atom_element), cudaMemcpyDeviceToHost,
                           s->stream));
   MB_CUDA(cudaStreamSynchronize(s->stream));
+  MB_CUDA(cudaMemcpy(&s->n_itl, s->d_nitl, sizeof(int), cudaMemcpyDeviceToHost));
   if (n_itl) *n_itl = s->n_itl;
   if (itl) MB_TRY(download_itl(s, itl, which, unkick));
   return MB_OK;
@@ -607,8 +639,9 @@ int mb_sim_sync(mb_sim *s) {
   if (s && s->ens) return mb_ensemble_sync(s->ens);
   if (!s) return fail(MB_ERR_ARG, "null sim");
   MB_CUDA(cudaStreamSynchronize(s->stream));
+  MB_CUDA(cudaMemcpy(&s->n_itl, s->d_nitl, sizeof(int), cudaMemcpyDeviceToHost));
   int fc[2] = {0, 0};
-  if (s->n_itl > 0) {
+  if (itl_active(s)) {
     MB_CUDA(cudaMemcpy(fc, s->flag_count, sizeof(fc), cudaMemcpyDeviceToHost));
     if (fc[1]) return fail(MB_ERR_ARG, "interstitial flag list overflowed");
   }
@@ -707,6 +740,40 @@ int mb_sim_step_host(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl
                           s->stream));
   MB_CUDA(cudaStreamSynchronize(s->stream));
   if (itl) MB_TRY(download_itl(s, itl, 0, 0));
+  return MB_OK;
+}
+
+int mb_sim_set_conversion(mb_sim *s, double convert_distance, double recombine_distance) {
+  if (s && s->ens) {
+    MB_TRY(mixed_need_slot(s));
+    return mb_ensemble_set_conversion(s->ens, convert_distance, recombine_distance);
+  }
+  if (!s) return fail(MB_ERR_ARG, "null sim");
+  if (convert_distance < 0 || recombine_distance < 0 || (convert_distance > 0 && recombine_distance >= convert_distance))
+    return fail(MB_ERR_ARG, "need 0 <= recombine_distance < convert_distance (0 switches conversion off)");
+  if (convert_distance > 0 && s->cap_itl > MB_CONV_ITL_MAX)
+    return fail(MB_ERR_ARG, "max_interstitials above the conversion limit (65536)");
+  if (convert_distance > 0 && s->cap_itl < 1) return fail(MB_ERR_ARG, "conversion needs max_interstitials > 0");
+  MB_CUDA(cudaStreamSynchronize(s->stream));
+  s->conv_d = convert_distance;
+  s->rec_d = convert_distance > 0 ? recombine_distance : 0.0;
+  drop_graph(s); // the captured step pair changes
+  return MB_OK;
+}
+
+int mb_sim_conversion_stats(mb_sim *s, int64_t *counters, int32_t *n_itl) {
+  if (s && s->ens) {
+    MB_TRY(mixed_need_slot(s));
+    return mb_ensemble_conversion_stats(s->ens, s->slot, counters, n_itl);
+  }
+  if (!s) return fail(MB_ERR_ARG, "null sim");
+  MB_CUDA(cudaStreamSynchronize(s->stream));
+  long long c[4] = {0, 0, 0, 0};
+  MB_CUDA(cudaMemcpy(c, s->d_conv_counters, sizeof(c), cudaMemcpyDeviceToHost));
+  MB_CUDA(cudaMemcpy(&s->n_itl, s->d_nitl, sizeof(int), cudaMemcpyDeviceToHost));
+  if (counters)
+    for (int k = 0; k < 4; k++) counters[k] = (int64_t)c[k];
+  if (n_itl) *n_itl = s->n_itl;
   return MB_OK;
 }
 

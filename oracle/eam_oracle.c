@@ -547,6 +547,89 @@ void orc_compute_forces(const orc_pot *p, const orc_domain *d, orc_atom *atoms, 
   }
 }
 
+/* ------------------------------------- lattice <-> interstitial bookkeeping */
+
+static inline void box_ideal(int64_t x, int64_t y, int64_t z, double a0, double *X, double *Y, double *Z) {
+  const double h = 0.5 * (double)(x & 1);
+  *X = 0.5 * a0 * (double)x;
+  *Y = a0 * ((double)y + h);
+  *Z = a0 * ((double)z + h);
+}
+
+/* MISA-MD keeps atoms that have left their lattice site in its interstitial list (the
+ * plugin only ever sees type < 0 for such sites, src/kernels/kernel_itl.hpp:44).  After a
+ * step: every box site whose atom is farther than d_conv from the site's ideal position
+ * (box order) moves to the end of the interstitial list and the site becomes vacant;
+ * then every interstitial (list order) within d_rec of a vacant site's ideal position
+ * takes that site (the first claim wins) and leaves the list, which keeps its order.
+ * Returns the new count; counters[0] += conversions, [1] += recombinations, [2] += atoms
+ * that could not be converted because the list was full (they stay on their site). */
+int orc_convert(const orc_domain *d, double a0, orc_atom *atoms, orc_atom *itl, int n_itl, int cap, double d_conv,
+                double d_rec, int64_t *counters) {
+  const int64_t bx = d->box_size_x, by = d->box_size_y, bz = d->box_size_z;
+  const double c2 = d_conv * d_conv, r2 = d_rec * d_rec;
+  for (int64_t z = 0; z < bz; z++)
+    for (int64_t y = 0; y < by; y++)
+      for (int64_t x = 0; x < bx; x++) {
+        orc_atom *a = atoms + site_linear(d, x, y, z);
+        if (a->type < 0) continue;
+        double X, Y, Z;
+        box_ideal(x, y, z, a0, &X, &Y, &Z);
+        const double ux = a->x[0] - X, uy = a->x[1] - Y, uz = a->x[2] - Z;
+        if (ux * ux + uy * uy + uz * uz <= c2) continue;
+        if (n_itl >= cap) {
+          counters[2]++;
+          continue;
+        }
+        itl[n_itl++] = *a;
+        memset(a, 0, sizeof(*a));
+        a->type = -1;
+        a->x[0] = X;
+        a->x[1] = Y;
+        a->x[2] = Z;
+        counters[0]++;
+      }
+  int keep = 0;
+  for (int k = 0; k < n_itl; k++) {
+    const orc_atom q = itl[k];
+    /* nearest ideal site: the nearer of the two simple-cubic sublattices */
+    int64_t bs[3] = {0, 0, 0};
+    double best = 1e300, bu[3] = {0, 0, 0};
+    for (int s = 0; s < 2; s++) {
+      const double o = 0.5 * a0 * (double)s;
+      const int64_t cx = (int64_t)nearbyint((q.x[0] - o) / a0), cy = (int64_t)nearbyint((q.x[1] - o) / a0),
+                    cz = (int64_t)nearbyint((q.x[2] - o) / a0);
+      double X, Y, Z;
+      box_ideal(2 * cx + s, cy, cz, a0, &X, &Y, &Z);
+      const double u[3] = {q.x[0] - X, q.x[1] - Y, q.x[2] - Z};
+      const double dd = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+      if (dd < best) {
+        best = dd;
+        bs[0] = 2 * cx + s;
+        bs[1] = cy;
+        bs[2] = cz;
+        bu[0] = u[0];
+        bu[1] = u[1];
+        bu[2] = u[2];
+      }
+    }
+    const int64_t xb = pmod(bs[0], bx), yb = pmod(bs[1], by), zb = pmod(bs[2], bz);
+    orc_atom *site = atoms + site_linear(d, xb, yb, zb);
+    if (best < r2 && site->type < 0) {
+      double X, Y, Z;
+      box_ideal(xb, yb, zb, a0, &X, &Y, &Z);
+      *site = q;
+      site->x[0] = X + bu[0];
+      site->x[1] = Y + bu[1];
+      site->x[2] = Z + bu[2];
+      counters[1]++;
+      continue;
+    }
+    itl[keep++] = q;
+  }
+  return keep;
+}
+
 static void half_kick_and_drift(const orc_domain *d, orc_atom *atoms, orc_atom *itl, int n_itl, double h, double dt,
                                 int drift) {
 #pragma omp parallel for schedule(static) collapse(2)
@@ -593,6 +676,23 @@ void orc_md_run(const orc_pot *p, const orc_domain *d, orc_atom *atoms, orc_atom
       energies[s].ke = ke * ORC_MVV2E;
     }
   }
+}
+
+/* nsteps velocity-Verlet steps with the lattice <-> interstitial bookkeeping after
+ * every drift, before the forces at the new positions: the order of the device-resident
+ * run.  itl holds cap records, the first n_itl of them the list; returns the new count
+ * (forces in atoms / itl must be current on entry). */
+int orc_md_run_convert(const orc_pot *p, const orc_domain *d, orc_atom *atoms, orc_atom *itl, int n_itl, int cap,
+                       const int64_t *even, size_t n_even, const int64_t *odd, size_t n_odd,
+                       const orc_md_params *mp, int nsteps, double d_conv, double d_rec, int64_t *counters) {
+  const double h = 0.5 * mp->dt * ORC_FTM2V / mp->mass;
+  for (int s = 1; s <= nsteps; s++) {
+    half_kick_and_drift(d, atoms, itl, n_itl, h, mp->dt, 1);
+    n_itl = orc_convert(d, mp->a0, atoms, itl, n_itl, cap, d_conv, d_rec, counters);
+    orc_compute_forces(p, d, atoms, itl, n_itl, even, n_even, odd, n_odd, mp, NULL);
+    half_kick_and_drift(d, atoms, itl, n_itl, h, mp->dt, 0);
+  }
+  return n_itl;
 }
 
 int orc_num_threads(void) {

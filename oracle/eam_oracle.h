@@ -106,6 +106,18 @@ void orc_md_run(const orc_pot *p, const orc_domain *d, orc_atom *atoms, orc_atom
                 const int64_t *even, size_t n_even, const int64_t *odd, size_t n_odd, const orc_md_params *mp,
                 int nsteps, orc_energy *energies);
 
+/* Lattice <-> interstitial bookkeeping after a step (see eam_oracle.c): atoms farther
+ * than d_conv from their site join the interstitial list (box order), interstitials
+ * within d_rec of a vacant site take it (list order).  Returns the new count;
+ * counters[3] accumulates conversions, recombinations, refused conversions. */
+int orc_convert(const orc_domain *d, double a0, orc_atom *atoms, orc_atom *itl, int n_itl, int cap, double d_conv,
+                double d_rec, int64_t *counters);
+
+/* nsteps steps with orc_convert after every drift (before the new forces). */
+int orc_md_run_convert(const orc_pot *p, const orc_domain *d, orc_atom *atoms, orc_atom *itl, int n_itl, int cap,
+                       const int64_t *even, size_t n_even, const int64_t *odd, size_t n_odd,
+                       const orc_md_params *mp, int nsteps, double d_conv, double d_rec, int64_t *counters);
+
 int orc_num_threads(void);
 void orc_set_threads(int n);
 

@@ -79,6 +79,11 @@ def lib() -> C.CDLL:
             "orc_rho_pass": (None, [_P, C.POINTER(Domain), _P, _PI64, C.c_size_t, _PI64, C.c_size_t, C.c_double]),
             "orc_df_pass": (None, [_P, C.POINTER(Domain), _P]),
             "orc_force_pass": (None, [_P, C.POINTER(Domain), _P, _PI64, C.c_size_t, _PI64, C.c_size_t, C.c_double]),
+            "orc_md_run_convert": (C.c_int, [_P, C.POINTER(Domain), _P, _P, C.c_int, C.c_int, _PI64, C.c_size_t,
+                                             _PI64, C.c_size_t, C.POINTER(MdParams), C.c_int, C.c_double,
+                                             C.c_double, _PI64]),
+            "orc_convert": (C.c_int, [C.POINTER(Domain), C.c_double, _P, _P, C.c_int, C.c_int, C.c_double,
+                                      C.c_double, _PI64]),
             "orc_rho_pass_half": (None, [_P, C.POINTER(Domain), _P, _PI64, C.c_size_t, _PI64, C.c_size_t,
                                          C.c_double]),
             "orc_force_pass_half": (None, [_P, C.POINTER(Domain), _P, _PI64, C.c_size_t, _PI64, C.c_size_t,
@@ -184,6 +189,25 @@ def df_pass(pot: Pot, dom: Domain, ext: np.ndarray) -> None:
 
 def force_pass(pot: Pot, dom: Domain, ext: np.ndarray, even, odd, cutoff: float) -> None:
     lib().orc_force_pass(pot.h, C.byref(dom), _a(ext), _i(even), even.size, _i(odd), odd.size, cutoff)
+
+
+def convert(dom: Domain, a0: float, ext: np.ndarray, itl: np.ndarray, n_itl: int, d_conv: float, d_rec: float,
+            counters: np.ndarray | None = None) -> int:
+    """Lattice <-> interstitial bookkeeping after a step (orc_convert): itl is a buffer
+    whose length is the capacity, its first n_itl records the list; returns the new
+    count.  counters (int64[3]) accumulates conversions, recombinations, refusals."""
+    c = np.zeros(3, dtype=np.int64) if counters is None else counters
+    assert c.dtype == np.int64 and c.size == 3
+    return int(lib().orc_convert(C.byref(dom), a0, _a(ext), _a(itl), n_itl, itl.shape[0], d_conv, d_rec, _i(c)))
+
+
+def md_run_convert(pot: Pot, dom: Domain, ext: np.ndarray, itl: np.ndarray, n_itl: int, even, odd, mp: MdParams,
+                   nsteps: int, d_conv: float, d_rec: float, counters: np.ndarray | None = None) -> int:
+    """nsteps steps with the lattice <-> interstitial bookkeeping after every drift
+    (orc_md_run_convert); itl is a buffer of capacity len(itl).  Returns the new count."""
+    c = np.zeros(3, dtype=np.int64) if counters is None else counters
+    return int(lib().orc_md_run_convert(pot.h, C.byref(dom), _a(ext), _a(itl), n_itl, itl.shape[0], _i(even),
+                                        even.size, _i(odd), odd.size, C.byref(mp), nsteps, d_conv, d_rec, _i(c)))
 
 
 def half_stencil(st: np.ndarray) -> np.ndarray:
