@@ -403,7 +403,9 @@ def run_nve(args, mb, world, rank, local, pg) -> None:
     forces at those positions) is read back and the FP64 path evaluates the forces at the
     same positions; the FP64 path matches the CPU oracle to ~1e-15
     (tests/test_gpu_parity.py).  Atoms that leave their lattice site move to the
-    interstitial list and back (mb_sim_set_conversion, on unless --no-conversion).
+    interstitial list and back (mb_sim_set_conversion, on unless --no-conversion; 1.0 A
+    and 0.5 A by default: thermal excursions at 900 K reach ~0.7 A with this potential,
+    while an atom hopping to a neighbouring vacancy passes 1.24 A from its site).
     Energy drift is reported over the --nve-steps production steps after the
     equilibration (E(t) - E(t_eq)) / N in eV/atom, plus the offset from step 0: a run
     started from a perfect lattice moves about 1e-5 eV/atom within its first few hundred
@@ -421,15 +423,20 @@ def run_nve(args, mb, world, rank, local, pg) -> None:
     tables = mb.potential.fe_analytic()
     conversion = not args.no_conversion
     cap = itl.shape[0] + (4096 if conversion else 0)
-    kw = dict(lattice_const=A0, mass=MASS, dt=DT, cutoff=RC, stencil_skin=SKIN, max_interstitials=max(1, cap))
+    kw = dict(lattice_const=A0, mass=MASS, dt=DT, cutoff=RC, stencil_skin=args.nve_skin,
+              max_interstitials=max(1, cap))
     every = max(1, args.check_every)
     total = args.nve_equil + args.nve_steps
     prec = mb.MB_PREC_FP64 if args.nve_precision == "fp64" else mb.MB_PREC_MIXED
     mixed = mb.Sim(wl["cells"], tables, precision=prec, **kw)
+    # the checks evaluate both paths on the read-back state (same positions, same
+    # lattice / interstitial membership): a fresh probe of the run's precision and the
+    # FP64 reference, neither doing bookkeeping
+    probe = mb.Sim(wl["cells"], tables, precision=prec, **kw)
     ref = mb.Sim(wl["cells"], tables, precision=mb.MB_PREC_FP64, **kw)
     mixed.upload(box, itl)
     if conversion:
-        mixed.set_conversion(SKIN, 0.5 * SKIN)
+        mixed.set_conversion(args.conv_distance, args.rec_distance)
     del box, itl
     steps_done, rms, rms_steps, e_rec = 0, [], [], []
     t_md = 0.0
@@ -439,14 +446,17 @@ def run_nve(args, mb, world, rank, local, pg) -> None:
     while True:
         b, i = mixed.download()
         live = b["type"] >= 0
-        f32 = np.concatenate([b["f"][live], i["f"]])
+        probe.upload(b, i)
+        probe.run(0)
+        pb, pi = probe.download()
+        f32 = np.concatenate([pb["f"][live], pi["f"]])
         ref.upload(b, i)
         ref.run(0)
         rb, ri = ref.download()
         f64 = np.concatenate([rb["f"][live], ri["f"]])
         rms.append(float(np.sqrt(np.sum((f32 - f64) ** 2) / np.sum(f64 ** 2))))
         rms_steps.append(steps_done)
-        del b, i, rb, ri, f32, f64, live
+        del b, i, pb, pi, rb, ri, f32, f64, live
         if steps_done >= total:
             break
         n = min(every, total - steps_done)
@@ -459,6 +469,7 @@ def run_nve(args, mb, world, rank, local, pg) -> None:
     e = np.concatenate([x for x in e_rec if x.size], axis=0)
     conv = mixed.conversion_stats() if conversion else None
     mixed.close()
+    probe.close()
     ref.close()
     etot = e[:, 1] + e[:, 2]
     e0 = float(etot[0])
@@ -475,6 +486,8 @@ def run_nve(args, mb, world, rank, local, pg) -> None:
             "dtype": "f64" if prec == mb.MB_PREC_FP64 else "f32+f64",
             "data": "synthetic (seeded lattice, analytic tabulated potential)",
             "config": {"workload": wl["name"] + "_nve", "cells": list(wl["cells"]), "atoms_per_gpu": n_atoms,
+                       "stencil_skin": args.nve_skin, "convert_distance": args.conv_distance if conversion else None,
+                       "recombine_distance": args.rec_distance if conversion else None,
                        "check_every": every, "timing": "wall clock of the MD segments (energy steps included)"},
             "force_rms_rel_err_vs_fp64": {"max": max(rms), "mean": float(np.mean(rms)), "final": rms[-1],
                                           "steps": rms_steps, "values": rms},
@@ -589,6 +602,11 @@ def main() -> None:
     ap.add_argument("--nve-itl", type=int, default=None, help="interstitials of --config nve (default 763)")
     ap.add_argument("--nve-equil", type=int, default=1000, help="equilibration steps before the drift window")
     ap.add_argument("--no-conversion", action="store_true", help="--config nve without lattice <-> interstitial moves")
+    ap.add_argument("--conv-distance", type=float, default=1.0,
+                    help="--config nve: an atom this far (A) from its site joins the interstitial list")
+    ap.add_argument("--nve-skin", type=float, default=SKIN, help="--config nve: stencil skin (A)")
+    ap.add_argument("--rec-distance", type=float, default=0.5,
+                    help="--config nve: an interstitial this close (A) to a vacant site takes it")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, pg = dist_setup()
