@@ -604,7 +604,10 @@ def main() -> None:
     ap.add_argument("--no-conversion", action="store_true", help="--config nve without lattice <-> interstitial moves")
     ap.add_argument("--conv-distance", type=float, default=1.0,
                     help="--config nve: an atom this far (A) from its site joins the interstitial list")
-    ap.add_argument("--nve-skin", type=float, default=SKIN, help="--config nve: stencil skin (A)")
+    ap.add_argument("--nve-skin", type=float, default=1.3,
+                    help="--config nve: stencil skin (A); at 900 K thermal excursions reach ~0.7 A with this "
+                         "potential, so the stencil must cover twice that (1.3 A: every site closer than 6.9 A, "
+                         "complete up to 1.39 A of combined displacement)")
     ap.add_argument("--rec-distance", type=float, default=0.5,
                     help="--config nve: an interstitial this close (A) to a vacant site takes it")
     args = ap.parse_args()

@@ -594,10 +594,14 @@ static const char *mx_stencil(const mb_ensemble *e, const LatDesc &d, MxStencil 
   S.walk.nyb = nyb;
   S.walk.m_nyb = 0xFFFFFFFFu / nyb;
   S.walk.n_units = (unsigned)units;
-  // built-in shells: the stencil must be exactly BCC shells 1-7 (|h|^2 <= 19 < 20)
-  const double r7 = h * sqrt(19.0), r8 = h * sqrt(20.0);
-  S.fixed = (vs.size() == 88 && r7 < reach && reach <= r8 && (long long)ey * ecx < (1ll << 31)) ? 1 : 0;
-  const int n2s[MX_SHELLS] = {3, 4, 8, 11, 12, 16, 19};
+  // built-in shells: the stencil must be exactly BCC shells 1-7 (|h|^2 <= 19 < 20) or
+  // 1-8 (|h|^2 <= 20 < 24)
+  const double r7 = h * sqrt(19.0), r8 = h * sqrt(20.0), r9 = h * sqrt(24.0);
+  const bool small = (long long)ey * ecx < (1ll << 31);
+  S.fixed = (small && vs.size() == 88 && r7 < reach && reach <= r8)    ? 7
+            : (small && vs.size() == 112 && r8 < reach && reach <= r9) ? 8
+                                                                        : 0;
+  const int n2s[MX_SHELLS] = {3, 4, 8, 11, 12, 16, 19, 20};
   MxShells &Q = S.sh;
   const double grid_ds[2] = {pp.ds_r, pp.ds_f};
   const int grid_n[2] = {pp.n_rs, pp.n_fs};

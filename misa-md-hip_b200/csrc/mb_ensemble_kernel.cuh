@@ -139,10 +139,11 @@ struct MxWalk {
 };
 
 // Split-mode stencil built into the kernel: the BCC neighbour shells up to |h|^2 = 19
-// (half-lattice units), which is the stencil whenever cutoff + skin lies between the
-// 7th and 8th shell (a0 = 2.855, rc = 5.6, skin = 0.7 for iron).  Only per-shell and
-// per-lattice scalars are runtime values.
-#define MX_SHELLS 7
+// (7 shells, 88 vectors: cutoff + skin between the 7th and 8th shell, e.g. a0 = 2.855,
+// rc = 5.6, skin = 0.7 for iron) or up to |h|^2 = 20 (8 shells, 112 vectors: between the
+// 8th and 9th shell, e.g. skin 1.3).  Only per-shell and per-lattice scalars are runtime
+// values.
+#define MX_SHELLS 8
 struct MxGrid {
   float rds, mmax;     // 1 / ds, last interval
   float fr[MX_SHELLS]; // frac(R^2 / ds)
@@ -164,7 +165,7 @@ struct MxStencil {
   float rds, rds_f; // 1 / ds of the density / force grid
   MxEntry odd[MX_PAR_MAX], even[MX_PAR_MAX], far[ENS_MAX_ST];
   MxWalk walk;
-  int fixed;   // 1: the built-in shell stencil applies (see MxShells)
+  int fixed;   // 7 or 8: the built-in shell stencil of that many shells applies (see MxShells); 0: runtime
   MxShells sh;
 };
 

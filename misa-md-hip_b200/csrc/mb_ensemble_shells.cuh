@@ -19,14 +19,14 @@ struct HVec {
   int hx, hy, hz, n2;
 };
 struct BccShells {
-  HVec v[88];
+  HVec v[112];
   int start[MX_SHELLS + 1];
   int n2[MX_SHELLS];
 };
 
 constexpr BccShells make_bcc_shells() {
   BccShells t{};
-  const int n2s[MX_SHELLS] = {3, 4, 8, 11, 12, 16, 19};
+  const int n2s[MX_SHELLS] = {3, 4, 8, 11, 12, 16, 19, 20};
   int n = 0;
   for (int s = 0; s < MX_SHELLS; s++) {
     t.start[s] = n;
@@ -42,7 +42,7 @@ constexpr BccShells make_bcc_shells() {
   return t;
 }
 constexpr BccShells kBcc = make_bcc_shells();
-static_assert(kBcc.start[MX_SHELLS] == 88, "BCC shells 1-7 hold 88 vectors");
+static_assert(kBcc.start[7] == 88 && kBcc.start[8] == 112, "BCC shells 1-7 hold 88 vectors, 1-8 112");
 
 constexpr int shell_of(int k) {
   int s = 0;

@@ -197,7 +197,7 @@ __device__ __forceinline__ void mx_unpack(unsigned p, int &s, int &cx, int &y, i
   s = (int)(p >> 31);
 }
 
-template <bool ENERGY, bool FIXED>
+template <bool ENERGY, int FIXED>
 __device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStencil &S, const LatDesc &d,
                                               const float2 *s_f, float ma0, long long i, unsigned pos) {
   const int s = (int)(pos >> 31);
@@ -210,12 +210,12 @@ __device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStenci
   if constexpr (FIXED) {
     const MxShells &Q = S.sh;
     const MxSite b = mx_site_bases(d, u4, i, s);
-    constexpr int nbf = 64; // shells 1-6, walked without a branch; shell 7 with one
+    constexpr int nbf = 64; // shells 1-6, walked without a branch; shells 7 (and 8) with one
     static_for<0, nbf / 2>([&](auto pc) {
       constexpr int k = 2 * decltype(pc)::value;
       two_sum(rs, rc, mxc_rho<k>(Q, ma0, b, u, s_f) + mxc_rho<k + 1>(Q, ma0, b, u, s_f));
     });
-    static_for<nbf, 88>([&](auto kc) {
+    static_for<nbf, kBcc.start[FIXED]>([&](auto kc) {
       constexpr int k = decltype(kc)::value;
       const float4 nb = mxc_load<k>(b);
       float2 exy;
@@ -267,7 +267,7 @@ __device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStenci
 
 // Force + velocity-Verlet of one site; adds pair energy and kinetic energy.  Pair terms
 // are added two at a time before one compensated add.
-template <bool ENERGY, bool FIXED>
+template <bool ENERGY, int FIXED>
 __device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStencil &S, const LatDesc &d,
                                               const float2 *s_ab, float ma0, long long i, unsigned pos,
                                               double &e_pair, double &e_kin) {
@@ -302,7 +302,7 @@ __device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStenci
       const float f1 = mxc_force<k + 1, ENERGY>(Q, ma0, b, u, s_ab, ptab, d1, z1, e1);
       add2(d0, z0, f0, e0, d1, z1, f1, e1);
     });
-    static_for<nbf, 88>([&](auto kc) {
+    static_for<nbf, kBcc.start[FIXED]>([&](auto kc) {
       constexpr int k = decltype(kc)::value;
       const float4 nb = mxc_load<k>(b);
       float2 exy;
@@ -383,7 +383,7 @@ __device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStenci
 
 // Density pass.  FIXED: the built-in BCC shells (MxShells), else the runtime stencil
 // (brick walk only).  Energy steps leave one {F(rho), 0} partial per walk item.
-template <bool ENERGY, bool FIXED, int WALK>
+template <bool ENERGY, int FIXED, int WALK>
 __global__ void __launch_bounds__(MX_RHO_THREADS, 1)
     k_mx_rho(const __grid_constant__ EnsParams P, const MxStencil S, int lat) {
   extern __shared__ float2 s_f[];
@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(MX_RHO_THREADS, 1)
 
 // Force + velocity-Verlet pass; energy steps add the pair energy to the item's partial
 // and store its kinetic energy.
-template <bool ENERGY, bool FIXED, int WALK>
+template <bool ENERGY, int FIXED, int WALK>
 __global__ void __launch_bounds__(MX_FORCE_THREADS, 1)
     k_mx_force(const __grid_constant__ EnsParams P, const MxStencil S, int lat) {
   extern __shared__ float2 s_ab[];
@@ -674,7 +674,7 @@ __global__ void k_mx_bookkeeping(const __grid_constant__ EnsParams P) {
   }
 }
 
-template <bool FIXED, int WALK>
+template <int FIXED, int WALK>
 static int mx_set_attrs() {
   MB_CUDA(cudaFuncSetAttribute(k_mx_rho<false, FIXED, WALK>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
   MB_CUDA(cudaFuncSetAttribute(k_mx_rho<true, FIXED, WALK>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM_MAX));
@@ -684,7 +684,7 @@ static int mx_set_attrs() {
   return MB_OK;
 }
 
-template <bool FIXED, int WALK>
+template <int FIXED, int WALK>
 static void mx_pass(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s, int which,
                     size_t smem) {
   const int sms = device_sm_count();
@@ -704,11 +704,13 @@ static void mx_pass(const EnsParams &P, const MxStencil &S, int lat, int energy,
 static void mx_passes(const EnsParams &P, const MxStencil &S, int lat, int energy, cudaStream_t s, int which,
                       size_t smem) {
   if (S.walk.linear)
-    mx_pass<true, 1>(P, S, lat, energy, s, which, smem);
+    S.fixed == 8 ? mx_pass<8, 1>(P, S, lat, energy, s, which, smem) : mx_pass<7, 1>(P, S, lat, energy, s, which, smem);
+  else if (S.fixed == 8)
+    mx_pass<8, 0>(P, S, lat, energy, s, which, smem);
   else if (S.fixed)
-    mx_pass<true, 0>(P, S, lat, energy, s, which, smem);
+    mx_pass<7, 0>(P, S, lat, energy, s, which, smem);
   else
-    mx_pass<false, 0>(P, S, lat, energy, s, which, smem);
+    mx_pass<0, 0>(P, S, lat, energy, s, which, smem);
 }
 
 // Per-lattice energies of an energy step: block l sums the partials of lattice l's items
@@ -743,9 +745,11 @@ int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, 
   if (S.walk.linear && !S.fixed) return fail(MB_ERR_STATE, "linear walk needs the built-in shells");
   static bool attr = false;
   if (!attr) {
-    MB_TRY((mx_set_attrs<false, 0>()));
-    MB_TRY((mx_set_attrs<true, 0>()));
-    MB_TRY((mx_set_attrs<true, 1>()));
+    MB_TRY((mx_set_attrs<0, 0>()));
+    MB_TRY((mx_set_attrs<7, 0>()));
+    MB_TRY((mx_set_attrs<7, 1>()));
+    MB_TRY((mx_set_attrs<8, 0>()));
+    MB_TRY((mx_set_attrs<8, 1>()));
     attr = true;
   }
   const int itl_grid = 2 * sms;

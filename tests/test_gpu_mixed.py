@@ -77,6 +77,25 @@ def test_split_brick_walk_forces_within_1e6_of_fp64_oracle():
     assert rms_rel(bg["rho"][live], bo["rho"][live]) < 1e-6
 
 
+@pytest.mark.parametrize("cells", [(32, 9, 10), (9, 8, 10)])
+def test_eight_shell_stencil_forces_within_1e6_of_fp64_oracle(cells):
+    # skin 1.3 A: the built-in stencil of BCC shells 1-8 (112 vectors), brick and linear walks
+    sc = make(cells=cells, temperature=900.0, vacancy=0.01, n_itl=2, seed=77, jitter=0.15)
+    sc.skin = 1.3
+    sc.ghost = mb.lattice.ghost_for_reach(A0, sc.cutoff + sc.skin)
+    bo, io, pe = _oracle_forces(sc, itl=sc.itl)
+    with _ens(sc) as ens:
+        ens.set_mode(2)
+        slot = ens.add(sc.cells, sc.box, sc.itl, steps=0)
+        ens.run(0)
+        bg, ig = ens.download(slot)
+    live = bo["type"] >= 0
+    fo = np.concatenate([bo["f"][live], io["f"]])
+    fg = np.concatenate([bg["f"][live], ig["f"]])
+    assert rms_rel(fg, fo) < F_RMS_TOL
+    assert rms_rel(bg["rho"][live], bo["rho"][live]) < 1e-6
+
+
 def test_split_kernels_track_persistent_kernel():
     sc = make(cells=(10, 9, 8), temperature=900.0, vacancy=0.005, n_itl=2, seed=74)
     out = {}
