@@ -192,6 +192,8 @@ struct mb_ensemble {
   unsigned *d_item_first = nullptr; // linear walk: first item of each lattice
   double *d_epart_items = nullptr;  // split: energy partials per walk item
   size_t cap_items = 0;
+  int *d_icell = nullptr; // interstitial cell lists of every lattice (rebuilt each step)
+  size_t cap_icell = 0;
   mb::MxStencil mxs{};
   size_t device_bytes = 0;
   size_t fixed_bytes = 0;
@@ -407,6 +409,57 @@ static int rebuild(mb_ensemble *e) {
   for (int c = 0; c < nl; c++) { // descriptors point into d_eitl
     e->slots[e->order[c]].d.e_itl = e->d_eitl + 2 * c;
     descs[c].e_itl = e->d_eitl + 2 * c;
+  }
+  // interstitial cell lists: cells of edge >= cutoff + skin, at least 3 per dimension
+  // (27 distinct neighbour cells); lattices below that walk the whole list
+  {
+    const double reach = e->cfg.cutoff + e->cfg.stencil_skin;
+    std::vector<size_t> off(nl, 0);
+    size_t total = 0;
+    for (int q : itl_lats) {
+      LatDesc &d = e->slots[e->order[q]].d;
+      const int n3[3] = {(int)(d.Lx / reach), (int)(d.Ly / reach), (int)(d.Lz / reach)};
+      if (n3[0] < 3 || n3[1] < 3 || n3[2] < 3 || d.cap_itl < 1) continue;
+      off[q] = total + 1; // 1-based: 0 = none
+      total += 2 * (size_t)n3[0] * n3[1] * n3[2] + 2 * (size_t)d.cap_itl + 2;
+    }
+    if (total > e->cap_icell) {
+      if (e->d_icell) {
+        cudaFree(e->d_icell);
+        e->device_bytes -= e->cap_icell * sizeof(int);
+        e->fixed_bytes -= e->cap_icell * sizeof(int);
+      }
+      e->d_icell = nullptr;
+      const size_t C = std::max(total, 2 * e->cap_icell);
+      MB_TRY(edalloc(e, (void **)&e->d_icell, C * sizeof(int)));
+      e->cap_icell = C;
+    }
+    if (total) MB_CUDA(cudaMemsetAsync(e->d_icell, 0, total * sizeof(int), e->stream));
+    for (int c = 0; c < nl; c++) {
+      LatDesc &d = e->slots[e->order[c]].d;
+      d.icn[0] = d.icn[1] = d.icn[2] = 0;
+      d.icount = d.istart = d.iitem = d.icell_of = d.iflag = nullptr;
+      if (off[c]) {
+        int *b = e->d_icell + (off[c] - 1);
+        d.icn[0] = (int)(d.Lx / reach);
+        d.icn[1] = (int)(d.Ly / reach);
+        d.icn[2] = (int)(d.Lz / reach);
+        const size_t nc = (size_t)d.icn[0] * d.icn[1] * d.icn[2];
+        d.icount = b;
+        d.istart = b + nc;
+        d.iitem = b + 2 * nc;
+        d.icell_of = b + 2 * nc + d.cap_itl;
+        d.iflag = b + 2 * nc + 2 * (size_t)d.cap_itl;
+      }
+      descs[c].icn[0] = d.icn[0];
+      descs[c].icn[1] = d.icn[1];
+      descs[c].icn[2] = d.icn[2];
+      descs[c].icount = d.icount;
+      descs[c].istart = d.istart;
+      descs[c].iitem = d.iitem;
+      descs[c].icell_of = d.icell_of;
+      descs[c].iflag = d.iflag;
+    }
   }
   if (need_t > e->cap_tiles) {
     const size_t C = std::max<size_t>({need_t, 2 * e->cap_tiles, 256});
@@ -829,7 +882,7 @@ int mb_ensemble_destroy(mb_ensemble *e) {
   for (auto &L : e->slots) free_slot(e, L);
   void *ptrs[] = {e->d_lats, e->d_tile_lat, e->d_tile_idx, e->d_tile_first, e->d_itl_lats, e->d_tmaps,
                   e->d_epart, e->d_eout, e->d_eitl, e->d_bar, e->d_err, e->d_bad, e->d_item_first,
-                  e->d_epart_items};
+                  e->d_epart_items, e->d_icell};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &ev : e->ev)

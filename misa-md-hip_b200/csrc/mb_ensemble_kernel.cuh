@@ -68,7 +68,15 @@ struct LatDesc {
   long long *cand;       // [MB_CAND_CAP] box index of sites whose atom left them this step
   int *cand_n;
   long long *conv_counters; // [4] conversions, recombinations, refused, dropped
+  // interstitial cell list (rebuilt at the start of every step): the box cut into
+  // icn[0] x icn[1] x icn[2] cells of edge >= cutoff + skin (0: lattice too small, every
+  // item walks the whole list); icount / istart per cell, iitem the list indices sorted by
+  // (cell, index), icell_of the cell of each entry at the last build, iflag[0] = 1 when
+  // the list is valid this step, iflag[1] = entries of the last build
+  int icn[3];
+  int *icount, *istart, *iitem, *icell_of, *iflag;
 };
+#define MX_ICELL_MAX 4096 // interstitials a cell list is built for (sorted in shared memory)
 
 struct EnsParams {
   int n_st;                            // stencil entries, ordered by ideal distance

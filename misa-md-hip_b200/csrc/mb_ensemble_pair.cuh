@@ -156,12 +156,51 @@ __device__ __forceinline__ void itl_mark_one(const EnsParams &P, const LatDesc &
   }
 }
 
+// Coarse cell of a point of lattice d (wrapped into the box).
+__device__ __forceinline__ void itl_cell3(const LatDesc &d, double x, double y, double z, int &cx, int &cy, int &cz) {
+  const double fx = x / d.Lx - floor(x / d.Lx), fy = y / d.Ly - floor(y / d.Ly), fz = z / d.Lz - floor(z / d.Lz);
+  cx = max(0, min((int)(fx * d.icn[0]), d.icn[0] - 1));
+  cy = max(0, min((int)(fy * d.icn[1]), d.icn[1] - 1));
+  cz = max(0, min((int)(fz * d.icn[2]), d.icn[2] - 1));
+}
+
+// Interstitial-pair part of an item: every interstitial within the 27 cells around the
+// query point (the cells are at least cutoff + skin wide, so nothing in reach is left
+// out), lane c walking cell c in list order; or the whole list when there is no cell
+// list this step.  Each lane sums its own pairs in a fixed order.
+template <bool CELLS, class Pair>
+__device__ __forceinline__ void itl_pairs(const LatDesc &d, const Geom &g, int cur, double xi, double yi, double zi,
+                                          int skip, int lane, Pair pair, bool with_df) {
+  if (CELLS && d.icount && d.iflag[0]) {
+    if (lane >= 27) return;
+    int qx, qy, qz;
+    itl_cell3(d, xi, yi, zi, qx, qy, qz);
+    const int ox = lane % 3 - 1, oy = (lane / 3) % 3 - 1, oz = lane / 9 - 1;
+    const int cx = (qx + ox + d.icn[0]) % d.icn[0], cy = (qy + oy + d.icn[1]) % d.icn[1],
+              cz = (qz + oz + d.icn[2]) % d.icn[2];
+    const int c = (cz * d.icn[1] + cy) * d.icn[0] + cx;
+    const int n = d.icount[c], s0 = d.istart[c];
+    for (int j = s0; j < s0 + n; j++) {
+      const int K = d.iitem[j];
+      if (K == skip) continue;
+      pair(min_image(xi - d.ipx[cur][K], g.Lx, g.iLx), min_image(yi - d.ipy[cur][K], g.Ly, g.iLy),
+           min_image(zi - d.ipz[cur][K], g.Lz, g.iLz), d.itype[K], with_df ? d.idf[K] : 0.0);
+    }
+    return;
+  }
+  for (int K = lane; K < d.n_itl; K += 32) {
+    if (K == skip) continue;
+    pair(min_image(xi - d.ipx[cur][K], g.Lx, g.iLx), min_image(yi - d.ipy[cur][K], g.Ly, g.iLy),
+         min_image(zi - d.ipz[cur][K], g.Lz, g.iLz), d.itype[K], with_df ? d.idf[K] : 0.0);
+  }
+}
+
 // Work of one warp on item w of lattice d: a flagged site (w < nflag) or an
 // interstitial.  FORCE = false: density pass; true: force + integration pass.  A
 // flagged site's lattice-pair part comes from the lattice kernels (rho / f of the site);
 // its interstitial pairs, df, integration and ghost images are done here.  An
 // interstitial's pairs (lattice window and other interstitials) are all done here, FP64.
-template <bool FORCE, bool ENERGY>
+template <bool FORCE, bool ENERGY, bool CELLS>
 __device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag) {
   const int lane = threadIdx.x & 31;
   const Geom g = lat_geom(d);
@@ -232,11 +271,7 @@ __device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag)
       pair(-(ox + (double)uj.x), -(oy + (double)uj.y), -(oz + (double)uj.z), cj & 0x3F, FORCE ? (double)uj.w : 0.0);
     }
   }
-  for (int K = lane; K < d.n_itl; K += 32) {
-    if (!is_site && K == it) continue;
-    pair(min_image(xi - d.ipx[cur][K], g.Lx, g.iLx), min_image(yi - d.ipy[cur][K], g.Ly, g.iLy), min_image(zi - d.ipz[cur][K], g.Lz, g.iLz),
-         d.itype[K], FORCE ? d.idf[K] : 0.0);
-  }
+  itl_pairs<CELLS>(d, g, cur, xi, yi, zi, is_site ? -1 : it, lane, pair, FORCE);
   if (!FORCE) {
     acc0 = warp_sum(acc0);
     if (lane == 0) {
@@ -311,7 +346,9 @@ __device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag)
   }
 }
 
-template <bool FORCE, bool ENERGY>
+// CELLS: the split kernels' per-step interstitial cell list applies (the persistent
+// kernel walks whole lists).
+template <bool FORCE, bool ENERGY, bool CELLS = false>
 __device__ void itl_items(const EnsParams &P) {
   const int warps = gridDim.x * (blockDim.x >> 5);
   const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -320,7 +357,7 @@ __device__ void itl_items(const EnsParams &P) {
     if (!lat_active(d)) continue;
     const int nflag = min(d.flag_count[d.cur], d.cap_flag);
     const int n = nflag + d.n_itl;
-    for (int w = gw; w < n; w += warps) itl_item<FORCE, ENERGY>(P, d, w, nflag);
+    for (int w = gw; w < n; w += warps) itl_item<FORCE, ENERGY, CELLS>(P, d, w, nflag);
   }
 }
 

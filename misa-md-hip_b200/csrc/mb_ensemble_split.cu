@@ -454,6 +454,57 @@ __global__ void k_mx_itl_clear(const __grid_constant__ EnsParams P) {
   }
 }
 
+// Interstitial cell list of one lattice per CTA, from this step's positions: the counts
+// of the previous build are cleared, (cell, index) keys sorted in shared memory, and each
+// occupied cell gets its start and count.  The order (cell, index) does not depend on
+// thread timing.
+#define MX_BIN_THREADS 1024
+__global__ void __launch_bounds__(MX_BIN_THREADS, 1) k_mx_itl_bin(const __grid_constant__ EnsParams P) {
+  __shared__ long long key[MX_ICELL_MAX];
+  const LatDesc &d = P.lats[P.itl_lats[blockIdx.x]];
+  if (!lat_active(d) || !d.icount) return; // uniform per block
+  const int tid = threadIdx.x, n = d.n_itl, cur = d.cur;
+  const int nold = d.iflag[1];
+  for (int k = tid; k < nold; k += blockDim.x) d.icount[d.icell_of[k]] = 0;
+  __syncthreads();
+  if (n > MX_ICELL_MAX) { // too many for the shared-memory sort: items walk the whole list
+    if (tid == 0) {
+      d.iflag[0] = 0;
+      d.iflag[1] = 0;
+    }
+    return;
+  }
+  int n2 = 1;
+  while (n2 < n) n2 <<= 1;
+  for (int k = tid; k < n2; k += blockDim.x) {
+    if (k < n) {
+      int cx, cy, cz;
+      itl_cell3(d, d.ipx[cur][k], d.ipy[cur][k], d.ipz[cur][k], cx, cy, cz);
+      const int c = (cz * d.icn[1] + cy) * d.icn[0] + cx;
+      d.icell_of[k] = c;
+      key[k] = ((long long)c << 17) | (long long)k;
+    } else {
+      key[k] = LLONG_MAX;
+    }
+  }
+  __syncthreads();
+  if (n > 1) bitonic_sort(key, n2);
+  for (int r = tid; r < n; r += blockDim.x) {
+    const int c = (int)(key[r] >> 17);
+    d.iitem[r] = (int)(key[r] & 0x1FFFF);
+    if (r == 0 || (int)(key[r - 1] >> 17) != c) {
+      int e = r + 1;
+      while (e < n && (int)(key[e] >> 17) == c) e++;
+      d.istart[c] = r;
+      d.icount[c] = e - r;
+    }
+  }
+  if (tid == 0) {
+    d.iflag[0] = 1;
+    d.iflag[1] = n;
+  }
+}
+
 __global__ void k_mx_itl_mark(const __grid_constant__ EnsParams P) {
   const int warps = gridDim.x * (blockDim.x >> 5);
   const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -466,7 +517,7 @@ __global__ void k_mx_itl_mark(const __grid_constant__ EnsParams P) {
 
 template <bool FORCE, bool ENERGY>
 __global__ void k_mx_itl_items(const __grid_constant__ EnsParams P) {
-  itl_items<FORCE, ENERGY>(P);
+  itl_items<FORCE, ENERGY, true>(P);
 }
 
 // Lattice <-> interstitial bookkeeping after the drift, one CTA per lattice that can
@@ -755,6 +806,7 @@ int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, 
   const int itl_grid = 2 * sms;
   if (P.n_itl_lats > 0) {
     k_mx_itl_clear<<<itl_grid, 256, 0, s>>>(P);
+    k_mx_itl_bin<<<P.n_itl_lats, MX_BIN_THREADS, 0, s>>>(P);
     k_mx_itl_mark<<<itl_grid, 256, 0, s>>>(P);
   }
   if (ev) MB_CUDA(cudaEventRecord(ev[0], s));
