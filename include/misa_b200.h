@@ -202,8 +202,19 @@ int mb_sim_energies(mb_sim *sim, double *out_step_pe_ke, int32_t cap, int32_t *n
 int mb_sim_time_steps(mb_sim *sim, int32_t nsteps, float *ms);
 /* One full step through host buffers: upload box_atoms (x, v, f, type),
  * one velocity-Verlet step on the device, write x, v, f, rho, df back.  The
- * e2e form of the hot path: host<->device copies are part of every call. */
+ * e2e form of the hot path: host<->device copies are part of every call.  The box is
+ * streamed in z-slabs (box_atoms in box order, z slowest): records of later slabs
+ * travel in while earlier ones are computed and earlier results travel out.  The
+ * records are bitwise the same whatever the slab count.  Replaces the reference's
+ * RhoDoubleBufferImp / ForceDoubleBufferImp streaming
+ * (src/double-buffer/double_buffer.cpp:12-47) for a whole step. */
 int mb_sim_step_host(mb_sim *sim, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t n_itl);
+/* Slabs of mb_sim_step_host: 0 automatic (16, fewer on thin boxes), 1 one piece, else
+ * at most that many (each slab at least as thick as the stencil and the interstitial
+ * windows reach; fewer than 4 such slabs run in one piece).  mb_sim_host_slabs
+ * reports the count a step takes. */
+int mb_sim_set_host_slabs(mb_sim *sim, int32_t n_slabs);
+int mb_sim_host_slabs(mb_sim *sim, int32_t *n_slabs);
 /* Mean device milliseconds of the rho and force launches over 4 extra steps the sim
  * takes (mixed precision: as mb_ensemble_kernel_times). */
 int mb_sim_kernel_times(mb_sim *sim, float *rho_ms, float *force_ms);

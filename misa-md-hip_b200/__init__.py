@@ -152,6 +152,16 @@ class Sim:
         n = 0 if itl is None else int(itl.shape[0])
         check(lib().mb_sim_step_host(self._h, ptr(box), ptr(itl) if n else None, n))
 
+    def set_host_slabs(self, n_slabs: int) -> None:
+        """z-slabs step_host streams the box in (0 automatic, 1 one piece)."""
+        check(lib().mb_sim_set_host_slabs(self._h, int(n_slabs)))
+
+    def host_slabs(self) -> int:
+        """Slabs the next step_host takes."""
+        n = C.c_int32(0)
+        check(lib().mb_sim_host_slabs(self._h, C.byref(n)))
+        return n.value
+
     def info(self) -> dict:
         a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
         check(lib().mb_sim_info(self._h, C.byref(a), C.byref(b), C.byref(c)))

@@ -104,6 +104,8 @@ SIGNATURES: dict[str, tuple] = {
     "mb_sim_energies": (_I, [_P, _PD, C.c_int32, C.POINTER(C.c_int32)]),
     "mb_sim_time_steps": (_I, [_P, C.c_int32, _PF]),
     "mb_sim_step_host": (_I, [_P, _P, _P, C.c_int32]),
+    "mb_sim_set_host_slabs": (_I, [_P, C.c_int32]),
+    "mb_sim_host_slabs": (_I, [_P, C.POINTER(C.c_int32)]),
     "mb_sim_kernel_times": (_I, [_P, _PF, _PF]),
     "mb_sim_info": (_I, [_P, _PI64, _PI64, _PI64]),
     "mb_sim_set_graphs": (_I, [_P, _I]),

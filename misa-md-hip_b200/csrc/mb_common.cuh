@@ -167,23 +167,31 @@ __host__ __device__ __forceinline__ void site_ideal(int s, int cx, int y, int z,
 }
 
 // kernels (mb_kernels64.cu)
+// [z0, z1): the box layers a launch covers (z1 < 0: up to the last layer).  The
+// interstitial passes then take the flagged sites in those layers and the
+// interstitials whose wrapped z lies in them.
 int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, double rc2,
-                 double *e_partial, int energy, int skip_flagged, cudaStream_t s);
+                 double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0 = 0, int z1 = -1);
 int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const StepParams &sp,
-                   double *e_partial, int energy, int skip_flagged, cudaStream_t s);
+                   double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0 = 0, int z1 = -1);
 int launch_itl_mark64(const Geom &g, const Lattice64 &L, const Itl64 &I, cudaStream_t s);
+// Flags the sites of layers [z0, z1) near an interstitial, without clearing or
+// resetting the list first.
+int launch_itl_mark_slab64(const Geom &g, const Lattice64 &L, const Itl64 &I, int z0, int z1, cudaStream_t s);
 int launch_itl_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const Itl64 &I,
-                     double rc2, double *e_partial, int energy, cudaStream_t s);
+                     double rc2, double *e_partial, int energy, cudaStream_t s, int z0 = 0, int z1 = -1);
 int launch_itl_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const Itl64 &I,
-                       const StepParams &sp, double *e_partial, int energy, cudaStream_t s);
-int launch_images64(const Geom &g, const Lattice64 &L, int what, cudaStream_t s); // what: 1 pos+code, 2 df
+                       const StepParams &sp, double *e_partial, int energy, cudaStream_t s, int z0 = 0, int z1 = -1);
+int launch_images64(const Geom &g, const Lattice64 &L, int what, cudaStream_t s, int z0 = 0,
+                    int z1 = -1); // what: 1 pos+code, 2 df
 // Lattice <-> interstitial bookkeeping after a drift (one CTA): candidates of
 // sp.cand become interstitials (box order), then interstitials within sqrt(rec2) of a
 // vacant site take it (list order, first claim wins).  counters: [0] conversions,
 // [1] recombinations, [2] refused conversions (list full), [3] dropped candidates.
 int launch_convert64(const Geom &g, const Lattice64 &L, const Itl64 &I, const StepParams &sp, double rec2,
                      int64_t *site_id, int *nd, long long *counters, cudaStream_t s);
-int launch_kick_drift64(const Geom &g, const Lattice64 &L, const Itl64 &I, const StepParams &sp, cudaStream_t s);
+int launch_kick_drift64(const Geom &g, const Lattice64 &L, const Itl64 &I, const StepParams &sp, cudaStream_t s,
+                        int z0 = 0, int z1 = -1, int with_itl = 1);
 int launch_reduce(const double *partials, int n, double *out, cudaStream_t s);
 int energy_partials_needed();
 
@@ -199,9 +207,10 @@ int launch_unpack_box(const Geom &g, const mb_atom_element *aos, Lattice64 L, in
 int launch_pack_box(const Geom &g, mb_atom_element *aos, const Lattice64 &L, const double *px, const double *py,
                     const double *pz, double h, int unkick, cudaStream_t s);
 int launch_unpack_box_ids(const Geom &g, const mb_atom_element *aos, Lattice64 L, int with_f, int *bad_type,
-                          int64_t *ids, int n_types, cudaStream_t s);
+                          int64_t *ids, int n_types, cudaStream_t s, int z0 = 0, int z1 = -1);
 int launch_pack_box_ids(const Geom &g, mb_atom_element *aos, const Lattice64 &L, const double *px, const double *py,
-                        const double *pz, double h, int unkick, const int64_t *ids, cudaStream_t s);
+                        const double *pz, double h, int unkick, const int64_t *ids, cudaStream_t s, int z0 = 0,
+                        int z1 = -1);
 int launch_df_from_rho(const Geom &g, const DevPot &pot, const Lattice64 &L, cudaStream_t s);
 
 // Half-neighbour hook passes (mb_half.cu): a decoded half-stencil offset.

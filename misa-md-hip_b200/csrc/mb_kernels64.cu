@@ -31,6 +31,14 @@ namespace mb {
 
 __device__ __forceinline__ int itl_n(const Itl64 &I) { return I.nd ? *I.nd : I.n; }
 
+// Box z layer of a point, wrapped into the periodic box (z-slab filters of the
+// host-buffer step).
+__device__ __forceinline__ int z_layer(const Geom &g, double a0, double z) {
+  const double w = g.iLz > 0.0 ? z - g.Lz * floor(z * g.iLz) : z;
+  const double c = floor(w / a0);
+  return c < 0.0 ? 0 : (c >= (double)(g.bz - 1) ? g.bz - 1 : (int)c);
+}
+
 // Lists the box site of a drifted lattice atom that left its site (conversion on).
 __device__ __forceinline__ void conv_check(const Geom &g, const StepParams &sp, int s, int cx, int y, int z, double nx,
                                            double ny, double nz) {
@@ -61,7 +69,7 @@ struct RhoArgs {
   int skip_flagged;
   int m_lo;      // first knot kept in shared memory
   int chunks;    // 32-site chunks per row
-  long long n_items;
+  long long w0, n_items; // items [w0, n_items): a z-slab of the box (z slowest)
 };
 
 // One density term of a one-type lattice.  BF (branch-free): the stencil entry lies
@@ -97,7 +105,8 @@ __global__ void __launch_bounds__(MB_RHO_THREADS, 1)
   const int lane = threadIdx.x & 31;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
   double e_acc = 0.0;
-  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.n_items; w += wstride) {
+  for (long long w = a.w0 + (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.n_items;
+       w += wstride) {
     long long t = w;
     const int chunk = (int)(t % a.chunks);
     t /= a.chunks;
@@ -164,7 +173,7 @@ struct ForceArgs {
   int skip_flagged;
   int m_lo;
   int chunks;
-  long long n_items;
+  long long w0, n_items; // items [w0, n_items)
 };
 
 // One force term of a one-type lattice (see rho_term for BF).
@@ -223,7 +232,8 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
   const int lane = threadIdx.x & 31;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
   double e_pair = 0.0, e_kin = 0.0;
-  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.n_items; w += wstride) {
+  for (long long w = a.w0 + (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.n_items;
+       w += wstride) {
     long long t = w;
     const int chunk = (int)(t % a.chunks);
     t /= a.chunks;
@@ -342,7 +352,7 @@ static int smem_knots(const DevPot &pot, int bytes_per_knot) {
 }
 
 int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, double rc2,
-                 double *e_partial, int energy, int skip_flagged, cudaStream_t s) {
+                 double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0, int z1) {
   RhoArgs a;
   a.g = g;
   a.P = pot;
@@ -355,9 +365,12 @@ int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const L
   if (!one) nsm = 0;
   a.m_lo = pot.nr - nsm;
   a.chunks = (g.bcx + 31) / 32;
-  a.n_items = (long long)a.chunks * g.by * 2 * g.bz;
+  if (z1 < 0) z1 = g.bz;
+  if (z0 < 0 || z0 >= z1 || z1 > g.bz) return z0 == z1 ? MB_OK : fail(MB_ERR_ARG, "z-slab outside the box");
+  a.w0 = (long long)a.chunks * g.by * 2 * z0;
+  a.n_items = (long long)a.chunks * g.by * 2 * z1;
   const size_t smem = (size_t)nsm * sizeof(double4);
-  const int grid = grid_for(a.n_items, MB_RHO_THREADS);
+  const int grid = grid_for(a.n_items - a.w0, MB_RHO_THREADS);
   static bool attr_done = false;
   if (!attr_done) {
     MB_CUDA(cudaFuncSetAttribute(k_rho64<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap));
@@ -380,7 +393,7 @@ int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const L
 }
 
 int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const StepParams &sp,
-                   double *e_partial, int energy, int skip_flagged, cudaStream_t s) {
+                   double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0, int z1) {
   ForceArgs a;
   a.g = g;
   a.P = pot;
@@ -394,9 +407,12 @@ int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const
   if (!one) nsm = 0;
   a.m_lo = pot.nr - nsm;
   a.chunks = (g.bcx + 31) / 32;
-  a.n_items = (long long)a.chunks * g.by * 2 * g.bz;
+  if (z1 < 0) z1 = g.bz;
+  if (z0 < 0 || z0 >= z1 || z1 > g.bz) return z0 == z1 ? MB_OK : fail(MB_ERR_ARG, "z-slab outside the box");
+  a.w0 = (long long)a.chunks * g.by * 2 * z0;
+  a.n_items = (long long)a.chunks * g.by * 2 * z1;
   const size_t smem = (size_t)nsm * 3 * sizeof(double2);
-  const int grid = grid_for(a.n_items, MB_FORCE_THREADS);
+  const int grid = grid_for(a.n_items - a.w0, MB_FORCE_THREADS);
   static bool attr_done = false;
   if (!attr_done) {
     MB_CUDA(cudaFuncSetAttribute(k_force64<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCap));
@@ -436,8 +452,9 @@ __global__ void k_itl_clear(const Lattice64 L, const Itl64 I) {
 }
 
 // ... then one warp per interstitial flags the sites within reach (the count was
-// reset in between).
-__global__ void k_itl_mark(const Geom g, const Lattice64 L, const Itl64 I) {
+// reset in between); only sites in box layers [z0, z1) when that is not the whole box.
+__global__ void k_itl_mark(const Geom g, const Lattice64 L, const Itl64 I, int z0, int z1) {
+  const bool all_z = z0 <= 0 && z1 >= g.bz;
   const int lane = threadIdx.x & 31;
   const int it = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
   if (it >= itl_n(I)) return;
@@ -448,6 +465,11 @@ __global__ void k_itl_mark(const Geom g, const Lattice64 L, const Itl64 I) {
     long long idx;
     double sx, sy, sz;
     if (!window_site(g, w, c, qx, qy, qz, I.a0, I.reach, idx, sx, sy, sz)) continue;
+    if (!all_z) {
+      int ss, scx, sy_, sz_;
+      decode_ext(g, idx, ss, scx, sy_, sz_);
+      if (sz_ < z0 || sz_ >= z1) continue;
+    }
     if (L.code[idx] < 0) continue;
     const uintptr_t addr = (uintptr_t)(L.code + idx);
     unsigned int *word = (unsigned int *)(addr & ~(uintptr_t)3);
@@ -466,8 +488,9 @@ __global__ void k_itl_mark(const Geom g, const Lattice64 L, const Itl64 I) {
 template <bool ENERGY>
 __global__ void __launch_bounds__(MB_ITL_THREADS)
     k_itl_rho64(const __grid_constant__ StencilSet st, const Geom g, const DevPot P, const Lattice64 L, const Itl64 I,
-                double rc2, double *e_partial) {
+                double rc2, double *e_partial, int z0, int z1) {
   const int lane = threadIdx.x & 31;
+  const bool all_z = z0 <= 0 && z1 >= g.bz; // else only items in box layers [z0, z1)
   const int nflag = min(I.flag_count[0], I.cap_flag);
   const int n_itl = itl_n(I);
   const long long n_items = (long long)nflag + n_itl;
@@ -478,6 +501,7 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
       const long long i = I.flag_list[w];
       int s, cx, y, z;
       decode_ext(g, i, s, cx, y, z);
+      if (!all_z && (z < z0 || z >= z1)) continue;
       const int ti = L.code[i] & 0x3F;
       const double xi = L.px[i], yi = L.py[i], zi = L.pz[i];
       double rho = 0.0;
@@ -504,6 +528,10 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
     } else {
       const int it = (int)(w - nflag);
       const double qx = I.px[it], qy = I.py[it], qz = I.pz[it];
+      if (!all_z) {
+        const int lz = z_layer(g, I.a0, qz);
+        if (lz < z0 || lz >= z1) continue;
+      }
       const Window win = make_window(qx, qy, qz, I.a0, I.reach);
       const int ncand = win.nx * win.ny * win.nz;
       double rho = 0.0;
@@ -542,8 +570,9 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
 template <bool ENERGY>
 __global__ void __launch_bounds__(MB_ITL_THREADS)
     k_itl_force64(const __grid_constant__ StencilSet st, const Geom g, const DevPot P, const Lattice64 L,
-                  const Itl64 I, const StepParams sp, double *e_pair, double *e_kin) {
+                  const Itl64 I, const StepParams sp, double *e_pair, double *e_kin, int z0, int z1) {
   const int lane = threadIdx.x & 31;
+  const bool all_z = z0 <= 0 && z1 >= g.bz; // else only items in box layers [z0, z1)
   const int nflag = min(I.flag_count[0], I.cap_flag);
   const int n_itl = itl_n(I);
   const long long n_items = (long long)nflag + n_itl;
@@ -569,6 +598,10 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
       yi = I.py[it];
       zi = I.pz[it];
       dfi = I.df[it];
+    }
+    if (!all_z) {
+      const int lz = is_site ? z : z_layer(g, I.a0, zi);
+      if (lz < z0 || lz >= z1) continue;
     }
     double fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
     auto add_pair = [&](double dx, double dy, double dz, int tj, double dfj) {
@@ -678,7 +711,14 @@ int launch_itl_mark64(const Geom &g, const Lattice64 &L, const Itl64 &I, cudaStr
   MB_CUDA(cudaGetLastError());
   MB_CUDA(cudaMemsetAsync(I.flag_count, 0, sizeof(int), s));
   const int nmax = I.nd ? I.cap : I.n;
-  if (nmax > 0) k_itl_mark<<<(nmax * 32 + 255) / 256, 256, 0, s>>>(g, L, I);
+  if (nmax > 0) k_itl_mark<<<(nmax * 32 + 255) / 256, 256, 0, s>>>(g, L, I, 0, g.bz);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+int launch_itl_mark_slab64(const Geom &g, const Lattice64 &L, const Itl64 &I, int z0, int z1, cudaStream_t s) {
+  const int nmax = I.nd ? I.cap : I.n;
+  if (nmax > 0 && z0 < z1) k_itl_mark<<<(nmax * 32 + 255) / 256, 256, 0, s>>>(g, L, I, z0, z1);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
@@ -693,26 +733,28 @@ static int itl_grid(const Itl64 &I) {
 }
 
 int launch_itl_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const Itl64 &I,
-                     double rc2, double *e_partial, int energy, cudaStream_t s) {
+                     double rc2, double *e_partial, int energy, cudaStream_t s, int z0, int z1) {
   if (!I.nd && I.n == 0) return MB_OK;
+  if (z1 < 0) z1 = g.bz;
   const int grid = itl_grid(I);
   if (energy)
-    k_itl_rho64<true><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, rc2, e_partial + 3 * MB_EPART_CAP);
+    k_itl_rho64<true><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, rc2, e_partial + 3 * MB_EPART_CAP, z0, z1);
   else
-    k_itl_rho64<false><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, rc2, nullptr);
+    k_itl_rho64<false><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, rc2, nullptr, z0, z1);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
 
 int launch_itl_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const Itl64 &I,
-                       const StepParams &sp, double *e_partial, int energy, cudaStream_t s) {
+                       const StepParams &sp, double *e_partial, int energy, cudaStream_t s, int z0, int z1) {
   if (!I.nd && I.n == 0) return MB_OK;
+  if (z1 < 0) z1 = g.bz;
   const int grid = itl_grid(I);
   if (energy)
     k_itl_force64<true><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, sp, e_partial + 4 * MB_EPART_CAP,
-                                                         e_partial + 5 * MB_EPART_CAP);
+                                                         e_partial + 5 * MB_EPART_CAP, z0, z1);
   else
-    k_itl_force64<false><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, sp, nullptr, nullptr);
+    k_itl_force64<false><<<grid, MB_ITL_THREADS, 0, s>>>(st, g, pot, L, I, sp, nullptr, nullptr, z0, z1);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
@@ -933,9 +975,11 @@ int launch_convert64(const Geom &g, const Lattice64 &L, const Itl64 &I, const St
 }
 
 // ------------------------------------------------ images / kick-drift
-__global__ void k_images64(const Geom g, const Lattice64 L, int what) {
-  const long long n = 2LL * g.bcx * g.by * g.bz;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+// Sites are numbered cx fastest, then y, sublattice, z: box layers [z0, z1) are the
+// numbers [t0, t1) = [z0, z1) * 2 * by * bcx.
+__global__ void k_images64(const Geom g, const Lattice64 L, int what, long long t0, long long t1) {
+  for (long long t = t0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; t < t1;
+       t += (long long)gridDim.x * blockDim.x) {
     const int cx = (int)(t % g.bcx);
     long long r = t / g.bcx;
     const int y = (int)(r % g.by);
@@ -960,24 +1004,31 @@ __global__ void k_images64(const Geom g, const Lattice64 L, int what) {
   }
 }
 
-int launch_images64(const Geom &g, const Lattice64 &L, int what, cudaStream_t s) {
-  const long long n = 2LL * g.bcx * g.by * g.bz;
+int launch_images64(const Geom &g, const Lattice64 &L, int what, cudaStream_t s, int z0, int z1) {
+  if (z1 < 0) z1 = g.bz;
+  const long long layer = 2LL * g.bcx * g.by;
+  const long long n = layer * (z1 - z0);
+  if (n <= 0) return MB_OK;
   int grid = (int)((n + 255) / 256);
   if (grid > 8 * device_sm_count()) grid = 8 * device_sm_count();
-  k_images64<<<grid, 256, 0, s>>>(g, L, what);
+  k_images64<<<grid, 256, 0, s>>>(g, L, what, layer * z0, layer * z1);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
 
 // First half of a velocity-Verlet step in place (used when the state arrives
 // from the host each step): v += h f ; x += dt v, then refresh ghost images.
-__global__ void k_kick_drift64(const Geom g, const Lattice64 L, const Itl64 I, const StepParams sp) {
-  const long long n = 2LL * g.bcx * g.by * g.bz;
-  const int n_itl = itl_n(I);
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n + n_itl;
-       t += (long long)gridDim.x * blockDim.x) {
-    if (t >= n) {
-      const int it = (int)(t - n);
+// Lattice sites [t0, t1) (numbered as in k_images64), then the interstitials when
+// with_itl is set.
+__global__ void k_kick_drift64(const Geom g, const Lattice64 L, const Itl64 I, const StepParams sp, long long t0,
+                               long long t1, int with_itl) {
+  const long long n = t1 - t0;
+  const int n_itl = with_itl ? itl_n(I) : 0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n + n_itl;
+       q += (long long)gridDim.x * blockDim.x) {
+    const long long t = t0 + q;
+    if (q >= n) {
+      const int it = (int)(q - n);
       I.vx[it] += sp.h * I.fx[it];
       I.vy[it] += sp.h * I.fy[it];
       I.vz[it] += sp.h * I.fz[it];
@@ -1010,11 +1061,15 @@ __global__ void k_kick_drift64(const Geom g, const Lattice64 L, const Itl64 I, c
   }
 }
 
-int launch_kick_drift64(const Geom &g, const Lattice64 &L, const Itl64 &I, const StepParams &sp, cudaStream_t s) {
-  const long long n = 2LL * g.bcx * g.by * g.bz + (I.nd ? I.cap : I.n);
+int launch_kick_drift64(const Geom &g, const Lattice64 &L, const Itl64 &I, const StepParams &sp, cudaStream_t s,
+                        int z0, int z1, int with_itl) {
+  if (z1 < 0) z1 = g.bz;
+  const long long layer = 2LL * g.bcx * g.by;
+  const long long n = layer * (z1 - z0) + (with_itl ? (I.nd ? I.cap : I.n) : 0);
+  if (n <= 0) return MB_OK;
   int grid = (int)((n + 255) / 256);
   if (grid > 8 * device_sm_count()) grid = 8 * device_sm_count();
-  k_kick_drift64<<<grid, 256, 0, s>>>(g, L, I, sp);
+  k_kick_drift64<<<grid, 256, 0, s>>>(g, L, I, sp, layer * z0, layer * z1, with_itl);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }

@@ -61,11 +61,13 @@ __global__ void k_pack_ext(const Geom g, mb_atom_element *aos, int ext_x, int ex
   }
 }
 
+// Box-order records (doubled x fastest, then y, z): records [t0, t1) are box layers
+// [t0, t1) / (2 * bcx * by).
 __global__ void k_unpack_box(const Geom g, const mb_atom_element *aos, Lattice64 L, int with_f, int *bad_type,
-                             int64_t *ids, int n_types) {
-  const long long n = 2LL * g.bcx * g.by * g.bz;
+                             int64_t *ids, int n_types, long long t0, long long t1) {
   const int bxd = 2 * g.bcx;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = t0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; t < t1;
+       t += (long long)gridDim.x * blockDim.x) {
     const int bx = (int)(t % bxd);
     const long long r = t / bxd;
     const int by = (int)(r % g.by), bz = (int)(r / g.by);
@@ -97,10 +99,11 @@ __global__ void k_unpack_box(const Geom g, const mb_atom_element *aos, Lattice64
 // Box-order records of the synchronised state.  px/py/pz: positions of the
 // step; unkick: v is stored half a step ahead and is brought back by h*f.
 __global__ void k_pack_box(const Geom g, mb_atom_element *aos, const Lattice64 L, const double *px,
-                           const double *py, const double *pz, double h, int unkick, const int64_t *ids) {
-  const long long n = 2LL * g.bcx * g.by * g.bz;
+                           const double *py, const double *pz, double h, int unkick, const int64_t *ids, long long t0,
+                           long long t1) {
   const int bxd = 2 * g.bcx;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = t0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; t < t1;
+       t += (long long)gridDim.x * blockDim.x) {
     const int bx = (int)(t % bxd);
     const long long r = t / bxd;
     const int by = (int)(r % g.by), bz = (int)(r / g.by);
@@ -186,8 +189,12 @@ int launch_pack_ext(const Geom &g, mb_atom_element *aos, int ext_x, int ext_y, c
 }
 
 int launch_unpack_box_ids(const Geom &g, const mb_atom_element *aos, Lattice64 L, int with_f, int *bad_type,
-                          int64_t *ids, int n_types, cudaStream_t s) {
-  k_unpack_box<<<flat_grid(2LL * g.bcx * g.by * g.bz), 256, 0, s>>>(g, aos, L, with_f, bad_type, ids, n_types);
+                          int64_t *ids, int n_types, cudaStream_t s, int z0, int z1) {
+  if (z1 < 0) z1 = g.bz;
+  const long long layer = 2LL * g.bcx * g.by;
+  if (z1 <= z0) return MB_OK;
+  k_unpack_box<<<flat_grid(layer * (z1 - z0)), 256, 0, s>>>(g, aos, L, with_f, bad_type, ids, n_types, layer * z0,
+                                                             layer * z1);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
@@ -198,8 +205,12 @@ int launch_unpack_box(const Geom &g, const mb_atom_element *aos, Lattice64 L, in
 }
 
 int launch_pack_box_ids(const Geom &g, mb_atom_element *aos, const Lattice64 &L, const double *px, const double *py,
-                        const double *pz, double h, int unkick, const int64_t *ids, cudaStream_t s) {
-  k_pack_box<<<flat_grid(2LL * g.bcx * g.by * g.bz), 256, 0, s>>>(g, aos, L, px, py, pz, h, unkick, ids);
+                        const double *pz, double h, int unkick, const int64_t *ids, cudaStream_t s, int z0, int z1) {
+  if (z1 < 0) z1 = g.bz;
+  const long long layer = 2LL * g.bcx * g.by;
+  if (z1 <= z0) return MB_OK;
+  k_pack_box<<<flat_grid(layer * (z1 - z0)), 256, 0, s>>>(g, aos, L, px, py, pz, h, unkick, ids, layer * z0,
+                                                           layer * z1);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }

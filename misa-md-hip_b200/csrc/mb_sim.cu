@@ -15,6 +15,7 @@
 
 #include "mb_common.cuh"
 
+#define MB_SLAB_MAX 32 // z-slabs of the pipelined host-buffer step
 
 struct mb_sim {
   mb_sim_config cfg{};
@@ -59,6 +60,11 @@ struct mb_sim {
   cudaGraphExec_t graph = nullptr; // steady step pair starting at cur == 0
   size_t device_bytes = 0;
   float last_rho_ms = 0.f, last_force_ms = 0.f;
+  // host-buffer step: z-slabs streamed in on cp_in and out on cp_out while the
+  // compute stream works on the slabs that have arrived
+  cudaStream_t cp_in = nullptr, cp_out = nullptr;
+  cudaEvent_t ev_go = nullptr, ev_in[MB_SLAB_MAX] = {}, ev_out[MB_SLAB_MAX] = {};
+  int host_slabs = 0; // 0: automatic (16, fewer on thin boxes), 1: one piece
   // mixed precision: the lattice lives in a one-slot ensemble (mb_ens_host.cu)
   mb_ensemble *ens = nullptr;
   int slot = -1;
@@ -477,6 +483,19 @@ int mb_sim_destroy(mb_sim *s) {
   }
   for (auto &e : s->ev)
     if (e) cudaEventDestroy(e);
+  for (int k = 0; k < MB_SLAB_MAX; k++) {
+    if (s->ev_in[k]) cudaEventDestroy(s->ev_in[k]);
+    if (s->ev_out[k]) cudaEventDestroy(s->ev_out[k]);
+  }
+  if (s->ev_go) cudaEventDestroy(s->ev_go);
+  if (s->cp_in) {
+    cudaStreamSynchronize(s->cp_in);
+    cudaStreamDestroy(s->cp_in);
+  }
+  if (s->cp_out) {
+    cudaStreamSynchronize(s->cp_out);
+    cudaStreamDestroy(s->cp_out);
+  }
   if (s->stream) cudaStreamDestroy(s->stream);
   pot_free(s->pot);
   delete s;
@@ -711,13 +730,36 @@ int mb_sim_kernel_times(mb_sim *s, float *rho_ms, float *force_ms) {
   return MB_OK;
 }
 
-int mb_sim_step_host(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t n_itl) {
-  if (!s || !box_atoms) return fail(MB_ERR_ARG, "null argument");
-  if (s->cfg.precision != MB_PREC_FP64) return fail(MB_ERR_UNSUPPORTED, "host-buffer steps run the FP64 path");
-  MB_TRY(ensure_stage(s, (size_t)s->n_box));
-  drop_graph(s);
-  s->cur = 0;
-  s->primed = false;
+// Box layers [zb[k], zb[k+1]) of the host-buffer step's z-slabs.  Each slab is at
+// least as thick as anything a site or an interstitial reaches (the stencil's ghost
+// layers; interstitial windows of cutoff + skin, flagged sites within them), so the
+// work on slab k reads only slabs k-1, k, k+1 (periodic in z).  Fewer than 4 such
+// slabs: one piece.
+static int slab_plan(const mb_sim *s, int *zb) {
+  const int bz = s->g.bz;
+  const double reach = s->cfg.cutoff + s->cfg.stencil_skin;
+  const int rz = std::max(s->g.gz, (int)ceil(reach / s->cfg.lattice_const) + 2);
+  const int want = s->host_slabs > 0 ? s->host_slabs : 16;
+  int n = std::min(std::min(want, bz / std::max(rz, 1)), MB_SLAB_MAX);
+  if (n < 4) n = 1;
+  for (int k = 0; k <= n; k++) zb[k] = (int)((long long)k * bz / n);
+  return n;
+}
+
+static int ensure_pipe(mb_sim *s) {
+  if (s->cp_in) return MB_OK;
+  MB_CUDA(cudaStreamCreateWithFlags(&s->cp_in, cudaStreamNonBlocking));
+  MB_CUDA(cudaStreamCreateWithFlags(&s->cp_out, cudaStreamNonBlocking));
+  MB_CUDA(cudaEventCreateWithFlags(&s->ev_go, cudaEventDisableTiming));
+  for (int k = 0; k < MB_SLAB_MAX; k++) {
+    MB_CUDA(cudaEventCreateWithFlags(&s->ev_in[k], cudaEventDisableTiming));
+    MB_CUDA(cudaEventCreateWithFlags(&s->ev_out[k], cudaEventDisableTiming));
+  }
+  return MB_OK;
+}
+
+// One step on the whole box: records in, then every pass, then records out.
+static int step_host_whole(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t n_itl) {
   MB_CUDA(cudaMemcpyAsync(s->stage, box_atoms, (size_t)s->n_box * sizeof(mb_atom_element), cudaMemcpyHostToDevice,
                           s->stream));
   Lattice64 L = sim_lattice(s, 0);
@@ -740,6 +782,109 @@ int mb_sim_step_host(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl
                           s->stream));
   MB_CUDA(cudaStreamSynchronize(s->stream));
   if (itl) MB_TRY(download_itl(s, itl, 0, 0));
+  return MB_OK;
+}
+
+// The same step streamed by z-slabs.  The records of slab k come in on cp_in; once
+// they are there the compute stream unpacks, drifts and flags slab k, computes
+// rho / df of slab k-1 >= 1 (its neighbours k-2..k have drifted) and the forces of
+// slab k-2 >= 2 (the df of k-3..k-1 is there), whose records then go out on cp_out
+// while later slabs still come in.  The periodic ring closes at the end: rho / df of
+// slabs n-1 and 0, then the forces of slabs n-2, n-1, 0 and 1.
+// Every site is computed by the same kernels in the same order as in one piece, so the
+// records are bitwise the same.
+static int step_host_slabs(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t n_itl, int n,
+                           const int *zb) {
+  MB_TRY(ensure_pipe(s));
+  MB_TRY(upload_itl(s, itl, n_itl, 1));
+  const Geom &g = s->g;
+  Lattice64 L = sim_lattice(s, 0);
+  L.nx = L.ny = L.nz = nullptr;
+  Itl64 I = sim_itl(s, 0);
+  const StepParams sp = sim_params(s, 1, 0);
+  const DevPot &P = pot_dev(s->pot);
+  const int it = s->n_itl > 0;
+  const long long layer = 2LL * g.bcx * g.by; // records per box layer
+  const size_t rec = sizeof(mb_atom_element);
+  cudaStream_t cs = s->stream;
+  if (it) { // interstitials drift first (their forces came with them); no site is flagged yet
+    MB_CUDA(cudaMemsetAsync(s->flag_count, 0, sizeof(int), cs));
+    MB_TRY(launch_kick_drift64(g, L, I, sp, cs, 0, 0, 1));
+  }
+  MB_CUDA(cudaEventRecord(s->ev_go, cs));
+  MB_CUDA(cudaStreamWaitEvent(s->cp_in, s->ev_go, 0));
+  for (int k = 0; k < n; k++) {
+    const long long r0 = zb[k] * layer, r1 = zb[k + 1] * layer;
+    MB_CUDA(cudaMemcpyAsync(s->stage + r0, box_atoms + r0, (size_t)(r1 - r0) * rec, cudaMemcpyHostToDevice, s->cp_in));
+    MB_CUDA(cudaEventRecord(s->ev_in[k], s->cp_in));
+  }
+  auto arrive = [&](int k) -> int {
+    MB_CUDA(cudaStreamWaitEvent(cs, s->ev_in[k], 0));
+    MB_TRY(launch_unpack_box_ids(g, s->stage, L, 1, s->bad, s->id, P.n_types, cs, zb[k], zb[k + 1]));
+    MB_TRY(launch_images64(g, L, 1, cs, zb[k], zb[k + 1]));
+    MB_TRY(launch_kick_drift64(g, L, I, sp, cs, zb[k], zb[k + 1], 0));
+    if (it) MB_TRY(launch_itl_mark_slab64(g, L, I, zb[k], zb[k + 1], cs));
+    return MB_OK;
+  };
+  auto rho = [&](int k) -> int {
+    MB_TRY(launch_rho64(g, s->st, P, L, sp.rc2, nullptr, 0, it, cs, zb[k], zb[k + 1]));
+    if (it) MB_TRY(launch_itl_rho64(g, s->st, P, L, I, sp.rc2, nullptr, 0, cs, zb[k], zb[k + 1]));
+    return MB_OK;
+  };
+  auto force = [&](int k) -> int {
+    MB_TRY(launch_force64(g, s->st, P, L, sp, nullptr, 0, it, cs, zb[k], zb[k + 1]));
+    if (it) MB_TRY(launch_itl_force64(g, s->st, P, L, I, sp, nullptr, 0, cs, zb[k], zb[k + 1]));
+    MB_TRY(launch_pack_box_ids(g, s->stage, L, L.px, L.py, L.pz, sp.h, 0, s->id, cs, zb[k], zb[k + 1]));
+    MB_CUDA(cudaEventRecord(s->ev_out[k], cs));
+    MB_CUDA(cudaStreamWaitEvent(s->cp_out, s->ev_out[k], 0));
+    const long long r0 = zb[k] * layer, r1 = zb[k + 1] * layer;
+    MB_CUDA(cudaMemcpyAsync(box_atoms + r0, s->stage + r0, (size_t)(r1 - r0) * rec, cudaMemcpyDeviceToHost, s->cp_out));
+    return MB_OK;
+  };
+  int rc = MB_OK;
+  for (int k = 0; k < n && rc == MB_OK; k++) {
+    rc = arrive(k);
+    if (rc == MB_OK && k >= 2) rc = rho(k - 1);
+    if (rc == MB_OK && k >= 4) rc = force(k - 2);
+  }
+  const int tail_rho[2] = {n - 1, 0}, tail_force[4] = {n - 2, n - 1, 0, 1};
+  for (int q = 0; q < 2 && rc == MB_OK; q++) rc = rho(tail_rho[q]);
+  for (int q = 0; q < 4 && rc == MB_OK; q++) rc = force(tail_force[q]);
+  // drain all three streams, also after an error, so the caller's buffer is not in use
+  const cudaError_t e0 = cudaStreamSynchronize(s->cp_in), e1 = cudaStreamSynchronize(cs),
+                    e2 = cudaStreamSynchronize(s->cp_out);
+  MB_TRY(rc);
+  MB_CUDA(e0);
+  MB_CUDA(e1);
+  MB_CUDA(e2);
+  if (itl) MB_TRY(download_itl(s, itl, 0, 0));
+  return MB_OK;
+}
+
+int mb_sim_step_host(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t n_itl) {
+  if (!s || !box_atoms) return fail(MB_ERR_ARG, "null argument");
+  if (s->cfg.precision != MB_PREC_FP64) return fail(MB_ERR_UNSUPPORTED, "host-buffer steps run the FP64 path");
+  MB_TRY(ensure_stage(s, (size_t)s->n_box));
+  drop_graph(s);
+  s->cur = 0;
+  s->primed = false;
+  int zb[MB_SLAB_MAX + 1];
+  const int n = slab_plan(s, zb);
+  if (n == 1) return step_host_whole(s, box_atoms, itl, n_itl);
+  return step_host_slabs(s, box_atoms, itl, n_itl, n, zb);
+}
+
+int mb_sim_set_host_slabs(mb_sim *s, int32_t n_slabs) {
+  if (!s) return fail(MB_ERR_ARG, "null sim");
+  if (n_slabs < 0 || n_slabs > MB_SLAB_MAX) return fail(MB_ERR_ARG, "n_slabs must lie in [0, 32]");
+  s->host_slabs = n_slabs;
+  return MB_OK;
+}
+
+int mb_sim_host_slabs(mb_sim *s, int32_t *n_slabs) {
+  if (!s || !n_slabs) return fail(MB_ERR_ARG, "null argument");
+  int zb[MB_SLAB_MAX + 1];
+  *n_slabs = slab_plan(s, zb);
   return MB_OK;
 }
 

@@ -277,6 +277,58 @@ def test_host_buffer_step_matches_oracle():
     assert rel_err(itl_g["f"], itl["f"]) < F_TOL
 
 
+def _host_state(sc):
+    """Box records and interstitials with the forces of their starting positions."""
+    odom = sc.orc_domain()
+    even, odd = orc.stencil(odom, sc.a0, sc.reach)
+    ext = sc.ext().view(orc.ATOM)
+    itl = sc.itl.view(orc.ATOM).copy()
+    orc.compute_forces(sc.orc_pot(), odom, ext, itl, even, odd, sc.md_params())
+    return odom, even, odd, ext, itl
+
+
+def test_host_buffer_step_in_slabs_matches_oracle():
+    # 23 layers in z: 4 slabs of 5-6 layers (the stencil and the interstitial windows
+    # reach 5), interstitials spread over the box, some near the periodic z faces
+    sc = make(cells=(8, 6, 23), temperature=900.0, vacancy=0.01, n_itl=7, seed=43)
+    odom, even, odd, ext, itl = _host_state(sc)
+    box = _box(ext, sc).view(mb.ATOM_DTYPE).copy()
+    itl_g = itl.view(mb.ATOM_DTYPE).copy()
+    orc.md_run(sc.orc_pot(), odom, ext, itl, even, odd, sc.md_params(), 3)
+    bo = _box(ext, sc)
+    with _sim(sc) as sim:
+        assert sim.host_slabs() == 4
+        for _ in range(3):
+            sim.step_host(box, itl_g)
+    live = bo["type"] >= 0
+    assert rel_err(box["f"][live], bo["f"][live]) < F_TOL
+    assert np.max(np.abs(box["x"][live] - bo["x"][live])) < 1e-10
+    assert np.max(np.abs(box["v"][live] - bo["v"][live])) < 1e-10
+    assert rel_err(itl_g["f"], itl["f"]) < F_TOL
+    assert np.max(np.abs(itl_g["x"] - itl["x"])) < 1e-10
+
+
+@pytest.mark.parametrize("cells,n_itl", [((6, 6, 40), 9), ((7, 5, 33), 0)])
+def test_host_buffer_slabs_are_bitwise_one_piece(cells, n_itl):
+    sc = make(cells=cells, temperature=1200.0, vacancy=0.01, n_itl=n_itl, seed=47)
+    _, _, _, ext, itl = _host_state(sc)
+    box0 = _box(ext, sc).view(mb.ATOM_DTYPE).copy()
+    itl0 = itl.view(mb.ATOM_DTYPE).copy()
+    out = {}
+    for slabs in (1, 0, 5, 4):
+        box, ig = box0.copy(), itl0.copy()
+        with _sim(sc) as sim:
+            sim.set_host_slabs(slabs)
+            out[slabs, "n"] = sim.host_slabs()
+            for _ in range(4):
+                sim.step_host(box, ig if n_itl else None)
+        out[slabs] = (box, ig)
+    assert out[1, "n"] == 1 and out[0, "n"] == cells[2] // 5 and out[5, "n"] == 5 and out[4, "n"] == 4
+    for slabs in (0, 5, 4):
+        for a, b in zip(out[1], out[slabs]):
+            assert a.tobytes() == b.tobytes(), slabs
+
+
 def test_graph_replay_is_bitwise_identical_to_direct_launches():
     sc = make(cells=(8, 8, 8), temperature=600.0, vacancy=0.005, n_itl=2, seed=51)
     out = []
