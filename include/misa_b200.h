@@ -209,10 +209,10 @@ int mb_sim_time_steps(mb_sim *sim, int32_t nsteps, float *ms);
  * RhoDoubleBufferImp / ForceDoubleBufferImp streaming
  * (src/double-buffer/double_buffer.cpp:12-47) for a whole step. */
 int mb_sim_step_host(mb_sim *sim, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t n_itl);
-/* Slabs of mb_sim_step_host: 0 automatic (16, fewer on thin boxes), 1 one piece, else
- * at most that many (each slab at least as thick as the stencil and the interstitial
- * windows reach; fewer than 4 such slabs run in one piece).  mb_sim_host_slabs
- * reports the count a step takes. */
+/* Slabs of mb_sim_step_host: 0 automatic (as many as fit, at most 32, with at least
+ * 4 MiB of records each), 1 one piece, else at most that many.  Each slab is at least
+ * as thick as the stencil and the interstitial windows reach; fewer than 4 such slabs
+ * run in one piece.  mb_sim_host_slabs reports the count a step takes. */
 int mb_sim_set_host_slabs(mb_sim *sim, int32_t n_slabs);
 int mb_sim_host_slabs(mb_sim *sim, int32_t *n_slabs);
 /* Mean device milliseconds of the rho and force launches over 4 extra steps the sim

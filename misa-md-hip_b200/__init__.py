@@ -153,7 +153,8 @@ class Sim:
         check(lib().mb_sim_step_host(self._h, ptr(box), ptr(itl) if n else None, n))
 
     def set_host_slabs(self, n_slabs: int) -> None:
-        """z-slabs step_host streams the box in (0 automatic, 1 one piece)."""
+        """z-slabs step_host streams the box in (0 automatic, 1 one piece, else at most
+        that many)."""
         check(lib().mb_sim_set_host_slabs(self._h, int(n_slabs)))
 
     def host_slabs(self) -> int:

@@ -64,7 +64,7 @@ struct mb_sim {
   // compute stream works on the slabs that have arrived
   cudaStream_t cp_in = nullptr, cp_out = nullptr;
   cudaEvent_t ev_go = nullptr, ev_in[MB_SLAB_MAX] = {}, ev_out[MB_SLAB_MAX] = {};
-  int host_slabs = 0; // 0: automatic (16, fewer on thin boxes), 1: one piece
+  int host_slabs = 0; // 0: automatic (at least 4 MiB of records per slab), 1: one piece
   // mixed precision: the lattice lives in a one-slot ensemble (mb_ens_host.cu)
   mb_ensemble *ens = nullptr;
   int slot = -1;
@@ -733,13 +733,15 @@ int mb_sim_kernel_times(mb_sim *s, float *rho_ms, float *force_ms) {
 // Box layers [zb[k], zb[k+1]) of the host-buffer step's z-slabs.  Each slab is at
 // least as thick as anything a site or an interstitial reaches (the stencil's ghost
 // layers; interstitial windows of cutoff + skin, flagged sites within them), so the
-// work on slab k reads only slabs k-1, k, k+1 (periodic in z).  Fewer than 4 such
-// slabs: one piece.
+// work on slab k reads only slabs k-1, k, k+1 (periodic in z).  Automatic: as many as
+// fit, with at least 4 MiB of records per slab (a slab's copy then outlasts the
+// launches of its passes).  Fewer than 4 slabs: one piece.
 static int slab_plan(const mb_sim *s, int *zb) {
   const int bz = s->g.bz;
   const double reach = s->cfg.cutoff + s->cfg.stencil_skin;
   const int rz = std::max(s->g.gz, (int)ceil(reach / s->cfg.lattice_const) + 2);
-  const int want = s->host_slabs > 0 ? s->host_slabs : 16;
+  const long long by_bytes = (long long)s->n_box * (long long)sizeof(mb_atom_element) / (4LL << 20);
+  const int want = s->host_slabs > 0 ? s->host_slabs : (int)std::min<long long>(by_bytes, MB_SLAB_MAX);
   int n = std::min(std::min(want, bz / std::max(rz, 1)), MB_SLAB_MAX);
   if (n < 4) n = 1;
   for (int k = 0; k <= n; k++) zb[k] = (int)((long long)k * bz / n);

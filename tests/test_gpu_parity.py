@@ -297,6 +297,8 @@ def test_host_buffer_step_in_slabs_matches_oracle():
     orc.md_run(sc.orc_pot(), odom, ext, itl, even, odd, sc.md_params(), 3)
     bo = _box(ext, sc)
     with _sim(sc) as sim:
+        assert sim.host_slabs() == 1  # automatic: too few records to be worth streaming
+        sim.set_host_slabs(4)
         assert sim.host_slabs() == 4
         for _ in range(3):
             sim.step_host(box, itl_g)
@@ -315,7 +317,7 @@ def test_host_buffer_slabs_are_bitwise_one_piece(cells, n_itl):
     box0 = _box(ext, sc).view(mb.ATOM_DTYPE).copy()
     itl0 = itl.view(mb.ATOM_DTYPE).copy()
     out = {}
-    for slabs in (1, 0, 5, 4):
+    for slabs in (1, 32, 5, 4):
         box, ig = box0.copy(), itl0.copy()
         with _sim(sc) as sim:
             sim.set_host_slabs(slabs)
@@ -323,8 +325,9 @@ def test_host_buffer_slabs_are_bitwise_one_piece(cells, n_itl):
             for _ in range(4):
                 sim.step_host(box, ig if n_itl else None)
         out[slabs] = (box, ig)
-    assert out[1, "n"] == 1 and out[0, "n"] == cells[2] // 5 and out[5, "n"] == 5 and out[4, "n"] == 4
-    for slabs in (0, 5, 4):
+    # as many as the reach allows: slabs of at least 5 layers
+    assert out[1, "n"] == 1 and out[32, "n"] == cells[2] // 5 and out[5, "n"] == 5 and out[4, "n"] == 4
+    for slabs in (32, 5, 4):
         for a, b in zip(out[1], out[slabs]):
             assert a.tobytes() == b.tobytes(), slabs
 
