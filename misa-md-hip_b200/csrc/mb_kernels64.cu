@@ -76,7 +76,7 @@ struct RhoArgs {
 // inside the cutoff at the ideal lattice, so nearly every lane needs the spline; the
 // value is masked instead of branched around, which lets iterations overlap.
 template <bool BF>
-__device__ __forceinline__ double rho_term(const RhoArgs &a, const Lattice64 &L, const double4 *s_fval, long long j,
+__device__ __forceinline__ double rho_term(const RhoArgs &a, const Lattice64 &L, const double2 *s_f2, long long j,
                                            double xi, double yi, double zi) {
   const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
   const double d2 = dx * dx + dy * dy + dz * dz;
@@ -86,7 +86,14 @@ __device__ __forceinline__ double rho_term(const RhoArgs &a, const Lattice64 &L,
   int m;
   double p;
   spl_locate(r, a.P.rdr, a.P.nr, m, p);
-  const double4 c = (m >= a.m_lo) ? s_fval[m - a.m_lo] : ldg4(&a.P.f_val[m]);
+  double4 c;
+  if (m >= a.m_lo) {
+    const int k = m - a.m_lo, b = (k >> 2) & 1; // halves swapped on every other group of 4 knots
+    const double2 lo = s_f2[2 * k + b], hi = s_f2[2 * k + (b ^ 1)];
+    c = make_double4(lo.x, lo.y, hi.x, hi.y);
+  } else {
+    c = ldg4(&a.P.f_val[m]);
+  }
   const double v = cubic(c, p);
   return (BF && !in) ? 0.0 : v;
 }
@@ -94,10 +101,19 @@ __device__ __forceinline__ double rho_term(const RhoArgs &a, const Lattice64 &L,
 template <bool ENERGY, bool ONE_TYPE>
 __global__ void __launch_bounds__(MB_RHO_THREADS, 1)
     k_rho64(const __grid_constant__ StencilSet st, const __grid_constant__ RhoArgs a) {
-  extern __shared__ double4 s_fval[];
+  // Spline pieces of knots m_lo.. as 16-byte halves; the halves of knot k trade places
+  // when bit 2 of k is set.  A quarter-warp's 16-byte loads of one half then spread over
+  // all 8 groups of 4 banks (by k mod 8) instead of 4 (k mod 4): fewer bank conflicts
+  // for the random per-lane knots of a stencil entry.
+  extern __shared__ double2 s_f2[];
   const DevPot &P = a.P;
   const int nsm = P.nr - a.m_lo;
-  for (int k = threadIdx.x; k < nsm; k += blockDim.x) s_fval[k] = P.f_val[a.m_lo + k];
+  for (int k = threadIdx.x; k < nsm; k += blockDim.x) {
+    const double4 v = P.f_val[a.m_lo + k];
+    const int b = (k >> 2) & 1;
+    s_f2[2 * k + b] = make_double2(v.x, v.y);
+    s_f2[2 * k + (b ^ 1)] = make_double2(v.z, v.w);
+  }
   __syncthreads();
 
   const Geom &g = a.g;
@@ -127,12 +143,12 @@ __global__ void __launch_bounds__(MB_RHO_THREADS, 1)
       double r0 = 0.0, r1 = 0.0;
       int k = 0;
       for (; k + 1 < st.n_near; k += 2) {
-        r0 += rho_term<true>(a, L, s_fval, i + off[k], xi, yi, zi);
-        r1 += rho_term<true>(a, L, s_fval, i + off[k + 1], xi, yi, zi);
+        r0 += rho_term<true>(a, L, s_f2, i + off[k], xi, yi, zi);
+        r1 += rho_term<true>(a, L, s_f2, i + off[k + 1], xi, yi, zi);
       }
-      if (k < st.n_near) r0 += rho_term<true>(a, L, s_fval, i + off[k++], xi, yi, zi);
+      if (k < st.n_near) r0 += rho_term<true>(a, L, s_f2, i + off[k++], xi, yi, zi);
 #pragma unroll 2
-      for (; k < st.n; k++) r1 += rho_term<false>(a, L, s_fval, i + off[k], xi, yi, zi);
+      for (; k < st.n; k++) r1 += rho_term<false>(a, L, s_f2, i + off[k], xi, yi, zi);
       rho = r0 + r1;
     } else {
 #pragma unroll 4
