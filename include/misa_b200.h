@@ -103,7 +103,10 @@ int mb_pot_init(const mb_eam_tables *tables);
 /* hip_eam_rho_calc (src/hip_arch_acc_imp.cpp:163-181): for every box site with
  * type >= 0, rho = sum over the stencil of f_{t_j}(r) for r < cutoff, then
  * df = F'(rho) (fused, full-neighbour build).  atoms is the host's
- * ghost-extended AoS array (ghosts already filled); rho and df are written back. */
+ * ghost-extended AoS array (ghosts already filled); rho and df are written back.
+ * The array travels in z-slabs (mb_cli_set_batches): later slabs come in while earlier
+ * ones are computed and their box rows go back; page-locked memory from
+ * mb_create_atoms_mem lets those copies run asynchronously. */
 int mb_eam_rho_calc(mb_atom_element *atoms, double cutoff_radius);
 /* hip_eam_df_calc (src/hip_arch_acc_imp.cpp:183-205): a no-op in the full-neighbour
  * build, exactly like the reference (df is produced by the rho pass); in
@@ -111,7 +114,7 @@ int mb_eam_rho_calc(mb_atom_element *atoms, double cutoff_radius);
 int mb_eam_df_calc(mb_atom_element *atoms, double cutoff_radius);
 /* hip_eam_force_calc (src/hip_arch_acc_imp.cpp:207-225): f = sum del * fpair over
  * the stencil, overwriting f of every box site with type >= 0 (needs df of the
- * ghost sites filled by the host). */
+ * ghost sites filled by the host).  Streamed in z-slabs like mb_eam_rho_calc. */
 int mb_eam_force_calc(mb_atom_element *atoms, double cutoff_radius);
 /* The rho pass of mb_eam_rho_calc (same inputs, same results) for hosts that cannot
  * let a plugin allocate device memory: a process whose device memory is already
@@ -145,7 +148,11 @@ int mb_create_atoms_mem(void **atoms, size_t data_type_size, int64_t size_x, int
 /* hip_release_atoms_mem (src/mem.cpp:25-32). */
 int mb_release_atoms_mem(void *atoms, int *released);
 /* hip_cli_options / hip_cli_options_parse (src/cli.cpp:16-27): the -b/--batches
- * value.  Accepted and reported; state is device-resident, so it changes no result. */
+ * value, the number of z-slabs the rho and force hooks stream the array in (as the
+ * reference's double buffer does, src/double-buffer/double_buffer.cpp:12-47, with the
+ * layers split evenly; at most 32).  1, the reference's default, lets the library
+ * choose (slabs of at least 4 MiB of records, at most 16).  The results are bitwise the
+ * same for every count. */
 int mb_cli_set_batches(unsigned int batches);
 unsigned int mb_cli_batches(void);
 
@@ -159,8 +166,9 @@ int mb_stencil_linear(double lattice_const, double reach, int ext_x, int ext_y, 
  * (y, s, c2, c3, s/dx, 2 c2/dx, 3 c3/dx), for checking the table build on the host. */
 int mb_spline_coeffs(const double *y, int n, double dx, double *coef7);
 
-/* Timing of the last hook call: device milliseconds of its kernels and of its
- * host<->device copies (CUDA events). */
+/* Timing of the last hook call (CUDA events): kernel_ms is the span of its device work
+ * (from the first conversion to the last), copy_ms the rest of the call, i.e. the
+ * copies that did not overlap it. */
 int mb_hook_last_timing(float *kernel_ms, float *copy_ms);
 
 /* Throughput of dependent-free FMA chains on the CUDA cores of the current device

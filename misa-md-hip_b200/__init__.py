@@ -65,6 +65,11 @@ class Hooks:
         assert atoms.dtype == ATOM_DTYPE
         check(lib().mb_eam_force_calc(ptr(atoms), cutoff))
 
+    def set_batches(self, batches: int) -> None:
+        """-b/--batches: z-slabs the rho and force hooks stream the array in (1: the
+        library chooses)."""
+        check(lib().mb_cli_set_batches(int(batches)))
+
     def last_timing(self) -> tuple[float, float]:
         k, c = C.c_float(), C.c_float()
         check(lib().mb_hook_last_timing(C.byref(k), C.byref(c)))

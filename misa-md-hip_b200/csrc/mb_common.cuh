@@ -198,10 +198,11 @@ int energy_partials_needed();
 // AoS conversion (mb_layout.cu)
 // Records whose type has no potential table (type >= n_types) raise *bad_type and
 // are kept out of the passes as vacant sites.
+// [t0, t1): ext records (t1 < 0: to the end); [z0, z1): box layers (z1 < 0: to the last).
 int launch_unpack_ext(const Geom &g, const mb_atom_element *aos, int ext_x, int ext_y, int ext_z, Lattice64 L,
-                      int with_df, int *bad_type, int n_types, cudaStream_t s);
+                      int with_df, int *bad_type, int n_types, cudaStream_t s, long long t0 = 0, long long t1 = -1);
 int launch_pack_ext(const Geom &g, mb_atom_element *aos, int ext_x, int ext_y, const Lattice64 &L, int what,
-                    cudaStream_t s); // what: 1 rho+df, 2 force, 3 df only
+                    cudaStream_t s, int z0 = 0, int z1 = -1); // what: 1 rho+df, 2 force, 3 df only
 int launch_unpack_box(const Geom &g, const mb_atom_element *aos, Lattice64 L, int with_f, int *bad_type,
                       int n_types, cudaStream_t s);
 int launch_pack_box(const Geom &g, mb_atom_element *aos, const Lattice64 &L, const double *px, const double *py,

@@ -10,10 +10,11 @@ __device__ __forceinline__ long long split_index(const Geom &g, int ex, int ey, 
   return (long long)(ex & 1) * g.E + ((long long)ez * g.ey + ey) * g.ecx + (ex >> 1);
 }
 
+// Records [t0, t1) of the ext array (x fastest, then y, z: ext layers [t0, t1) / (ext_x * ext_y)).
 __global__ void k_unpack_ext(const Geom g, const mb_atom_element *aos, int ext_x, int ext_y, int ext_z, Lattice64 L,
-                             int with_df, int *bad_type, int n_types) {
-  const long long n = (long long)ext_x * ext_y * ext_z;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+                             int with_df, int *bad_type, int n_types, long long t0, long long t1) {
+  for (long long t = t0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; t < t1;
+       t += (long long)gridDim.x * blockDim.x) {
     const int ex = (int)(t % ext_x);
     const long long r = t / ext_x;
     const int ey = (int)(r % ext_y), ez = (int)(r / ext_y);
@@ -35,12 +36,13 @@ __global__ void k_unpack_ext(const Geom g, const mb_atom_element *aos, int ext_x
 }
 
 // what: 1 rho+df, 2 force, 3 df only.  Only box sites with type >= 0 are written,
-// as the reference's kernels do (src/kernels/kernel_itl.hpp:44,90-103).
+// as the reference's kernels do (src/kernels/kernel_itl.hpp:44,90-103).  Box sites
+// [t0, t1) in box order (doubled x fastest, then y, z).
 __global__ void k_pack_ext(const Geom g, mb_atom_element *aos, int ext_x, int ext_y, const Lattice64 L, int what,
-                           int ghost_x) {
-  const long long n = 2LL * g.bcx * g.by * g.bz;
+                           int ghost_x, long long t0, long long t1) {
   const int bxd = 2 * g.bcx;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = t0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; t < t1;
+       t += (long long)gridDim.x * blockDim.x) {
     const int bx = (int)(t % bxd);
     const long long r = t / bxd;
     const int by = (int)(r % g.by), bz = (int)(r / g.by);
@@ -174,16 +176,23 @@ static int flat_grid(long long n) {
 }
 
 int launch_unpack_ext(const Geom &g, const mb_atom_element *aos, int ext_x, int ext_y, int ext_z, Lattice64 L,
-                      int with_df, int *bad_type, int n_types, cudaStream_t s) {
-  k_unpack_ext<<<flat_grid((long long)ext_x * ext_y * ext_z), 256, 0, s>>>(g, aos, ext_x, ext_y, ext_z, L, with_df,
-                                                                          bad_type, n_types);
+                      int with_df, int *bad_type, int n_types, cudaStream_t s, long long t0, long long t1) {
+  const long long n = (long long)ext_x * ext_y * ext_z;
+  if (t1 < 0 || t1 > n) t1 = n;
+  if (t0 < 0) t0 = 0;
+  if (t1 <= t0) return MB_OK;
+  k_unpack_ext<<<flat_grid(t1 - t0), 256, 0, s>>>(g, aos, ext_x, ext_y, ext_z, L, with_df, bad_type, n_types, t0, t1);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
 
 int launch_pack_ext(const Geom &g, mb_atom_element *aos, int ext_x, int ext_y, const Lattice64 &L, int what,
-                    cudaStream_t s) {
-  k_pack_ext<<<flat_grid(2LL * g.bcx * g.by * g.bz), 256, 0, s>>>(g, aos, ext_x, ext_y, L, what, 2 * g.gcx);
+                    cudaStream_t s, int z0, int z1) {
+  if (z1 < 0) z1 = g.bz;
+  const long long layer = 2LL * g.bcx * g.by;
+  if (z1 <= z0) return MB_OK;
+  k_pack_ext<<<flat_grid(layer * (z1 - z0)), 256, 0, s>>>(g, aos, ext_x, ext_y, L, what, 2 * g.gcx, layer * z0,
+                                                           layer * z1);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }

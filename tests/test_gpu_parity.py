@@ -71,6 +71,40 @@ def test_hook_rho_df_force_match_oracle(hooks, n_types, vac, start):
     assert k > 0 and c > 0
 
 
+@pytest.mark.parametrize("batches", [3, 9])
+def test_hooks_streamed_in_slabs_match_one_piece_and_oracle(hooks, batches):
+    # the reference's -b/--batches z-slab streaming: every slab count gives the same bytes
+    sc = make(cells=(7, 6, 9), temperature=900.0, vacancy=0.02, seed=29, jitter=0.1)
+    dom, odom, even, odd = _hook_setup(hooks, sc)
+    L = [sc.cells[0] * A0, sc.cells[1] * A0, sc.cells[2] * A0]
+    out = {}
+    try:
+        for b in (1, batches):
+            hooks.set_batches(b)
+            ext = sc.ext()
+            hooks.rho_calc(ext, sc.cutoff)
+            orc.ghost_fill(odom, ext.view(orc.ATOM), L, 2)
+            hooks.force_calc(ext, sc.cutoff)
+            out[b] = ext
+            k, c = hooks.last_timing()
+            assert k > 0 and c > 0
+    finally:
+        hooks.set_batches(1)
+    assert out[1].tobytes() == out[batches].tobytes()
+    pot = sc.orc_pot()
+    eo = sc.ext().view(orc.ATOM)
+    orc.rho_pass(pot, odom, eo, even, odd, sc.cutoff)
+    orc.ghost_fill(odom, eo, L, 2)
+    orc.force_pass(pot, odom, eo, even, odd, sc.cutoff)
+    bg, bo = _box(out[batches], sc), _box(eo, sc)
+    live = bg["type"] >= 0
+    assert rel_err(bg["rho"][live], bo["rho"][live]) < 1e-12
+    assert rel_err(bg["df"][live], bo["df"][live]) < 1e-12
+    assert rel_err(bg["f"][live], bo["f"][live]) < F_TOL
+    # ghost records come back as they went in
+    assert np.array_equal(out[batches]["x"], sc.ext()["x"])
+
+
 def test_hook_with_setfl_alloy_matches_oracle(hooks, tmp_path):
     # a two-element Fe-Cu table written as a setfl file and read back drives both paths
     t = mb.potential.alloy_analytic(2, nr=3000, nrho=3000)
