@@ -78,6 +78,13 @@ def test_hooks_validate_call_order_and_arguments():
     assert lib.mb_cli_set_batches(1) == 0
 
 
+def test_host_slab_calls_check_their_arguments():
+    lib = _abi.lib()
+    n = C.c_int32(-1)
+    assert lib.mb_sim_set_host_slabs(None, 4) == _abi.MB_ERR_ARG
+    assert lib.mb_sim_host_slabs(None, C.byref(n)) == _abi.MB_ERR_ARG and n.value == -1
+
+
 def test_stencil_beyond_ghost_is_rejected():
     lib = _abi.lib()
     dom = mb.lattice.domain((6, 6, 6), (2, 1, 1))
