@@ -270,6 +270,14 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
     if (ONE_TYPE) {
       double gx = 0.0, gy = 0.0, gz = 0.0, eq = 0.0;
       int k = 0;
+      // four entries per trip (the two sums alternate as with two), so more neighbour
+      // rows are in flight per warp: 1.547 -> 1.517 ms on 128^3 cells
+      for (; k + 3 < st.n_near; k += 4) {
+        force_term<ENERGY, true>(a, L, s_f1, i + off[k], xi, yi, zi, dfi, fx, fy, fz, ep);
+        force_term<ENERGY, true>(a, L, s_f1, i + off[k + 1], xi, yi, zi, dfi, gx, gy, gz, eq);
+        force_term<ENERGY, true>(a, L, s_f1, i + off[k + 2], xi, yi, zi, dfi, fx, fy, fz, ep);
+        force_term<ENERGY, true>(a, L, s_f1, i + off[k + 3], xi, yi, zi, dfi, gx, gy, gz, eq);
+      }
       for (; k + 1 < st.n_near; k += 2) {
         force_term<ENERGY, true>(a, L, s_f1, i + off[k], xi, yi, zi, dfi, fx, fy, fz, ep);
         force_term<ENERGY, true>(a, L, s_f1, i + off[k + 1], xi, yi, zi, dfi, gx, gy, gz, eq);
