@@ -168,27 +168,26 @@ static int run_hook(HookCtx &c, mb_atom_element *atoms, int with_df, int pack_wh
                               cudaMemcpyHostToDevice, c.cp_in));
       MB_CUDA(cudaEventRecord(c.ev_in[k], c.cp_in));
     }
-    int rc = MB_OK;
-    for (int k = 0; k < nsl && rc == MB_OK; k++) {
-      if (cudaStreamWaitEvent(s, c.ev_in[k], 0) != cudaSuccess) {
-        rc = cuda_fail(cudaGetLastError(), "cudaStreamWaitEvent");
-        break;
-      }
-      if (k == 0) cudaEventRecord(c.ev[1], s);
-      rc = launch_unpack_ext(c.g, c.aos, d.ext_size_x, d.ext_size_y, d.ext_size_z, L, with_df, c.bad, n_types, s,
-                             (long long)e0(k), (long long)e1(k));
-      if (rc == MB_OK) rc = body(L, s, zb[k], zb[k + 1]);
-      if (rc == MB_OK) rc = launch_pack_ext(c.g, c.aos, d.ext_size_x, d.ext_size_y, L, pack_what, s, zb[k], zb[k + 1]);
-      if (rc != MB_OK) break;
-      cudaEventRecord(c.ev_out[k], s);
-      cudaStreamWaitEvent(c.cp_out, c.ev_out[k], 0);
+    // one slab: wait for its layers, convert, compute, convert back, send its rows out
+    auto slab = [&](int k) -> int {
+      MB_CUDA(cudaStreamWaitEvent(s, c.ev_in[k], 0));
+      if (k == 0) MB_CUDA(cudaEventRecord(c.ev[1], s));
+      MB_TRY(launch_unpack_ext(c.g, c.aos, d.ext_size_x, d.ext_size_y, d.ext_size_z, L, with_df, c.bad, n_types, s,
+                               (long long)e0(k), (long long)e1(k)));
+      MB_TRY(body(L, s, zb[k], zb[k + 1]));
+      MB_TRY(launch_pack_ext(c.g, c.aos, d.ext_size_x, d.ext_size_y, L, pack_what, s, zb[k], zb[k + 1]));
+      MB_CUDA(cudaEventRecord(c.ev_out[k], s));
+      MB_CUDA(cudaStreamWaitEvent(c.cp_out, c.ev_out[k], 0));
       const size_t first = row0(zb[k]), last = row1(zb[k + 1] - 1);
-      if (cudaMemcpyAsync(atoms + first, c.aos + first, (last - first + 1) * sizeof(mb_atom_element),
-                          cudaMemcpyDeviceToHost, c.cp_out) != cudaSuccess)
-        rc = cuda_fail(cudaGetLastError(), "cudaMemcpyAsync");
-    }
-    cudaEventRecord(c.ev[2], s);
-    cudaEventRecord(c.ev[3], c.cp_out);
+      MB_CUDA(cudaMemcpyAsync(atoms + first, c.aos + first, (last - first + 1) * sizeof(mb_atom_element),
+                              cudaMemcpyDeviceToHost, c.cp_out));
+      return MB_OK;
+    };
+    int rc = MB_OK;
+    for (int k = 0; k < nsl && rc == MB_OK; k++) rc = slab(k);
+    if (rc == MB_OK && cudaEventRecord(c.ev[2], s) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "cudaEventRecord");
+    if (rc == MB_OK && cudaEventRecord(c.ev[3], c.cp_out) != cudaSuccess)
+      rc = cuda_fail(cudaGetLastError(), "cudaEventRecord");
     // drain both copy streams, also after an error, so the caller's array is not in use
     const cudaError_t e_in = cudaStreamSynchronize(c.cp_in), e_out = cudaStreamSynchronize(c.cp_out);
     MB_TRY(rc);
