@@ -798,21 +798,11 @@ static int step_host_whole(mb_sim *s, mb_atom_element *box_atoms, mb_atom_elemen
 static int step_host_slabs(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t n_itl, int n,
                            const int *zb) {
   MB_TRY(ensure_pipe(s));
-  MB_TRY(upload_itl(s, itl, n_itl, 1));
   const Geom &g = s->g;
-  Lattice64 L = sim_lattice(s, 0);
-  L.nx = L.ny = L.nz = nullptr;
-  Itl64 I = sim_itl(s, 0);
-  const StepParams sp = sim_params(s, 1, 0);
-  const DevPot &P = pot_dev(s->pot);
-  const int it = s->n_itl > 0;
   const long long layer = 2LL * g.bcx * g.by; // records per box layer
   const size_t rec = sizeof(mb_atom_element);
   cudaStream_t cs = s->stream;
-  if (it) { // interstitials drift first (their forces came with them); no site is flagged yet
-    MB_CUDA(cudaMemsetAsync(s->flag_count, 0, sizeof(int), cs));
-    MB_TRY(launch_kick_drift64(g, L, I, sp, cs, 0, 0, 1));
-  }
+  // the slabs start travelling at once (the stage is free: the last call ended synced) ...
   MB_CUDA(cudaEventRecord(s->ev_go, cs));
   MB_CUDA(cudaStreamWaitEvent(s->cp_in, s->ev_go, 0));
   for (int k = 0; k < n; k++) {
@@ -820,6 +810,23 @@ static int step_host_slabs(mb_sim *s, mb_atom_element *box_atoms, mb_atom_elemen
     MB_CUDA(cudaMemcpyAsync(s->stage + r0, box_atoms + r0, (size_t)(r1 - r0) * rec, cudaMemcpyHostToDevice, s->cp_in));
     MB_CUDA(cudaEventRecord(s->ev_in[k], s->cp_in));
   }
+  // ... while the interstitials go up on the compute stream
+  const int urc = upload_itl(s, itl, n_itl, 1);
+  if (urc != MB_OK) {
+    cudaStreamSynchronize(s->cp_in); // the caller's records are not in use after a refusal
+    return urc;
+  }
+  Lattice64 L = sim_lattice(s, 0);
+  L.nx = L.ny = L.nz = nullptr;
+  Itl64 I = sim_itl(s, 0);
+  const StepParams sp = sim_params(s, 1, 0);
+  const DevPot &P = pot_dev(s->pot);
+  const int it = s->n_itl > 0;
+  auto start = [&]() -> int { // interstitials drift first (their forces came with them); no site is flagged yet
+    if (!it) return MB_OK;
+    MB_CUDA(cudaMemsetAsync(s->flag_count, 0, sizeof(int), cs));
+    return launch_kick_drift64(g, L, I, sp, cs, 0, 0, 1);
+  };
   auto arrive = [&](int k) -> int {
     MB_CUDA(cudaStreamWaitEvent(cs, s->ev_in[k], 0));
     MB_TRY(launch_unpack_box_ids(g, s->stage, L, 1, s->bad, s->id, P.n_types, cs, zb[k], zb[k + 1]));
@@ -843,7 +850,7 @@ static int step_host_slabs(mb_sim *s, mb_atom_element *box_atoms, mb_atom_elemen
     MB_CUDA(cudaMemcpyAsync(box_atoms + r0, s->stage + r0, (size_t)(r1 - r0) * rec, cudaMemcpyDeviceToHost, s->cp_out));
     return MB_OK;
   };
-  int rc = MB_OK;
+  int rc = start();
   for (int k = 0; k < n && rc == MB_OK; k++) {
     rc = arrive(k);
     if (rc == MB_OK && k >= 2) rc = rho(k - 1);
