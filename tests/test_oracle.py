@@ -181,3 +181,71 @@ def test_golden_fixture_reproduced():
     np.testing.assert_allclose(box["x"], recs(g["box_out"], mb.ATOM_DTYPE)["x"], rtol=0, atol=1e-12)
     np.testing.assert_allclose(box["f"], recs(g["box_out"], mb.ATOM_DTYPE)["f"], rtol=1e-11, atol=1e-11)
     np.testing.assert_allclose(itl["f"], recs(g["itl_out"], orc.ATOM)["f"], rtol=1e-11, atol=1e-11)
+
+
+def _analytic_lattice(sc, conventional_F):
+    """rho, df, forces and energy per atom of the box from the analytic functions
+    f = (rc - r)^2, phi = 0.8 (rc - r)^2 (1 - 0.2 r) and F = -sqrt(rho), by direct pair
+    sums (minimum image).  conventional_F: F continues linearly past the table's last
+    density with the table's end slope, as the tabulated potential does."""
+    box = sc.box
+    live = box["type"] >= 0
+    x = box["x"][live]
+    L = np.array(sc.cells) * A0
+    d = x[:, None, :] - x[None, :, :]
+    d -= L * np.rint(d / L)
+    r = np.linalg.norm(d, axis=-1)
+    np.fill_diagonal(r, np.inf)
+    m = r < RC
+    rs = np.where(m, r, 1.0)
+    f = np.where(m, (RC - rs) ** 2, 0.0)
+    phi = np.where(m, 0.8 * (RC - rs) ** 2 * (1 - 0.2 * rs), 0.0)
+    dfr = np.where(m, -2 * (RC - rs), 0.0)
+    dphi = np.where(m, 0.8 * (-2 * (RC - rs) * (1 - 0.2 * rs) - 0.2 * (RC - rs) ** 2), 0.0)
+    rho = f.sum(1)
+    t = mb.potential.fe_analytic()
+    rmax = (t.nrho - 1) * t.drho
+    s = (t.F[0, -1] - t.F[0, -2]) / t.drho
+    if conventional_F:
+        F = np.where(rho <= rmax, -np.sqrt(rho), -np.sqrt(rmax) + s * (rho - rmax))
+        dF = np.where(rho <= rmax, -0.5 / np.sqrt(rho), s)
+    else:
+        F, dF = -np.sqrt(rho), -0.5 / np.sqrt(rho)
+    g = dphi + (dF[:, None] + dF[None, :]) * dfr
+    force = (-(g * np.where(m, 1.0 / rs, 0.0))[:, :, None] * d).sum(1)
+    return live, rho, dF, force, (F.sum() + 0.5 * phi.sum()) / x.shape[0]
+
+
+def test_tabulated_potential_against_its_analytic_functions():
+    """The tabulation error, apart from the parity of oracle and library: the 5000-knot
+    tables against the closed forms they sample."""
+    from scenarios import rel_err
+    t = mb.potential.fe_analytic()
+    pot = orc.Pot.from_tables(t)
+    dr = t.dr
+    # interior intervals reproduce the quadratic f and the cubic phi to rounding
+    for r in np.linspace(0.5, RC - 3 * dr, 97):
+        assert pot.rho(0, r) == pytest.approx((RC - r) ** 2, abs=1e-12)
+        assert pot.drho(0, r) == pytest.approx(-2 * (RC - r), abs=1e-10)
+        assert pot.phi(0, 0, r) == pytest.approx(0.8 * (RC - r) ** 2 * (1 - 0.2 * r), abs=1e-12)
+    # the last interval (one-sided end slope): small, bounded departures
+    r = RC - 0.5 * dr
+    assert abs(pot.rho(0, r) - (RC - r) ** 2) < 1e-6
+    assert abs(pot.drho(0, r) + 2 * (RC - r)) < 1e-3
+    # a disordered lattice (sigma 0.1 A: some pairs cross into the last interval)
+    sc = make(cells=(5, 5, 5), temperature=0.0, vacancy=0.02, seed=3, jitter=0.1)
+    ext = sc.ext().view(orc.ATOM)
+    even, odd = orc.stencil(sc.orc_domain(), A0, sc.reach)
+    pe, _ = orc.compute_forces(sc.orc_pot(), sc.orc_domain(), ext, None, even, odd, sc.md_params())
+    box = mb.lattice.ext_to_box(ext.view(mb.ATOM_DTYPE), sc.cells, sc.ghost)
+    live, rho, dF, force, e = _analytic_lattice(sc, conventional_F=True)
+    n = int(live.sum())
+    assert rel_err(box["rho"][live], rho) < 1e-8
+    assert rel_err(box["df"][live], dF) < 1e-12
+    assert rel_err(box["f"][live], force) < 1e-4
+    assert abs(pe / n - e) < 1e-8
+    # the table-range convention itself (F linear past rho = 50 against -sqrt(rho) at
+    # rho ~ 174) is a different potential, not an error: eV/atom and percent-level forces
+    live, rho, dF, force, e_pure = _analytic_lattice(sc, conventional_F=False)
+    assert 2.0 < abs(pe / n - e_pure) < 3.0
+    assert 0.05 < rel_err(box["f"][live], force) < 0.2
