@@ -249,3 +249,20 @@ def test_tabulated_potential_against_its_analytic_functions():
     live, rho, dF, force, e_pure = _analytic_lattice(sc, conventional_F=False)
     assert 2.0 < abs(pe / n - e_pure) < 3.0
     assert 0.05 < rel_err(box["f"][live], force) < 0.2
+
+
+def test_perfect_lattice_analytic_energy_known_answer():
+    # the survey's known answer for the analytic potential at config 1's perfect lattice:
+    # rho = 174.165 and E = -sqrt(rho) + 1/2 sum phi = 13.0355 eV/atom; the tabulated
+    # potential (F linear past rho = 50) gives 10.3813 eV/atom there, which the oracle hits
+    sc = make(cells=(5, 5, 5), temperature=0.0, jitter=0.0)
+    live, rho, _, force, e_pure = _analytic_lattice(sc, conventional_F=False)
+    assert np.allclose(rho, 174.165, atol=5e-3)
+    assert e_pure == pytest.approx(13.0355, abs=5e-4)
+    assert np.abs(force).max() < 1e-11
+    _, _, _, _, e_conv = _analytic_lattice(sc, conventional_F=True)
+    assert e_conv == pytest.approx(10.3813, abs=5e-4)
+    ext = sc.ext().view(orc.ATOM)
+    even, odd = orc.stencil(sc.orc_domain(), A0, sc.reach)
+    pe, _ = orc.compute_forces(sc.orc_pot(), sc.orc_domain(), ext, None, even, odd, sc.md_params())
+    assert pe / int(live.sum()) == pytest.approx(e_conv, rel=1e-10)
