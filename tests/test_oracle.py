@@ -252,8 +252,8 @@ def test_tabulated_potential_against_its_analytic_functions():
 
 
 def test_perfect_lattice_analytic_energy_known_answer():
-    # the survey's known answer for the analytic potential at config 1's perfect lattice:
-    # rho = 174.165 and E = -sqrt(rho) + 1/2 sum phi = 13.0355 eV/atom; the tabulated
+    # the known answer of the analytic potential at the perfect BCC Fe lattice (a0 2.855 A,
+    # rc 5.6 A): rho = 174.165 and E = -sqrt(rho) + 1/2 sum phi = 13.0355 eV/atom; the tabulated
     # potential (F linear past rho = 50) gives 10.3813 eV/atom there, which the oracle hits
     sc = make(cells=(5, 5, 5), temperature=0.0, jitter=0.0)
     live, rho, _, force, e_pure = _analytic_lattice(sc, conventional_F=False)
