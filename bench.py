@@ -379,8 +379,8 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
     sim.close()
     if precision == mb.MB_PREC_FP64:
         launches_per_step = 6 if itl.shape[0] else 2  # itl clear, itl mark, rho, itl rho, force, itl force
-    elif rho_ms > 0:  # split: itl clear, mark, rho, itl rho, force, itl force, bookkeeping
-        launches_per_step = 7 if itl.shape[0] else 3
+    elif rho_ms > 0:  # split: itl clear, bin, mark, rho, itl rho, force, itl force, bookkeeping
+        launches_per_step = 8 if itl.shape[0] else 3
     else:
         launches_per_step = 1
     if rank == 0:

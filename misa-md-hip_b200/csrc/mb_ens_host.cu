@@ -1287,7 +1287,9 @@ int mb_ensemble_kernel_times(mb_ensemble *e, float *rho_ms, float *force_ms, int
   if (force_ms) *force_ms = tf / reps;
   if (kernels_per_step)
     *kernels_per_step =
-        e->split ? (3 + (e->P.n_itl_lats > 0 ? 4 + (e->P.conv2 > 0.0 ? 1 : 0) : 0)) : 1;
+        // split: rho, force, bookkeeping; with interstitials also clear, bin, mark and the
+        // two item passes; with conversion the conversion kernel
+        e->split ? (3 + (e->P.n_itl_lats > 0 ? 5 + (e->P.conv2 > 0.0 ? 1 : 0) : 0)) : 1;
   return MB_OK;
 }
 
