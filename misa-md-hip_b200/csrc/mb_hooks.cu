@@ -57,6 +57,11 @@ struct HookCtx {
 static HookCtx g_ctx;
 static std::mutex g_mu;
 
+// Device address of the allocation-free rho pass's fixed scratch array, per device
+// ordinal (looked up on first use; see mb_eam_rho_calc_noalloc).
+#define MB_NOALLOC_MAX_DEVICES 64
+static unsigned char *g_noalloc_dev[MB_NOALLOC_MAX_DEVICES] = {};
+
 static void free_buffers(HookCtx &c) {
   void *ptrs[] = {c.aos, c.px, c.py, c.pz, c.df, c.rho, c.fx, c.fy, c.fz, c.code, c.bad};
   for (void *p : ptrs)
@@ -286,6 +291,7 @@ int mb_env_clean(void) {
   if (c.stream) cudaStreamDestroy(c.stream);
   c.stream = nullptr;
   c.env = c.domain = c.stencil = c.pot = false;
+  for (auto &p : g_noalloc_dev) p = nullptr; // looked up again on the next call
   return MB_OK;
 }
 
@@ -497,8 +503,6 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[MB_NOALLOC_SCRA
 
 namespace mb {
 
-static unsigned char *g_noalloc_dev[64] = {}; // device address of g_noalloc_scratch, per device ordinal
-
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // Bytes of scratch one ext site needs (AoS copy + positions + code + df + rho),
@@ -535,9 +539,14 @@ extern "C" int mb_eam_rho_calc_noalloc(mb_atom_element *atoms, double cutoff_rad
                                 " sites; the fixed scratch of " + std::to_string(MB_NOALLOC_SCRATCH_BYTES) +
                                 " bytes holds at most " + std::to_string(noalloc_max_sites()) +
                                 " (use mb_eam_rho_calc for larger lattices)");
+  // The hooks' stream lives on the device mb_env_init selected, and each GPU has its own
+  // copy of the scratch array: the address must be the one of that device.
   int dev = 0;
   MB_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return fail(MB_ERR_ARG, "device ordinal beyond 63");
+  if (dev != c.device)
+    return fail(MB_ERR_STATE, "mb_eam_rho_calc_noalloc: the calling thread's current device (" + std::to_string(dev) +
+                                  ") is not the device mb_env_init selected (" + std::to_string(c.device) + ")");
+  if (dev < 0 || dev >= MB_NOALLOC_MAX_DEVICES) return fail(MB_ERR_ARG, "device ordinal beyond 63");
   if (!g_noalloc_dev[dev]) {
     void *p = nullptr;
     MB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
@@ -567,14 +576,26 @@ extern "C" int mb_eam_rho_calc_noalloc(mb_atom_element *atoms, double cutoff_rad
   cudaStream_t s = c.stream;
   MB_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s)); // the flag must start at zero on every call
   MB_CUDA(cudaMemcpyAsync(aos, atoms, n * sizeof(mb_atom_element), cudaMemcpyHostToDevice, s));
-  MB_TRY(launch_unpack_ext(c.g, aos, d.ext_size_x, d.ext_size_y, d.ext_size_z, L, 0, bad, pot_dev(c.potp).n_types, s));
-  MB_TRY(launch_rho64(c.g, c.st, pot_dev(c.potp), L, cutoff_radius * cutoff_radius, nullptr, 0, 0, s));
-  MB_TRY(launch_pack_ext(c.g, aos, d.ext_size_x, d.ext_size_y, L, 1, s));
-  MB_CUDA(cudaMemcpyAsync(atoms + first, aos + first, (last - first + 1) * sizeof(mb_atom_element),
-                          cudaMemcpyDeviceToHost, s));
+  // From here the caller's array may be in use by a queued copy: every exit drains the
+  // stream first, so the caller can free or reuse the array as soon as this returns.
+  auto drained = [&](int rc) {
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (rc != MB_OK) return rc;
+    return e == cudaSuccess ? MB_OK : cuda_fail(e, "cudaStreamSynchronize");
+  };
+  int rc = launch_unpack_ext(c.g, aos, d.ext_size_x, d.ext_size_y, d.ext_size_z, L, 0, bad, pot_dev(c.potp).n_types, s);
+  if (rc == MB_OK) rc = launch_rho64(c.g, c.st, pot_dev(c.potp), L, cutoff_radius * cutoff_radius, nullptr, 0, 0, s);
   int flag = 0;
-  MB_CUDA(cudaMemcpyAsync(&flag, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
-  MB_CUDA(cudaStreamSynchronize(s));
-  if (flag) return fail(MB_ERR_ARG, "atom type >= 64 is not supported (treated as vacant)");
-  return MB_OK;
+  if (rc == MB_OK && cudaMemcpyAsync(&flag, bad, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    rc = cuda_fail(cudaGetLastError(), "cudaMemcpyAsync");
+  MB_TRY(drained(rc));
+  // A record whose type has no potential table: refuse before anything is written back,
+  // so the caller's array is left as it was.
+  if (flag) return fail(MB_ERR_ARG, "atom type without a potential table (treated as vacant)");
+  rc = launch_pack_ext(c.g, aos, d.ext_size_x, d.ext_size_y, L, 1, s);
+  if (rc == MB_OK &&
+      cudaMemcpyAsync(atoms + first, aos + first, (last - first + 1) * sizeof(mb_atom_element),
+                      cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    rc = cuda_fail(cudaGetLastError(), "cudaMemcpyAsync");
+  return drained(rc);
 }

@@ -50,6 +50,26 @@ def test_noalloc_rho_matches_allocating_rho_twice_in_a_row():
         assert np.array_equal(bgot["rho"][~live], bref["rho"][~live])
 
 
+def test_noalloc_refuses_types_without_a_potential_table_and_leaves_the_array():
+    hooks = mb.Hooks(0)
+    sc = make(cells=(6, 6, 6), seed=5)
+    _prepare(hooks, sc)
+    ext = sc.ext()
+    ext["type"][len(ext) // 2] = 2  # the one-type potential has a table for type 0 only
+    before = ext.copy()
+    rc = _abi.lib().mb_eam_rho_calc_noalloc(_abi.ptr(ext), sc.cutoff)
+    assert rc == _abi.MB_ERR_ARG
+    assert b"potential table" in _abi.lib().mb_last_error()
+    assert ext.tobytes() == before.tobytes()
+    # the next call on a valid lattice is not affected by the refused one
+    ok = sc.ext()
+    ref = ok.copy()
+    hooks.rho_calc(ref, sc.cutoff)
+    _abi.check(_abi.lib().mb_eam_rho_calc_noalloc(_abi.ptr(ok), sc.cutoff))
+    live = ref["type"] >= 0
+    assert rel_err(ok["rho"][live], ref["rho"][live]) < 1e-12
+
+
 def test_noalloc_refuses_lattices_beyond_its_scratch():
     hooks = mb.Hooks(0)
     sc = make(cells=(40, 40, 40), temperature=300.0, seed=3, jitter=0.0)
