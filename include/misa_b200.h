@@ -123,9 +123,12 @@ int mb_eam_force_calc(mb_atom_element *atoms, double cutoff_radius);
  * reference.  It calls no cudaMalloc / cudaFree: its scratch is a fixed 16 MiB
  * device array inside the library, present on every GPU that loads the library
  * until exit, which limits the ghost-extended lattice to about 115,000 sites
- * (145 bytes each); larger lattices are refused with MB_ERR_ARG.  The first call on
- * a device looks the array's device address up (cudaGetSymbolAddress) and should
- * come before any stream capture.  All calls share the array and it keeps the
+ * (145 bytes each); larger lattices are refused with MB_ERR_ARG.  The calling
+ * thread's current device must be the one mb_env_init selected (else MB_ERR_STATE).
+ * The first call on a device (and the first after mb_env_clean) looks the array's
+ * device address up (cudaGetSymbolAddress) and should come before any stream
+ * capture.  A record whose type has no potential table is refused with MB_ERR_ARG
+ * before anything is written back.  All calls share the array and it keeps the
  * previous call's contents; calls that overlap on the GPU race. */
 int mb_eam_rho_calc_noalloc(mb_atom_element *atoms, double cutoff_radius);
 /* The calDf kernel of the half-neighbour build (src/kernels/hip_kernels.hip.cpp:21-40):
@@ -297,6 +300,12 @@ int mb_ensemble_set_policy(mb_ensemble *e, int32_t policy);
 int mb_ensemble_autotune(mb_ensemble *e, int32_t steps, int32_t *policy, float *best_ms);
 int mb_ensemble_info(mb_ensemble *e, int64_t *n_sites, int64_t *n_tiles, int64_t *device_bytes, int32_t *n_slots);
 int mb_ensemble_set_graphs(mb_ensemble *e, int enable);
+/* Polls a grid barrier of the persistent step kernel (mode 1) makes before it gives up:
+ * the launch then ends early, the state of the lattices in flight is undefined, and the
+ * next sync / download returns MB_ERR_TIMEOUT (the barrier is reset, so later launches run
+ * normally).  Negative restores the default (2^25 polls, ~64 ns apart); 0 gives up at the
+ * first poll that finds the barrier still closed.  For failure-detection tests. */
+int mb_ensemble_set_wait_limit(mb_ensemble *e, int64_t barrier_polls);
 /* Kernel structure: 0 (default) runs the separate density and force kernels ("split":
  * one CUDA graph of up to 8 launches per step, every lattice in each launch) whenever
  * their built-in BCC stencil applies and the persistent one-launch-per-step tile

@@ -320,6 +320,11 @@ class Ensemble:
         """0: split kernels where their stencil applies (default), 1: persistent, 2: split."""
         check(lib().mb_ensemble_set_mode(self._h, mode))
 
+    def set_wait_limit(self, barrier_polls: int) -> None:
+        """Polls a grid barrier of the persistent kernel makes before giving up with
+        MB_ERR_TIMEOUT (mb_ensemble_set_wait_limit); negative restores the default."""
+        check(lib().mb_ensemble_set_wait_limit(self._h, int(barrier_polls)))
+
     def kernel_times(self) -> tuple[float, float, int]:
         """(density ms, force ms, kernels per step) of one step; see mb_ensemble_kernel_times."""
         a, b, n = C.c_float(), C.c_float(), C.c_int32()

@@ -131,6 +131,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_ensemble_autotune": (_I, [_P, C.c_int32, C.POINTER(C.c_int32), _PF]),
     "mb_ensemble_info": (_I, [_P, _PI64, _PI64, _PI64, C.POINTER(C.c_int32)]),
     "mb_ensemble_set_graphs": (_I, [_P, _I]),
+    "mb_ensemble_set_wait_limit": (_I, [_P, C.c_int64]),
     "mb_ensemble_set_mode": (_I, [_P, C.c_int32]),
     "mb_ensemble_kernel_times": (_I, [_P, _PF, _PF, C.POINTER(C.c_int32)]),
 }

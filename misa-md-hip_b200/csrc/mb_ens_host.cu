@@ -187,6 +187,7 @@ struct mb_ensemble {
   bool graphs_ok = true;
   int policy = -1; // -1: size model per lattice; 0..3: one shape for all
   int mode = 0;  // 0: split kernels when the built-in shells apply, else persistent; 1: persistent; 2: split
+  unsigned bar_spins = ENS_BAR_SPINS; // grid-barrier poll limit of the persistent kernel
   double conv_d = 0.0, rec_d = 0.0; // lattice <-> interstitial conversion (off while conv_d == 0)
   int split = 0; // kernels in use: 0 persistent, 1 split with the brick walk, 2 split with the linear walk
   unsigned *d_item_first = nullptr; // linear walk: first item of each lattice
@@ -502,6 +503,7 @@ static int rebuild(mb_ensemble *e) {
   P.itl_lats = e->d_itl_lats;
   P.n_itl_lats = (int)itl_lats.size();
   P.bar = e->d_bar;
+  P.bar_spins = e->bar_spins;
   P.err = e->d_err;
   e->grid = std::max(1, std::min(e->max_grid, e->n_tiles));
   // kernel structure: split kernels whenever their stencil applies (unless the
@@ -1415,6 +1417,17 @@ int mb_ensemble_set_mode(mb_ensemble *e, int32_t mode) {
   MB_TRY(sync_desc(e));
   e->mode = mode;
   e->dirty = true;
+  return MB_OK;
+}
+
+int mb_ensemble_set_wait_limit(mb_ensemble *e, int64_t barrier_polls) {
+  if (!e) return fail(MB_ERR_ARG, "null ensemble");
+  if (barrier_polls > 0xFFFFFFFFLL) return fail(MB_ERR_ARG, "barrier_polls above 2^32 - 1");
+  std::lock_guard<std::mutex> lk(e->mu);
+  MB_TRY(sync_desc(e));
+  e->bar_spins = barrier_polls < 0 ? ENS_BAR_SPINS : (unsigned)barrier_polls;
+  e->P.bar_spins = e->bar_spins;
+  drop_graph(e); // the captured launch holds the old limit
   return MB_OK;
 }
 

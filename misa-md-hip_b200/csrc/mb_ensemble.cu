@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(ENS_THREADS, 1) k_ens_step(const __grid_consta
       const LatDesc &d = P.lats[P.itl_lats[q]];
       if (lat_active(d)) itl_clear_flags(d);
     }
-    if (!grid_sync(P.bar, P.err)) return;
+    if (!grid_sync(P.bar, P.err, P.bar_spins)) return;
     const int warps = gridDim.x * (blockDim.x >> 5);
     const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     for (int q = 0; q < P.n_itl_lats; q++) {
@@ -370,23 +370,23 @@ __global__ void __launch_bounds__(ENS_THREADS, 1) k_ens_step(const __grid_consta
       if (!lat_active(d)) continue;
       for (int it = gw; it < d.n_itl; it += warps) itl_mark_one(P, d, it);
     }
-    if (!grid_sync(P.bar, P.err)) return;
+    if (!grid_sync(P.bar, P.err, P.bar_spins)) return;
   }
   // B: density over lattice tiles
   rho_tiles<ENERGY>(P, T, s_fv);
-  if (!grid_sync(P.bar, P.err)) return;
+  if (!grid_sync(P.bar, P.err, P.bar_spins)) return;
   // C: density of flagged sites and interstitials
   if (P.n_itl_lats > 0) {
     itl_items<false, ENERGY>(P);
-    if (!grid_sync(P.bar, P.err)) return;
+    if (!grid_sync(P.bar, P.err, P.bar_spins)) return;
   }
   // D: forces and integration over lattice tiles (flagged sites: lattice part only)
   force_tiles<ENERGY>(P, T, s_fd);
-  if (!grid_sync(P.bar, P.err)) return;
+  if (!grid_sync(P.bar, P.err, P.bar_spins)) return;
   // E: forces and integration of flagged sites and interstitials
   if (P.n_itl_lats > 0) {
     itl_items<true, ENERGY>(P);
-    if (!grid_sync(P.bar, P.err)) return;
+    if (!grid_sync(P.bar, P.err, P.bar_spins)) return;
   }
   // F: step bookkeeping
   if (blockIdx.x == 0) {

@@ -98,6 +98,7 @@ struct EnsParams {
   int n_tiles;
   const CUtensorMap *tmaps; // [lattice][buffer]
   unsigned *bar;
+  unsigned bar_spins; // polls a grid barrier makes before it gives up (ENS_BAR_SPINS by default)
   int *err;
   double *epart; // [tile][2]
   const int *itl_lats;
@@ -184,9 +185,11 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
   return v;
 }
 
-// Grid-wide barrier (all CTAs co-resident: cooperative launch).  Gives up after a
-// bounded number of polls, raising err; returns false once err is set.
-__device__ __forceinline__ bool grid_sync(unsigned *bar, int *err) {
+// Grid-wide barrier (all CTAs co-resident: cooperative launch).  Gives up after
+// `limit` polls, raising err; returns false once err is set.  Every CTA still arrives
+// before it waits, so the barrier that gave up completes its count and the CTAs that
+// return leave no tile copy in flight (barriers sit between the tile phases).
+__device__ __forceinline__ bool grid_sync(unsigned *bar, int *err, unsigned limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -201,7 +204,7 @@ __device__ __forceinline__ bool grid_sync(unsigned *bar, int *err) {
     } else {
       unsigned spins = 0;
       while (ld_acquire_u32(bar + 1) == gen) {
-        if (++spins > ENS_BAR_SPINS) {
+        if (++spins > limit) {
           atomicExch(err, 1);
           ok = 0;
           break;
