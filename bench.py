@@ -43,15 +43,18 @@ BYTES_MIXED_RHO, BYTES_MIXED_FORCE = 32, 128  # mixed: df and f stored as FP32
 BYTES_MIXED = BYTES_MIXED_RHO + BYTES_MIXED_FORCE
 FLOP_RHO, FLOP_FORCE = 58 * 20, 58 * 50 + 30
 
+# velocity_seed: seed of the Maxwell-Boltzmann draw; seed: vacancies and interstitial
+# sites.  oracle: the same workload's name in oracle/workload.py (the CPU reference arm
+# builds it there, from the same seeds, without loading this package).
 WORKLOADS = {
     "scale": dict(name="fe_bcc_128c_vac0.5pct_itl200_300K_fp64", cells=(128, 128, 128), temperature=300.0,
-                  vacancy=0.005, n_itl=200, seed=7, precision="fp64"),
+                  vacancy=0.005, n_itl=200, seed=7, velocity_seed=1007, precision="fp64", oracle="fe128"),
     "mixed": dict(name="fe_bcc_200c_vac0.5pct_itl763_900K_mixed", cells=(200, 200, 200), temperature=900.0,
-                  vacancy=0.005, n_itl=763, seed=7, precision="mixed"),
+                  vacancy=0.005, n_itl=763, seed=7, velocity_seed=1007, precision="mixed", oracle="fe200"),
     "scale_mixed": dict(name="fe_bcc_128c_vac0.5pct_itl200_300K_mixed", cells=(128, 128, 128), temperature=300.0,
-                        vacancy=0.005, n_itl=200, seed=7, precision="mixed"),
+                        vacancy=0.005, n_itl=200, seed=7, velocity_seed=1007, precision="mixed", oracle="fe128"),
     "small": dict(name="fe_bcc_20c_600K_fp64", cells=(20, 20, 20), temperature=600.0, vacancy=0.0, n_itl=0,
-                  seed=42, precision="fp64"),
+                  seed=42, velocity_seed=42, precision="fp64", oracle="fe20"),
 }
 
 
@@ -74,8 +77,7 @@ def build_state(mb, wl: dict, cells=None):
     scale = (cells[0] * cells[1] * cells[2]) / float(np.prod(wl["cells"]))
     n_itl = int(round(wl["n_itl"] * scale))
     itl = mb.lattice.octahedral_interstitials(n_itl, cells, A0, wl["seed"])
-    # interstitials never sit on a vacated site's octahedral neighbour twice: distinct sites suffice
-    mb.lattice.maxwell_boltzmann(box, itl, wl["temperature"], MASS, wl["seed"] + 1000)
+    mb.lattice.maxwell_boltzmann(box, itl, wl["temperature"], MASS, wl["velocity_seed"])
     return box, itl
 
 
@@ -194,46 +196,50 @@ def barrier(pg):
         pg.barrier()
 
 
-def cpu_oracle_rate(mb, wl: dict, cells, steps: int, threads: int | None = None):
-    """Atom-steps/s of the CPU oracle (the reference algorithm restated) on a sample lattice."""
+def cpu_oracle_rate(wl: dict, warmup: int, steps: int, threads: int | None = None) -> dict:
+    """Atom-steps/s of the CPU oracle (the reference's lattice EAM step restated in C,
+    OpenMP over sites) on the whole workload: the lattice and its defects are built by
+    oracle/workload.py from the workload's seeds, the forces at the start are computed
+    (untimed), then `warmup` untimed and `steps` timed velocity-Verlet steps, each one
+    rho / df / force evaluation of every atom.  Loads the oracle only, never this
+    package."""
     sys.path.insert(0, str(ROOT))
     from oracle import oracle as orc
+    from oracle import workload as W
     if threads:
         orc.set_threads(threads)
-    box, itl = build_state(mb, wl, cells)
-    ghost = mb.lattice.ghost_for_reach(A0, RC + SKIN)
-    dom = orc.make_domain(cells, ghost)
-    even, odd = orc.stencil(dom, A0, RC + SKIN)
-    ext = mb.lattice.box_to_ext(box, cells, ghost, A0).view(orc.ATOM)
-    io = itl.view(orc.ATOM).copy()
-    pot = orc.Pot.from_tables(mb.potential.fe_analytic())
-    mp = orc.md_params(A0, MASS, DT, RC)
-    n_atoms = int((box["type"] >= 0).sum()) + io.shape[0]
-    orc.compute_forces(pot, dom, ext, io, even, odd, mp)  # forces at the start (untimed)
+    box, itl = W.config_state(wl["oracle"])
+    run = W.OracleRun(box, itl, wl["cells"], reach=RC + SKIN)
+    del box
+    if warmup:
+        run.steps(warmup)
     t0 = time.perf_counter()
-    orc.md_run(pot, dom, ext, io, even, odd, mp, steps, record=False)  # one force evaluation per step
+    run.steps(steps)
     dt = time.perf_counter() - t0
-    return n_atoms, dt, orc.num_threads()
+    n_cells = "x".join(str(c) for c in wl["cells"])
+    return {"value": run.n_atoms * steps / dt, "unit": "atom-steps/s", "cores": orc.num_threads(), "kind": "port",
+            "sample": f"the whole workload ({n_cells} cells, {run.n_atoms} atoms): {warmup} untimed + {steps} "
+                      f"timed steps of the C oracle, OpenMP over sites", "ms_per_step": dt / steps * 1e3}
 
 
-def run_reference(args, mb, wl, world, rank) -> None:
-    if rank != 0:
+def run_reference(args, wl) -> None:
+    """The reference's CPU implementation of the path (the C oracle port: the
+    reference's own CPU EAM path lives in the MISA-MD host, which is not available) on
+    the same workload as the GPU arm, with every host thread: W untimed and K timed
+    steps of the whole lattice.  Under torchrun only rank 0 runs it."""
+    if "oracle" not in wl:
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU reference arm times the single-lattice "
+                          "configurations (scale, small, mixed, scale_mixed)"}), flush=True)
         return
-    cells = tuple(min(c, 48) for c in wl["cells"])
-    n_threads = os.cpu_count() or 1
-    # warm-up steps (untimed) then K timed steps, each one MD step of the sample lattice
-    if args.warmup:
-        cpu_oracle_rate(mb, wl, cells, 1, n_threads)
-    n_atoms, dt, thr = cpu_oracle_rate(mb, wl, cells, args.steps, n_threads)
-    step_time = dt / args.steps
-    value = n_atoms / step_time
-    sample = f"{cells[0]}x{cells[1]}x{cells[2]} cells of the same workload ({n_atoms} atoms), 1 step per timed step"
+    cpu = cpu_oracle_rate(wl, args.warmup, args.steps, os.cpu_count())
+    value = cpu["value"]
     line = {
         "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": step_time * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": wl["name"], "sample_cells": list(cells)},
-        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": thr, "kind": "port", "sample": sample},
+        "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice, analytic tabulated potential)",
+        "impl": "reference",
+        "config": {"workload": wl["name"], "cells": list(wl["cells"])},
+        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -369,10 +375,9 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cells = tuple(min(c, 32) for c in wl["cells"])
-        na, dt, thr = cpu_oracle_rate(mb, wl, cells, 3, os.cpu_count())
-        cpu = {"value": na * 3 / dt, "unit": "atom-steps/s", "cores": thr, "kind": "port",
-               "sample": f"{cells[0]}x{cells[1]}x{cells[2]} cells of the same workload ({na} atoms), 3 steps"}
+        # the reference arm's measurement (same lattice, same threads), with fewer steps
+        c = cpu_oracle_rate(wl, 1, 4, os.cpu_count())
+        cpu = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
     mixed = None
     if precision == mb.MB_PREC_FP64 and not args.no_mixed:
         mixed = mixed_comparison(args, mb, wl, box, itl, n_atoms, value / world, pg)
@@ -637,8 +642,8 @@ def run_serve(args, mb, world, rank, local, pg) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(WORKLOADS) + ["ensemble", "serve", "nve"], default="scale")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -660,13 +665,16 @@ def main() -> None:
                     help="--config nve: an interstitial this close (A) to a vacant site takes it")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    wl = WORKLOADS.get(args.config, {"name": args.config})
+    if args.impl == "reference":
+        # CPU only: no process group, no GPU, no product library; rank 0 alone measures
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_reference(args, wl)
+        return
     world, rank, local, pg = dist_setup()
     mb = _package()
-    wl = WORKLOADS.get(args.config, WORKLOADS["scale"])
     try:
-        if args.impl == "reference":
-            run_reference(args, mb, wl, world, rank)
-        elif args.config == "ensemble":
+        if args.config == "ensemble":
             run_ensemble(args, mb, world, rank, local, pg)
         elif args.config == "serve":
             run_serve(args, mb, world, rank, local, pg)

@@ -72,5 +72,21 @@ def test_reference_arm_under_torchrun_prints_one_line_from_rank_zero():
     assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
 
 
+def test_reference_arm_loads_the_oracle_and_not_the_product():
+    # The CPU reference arm builds its workload with oracle/workload.py and times the C
+    # oracle: the product library must not be mapped into its process.
+    code = ("import json, sys; sys.argv = ['bench.py', '--impl', 'reference', '--config', 'small', '--steps', '1', "
+            "'--warmup', '0']; import bench; bench.main(); "
+            "maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({'product': 'libmisa_b200' in maps, 'oracle': 'liboracle' in maps, "
+            "'pkg': 'misa_b200' in sys.modules}))")
+    env = dict(os.environ, OMP_NUM_THREADS="2")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=240, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(s) for s in r.stdout.splitlines() if s.startswith("{")]
+    assert lines[0]["impl"] == "reference" and lines[0]["value"] > 0
+    assert lines[1] == {"product": False, "oracle": True, "pkg": False}
+
+
 if __name__ == "__main__":
     pytest.main([__file__, "-q"])

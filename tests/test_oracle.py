@@ -266,3 +266,27 @@ def test_perfect_lattice_analytic_energy_known_answer():
     even, odd = orc.stencil(sc.orc_domain(), A0, sc.reach)
     pe, _ = orc.compute_forces(sc.orc_pot(), sc.orc_domain(), ext, None, even, odd, sc.md_params())
     assert pe / int(live.sum()) == pytest.approx(e_conv, rel=1e-10)
+
+
+@pytest.mark.parametrize("name,cells", [("fe20", (5, 6, 4)), ("fe128", (12, 10, 9))])
+def test_oracle_workload_builder_equals_the_package_set_up(name, cells):
+    # The CPU reference arm of the benchmark builds its inputs with oracle/workload.py
+    # (it must not load the product library); the GPU arm with the package.  Same seeds,
+    # same bytes: the two arms time the same workload.
+    from oracle import workload as W
+    c = W.CONFIGS[name]
+    box_o, itl_o = W.config_state(name, cells)
+    box = mb.lattice.bcc_box(cells, A0)
+    mb.lattice.add_vacancies(box, c["vacancy"], c["seed"])
+    n_itl = int(round(c["n_itl"] * np.prod(cells) / float(np.prod(c["cells"]))))
+    itl = mb.lattice.octahedral_interstitials(n_itl, cells, A0, c["seed"])
+    mb.lattice.maxwell_boltzmann(box, itl, c["temperature"], W.MASS, c["velocity_seed"])
+    assert box.tobytes() == box_o.tobytes()
+    assert itl.tobytes() == itl_o.tobytes()
+    ghost = mb.lattice.ghost_for_reach(A0, W.RC + W.SKIN)
+    assert W.ghost_for_reach(A0, W.RC + W.SKIN) == ghost
+    assert W.box_to_ext(box_o, cells, ghost).tobytes() == mb.lattice.box_to_ext(box, cells, ghost, A0).tobytes()
+    t, to = mb.potential.fe_analytic(), W.fe_tables()
+    for k in ("f", "F", "phi"):
+        assert np.array_equal(getattr(t, k), getattr(to, k))
+    assert (t.dr, t.drho, t.cutoff) == (to.dr, to.drho, to.cutoff)
