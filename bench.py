@@ -382,10 +382,23 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
     if precision == mb.MB_PREC_FP64 and not args.no_mixed:
         mixed = mixed_comparison(args, mb, wl, box, itl, n_atoms, value / world, pg)
     sim.close()
+    n_itl = int(itl.shape[0])
+    del box, itl
+    # the batched-ensemble and serving configurations, measured in the same run
+    ensemble = serving = None
+    if world == 1 and not args.no_extras:
+        try:
+            ensemble = ensemble_measure(mb, args.steps, args.warmup)
+        except Exception as e:  # an extra figure: reported, never fatal to the bench line
+            ensemble = {"error": str(e)[:300]}
+        try:
+            serving = serve_measure(mb, args.serve_requests, max_seconds=args.serve_seconds)
+        except Exception as e:
+            serving = {"error": str(e)[:300]}
     if precision == mb.MB_PREC_FP64:
-        launches_per_step = 6 if itl.shape[0] else 2  # itl clear, itl mark, rho, itl rho, force, itl force
+        launches_per_step = 6 if n_itl else 2  # itl clear, itl mark, rho, itl rho, force, itl force
     elif rho_ms > 0:  # split: itl clear, bin, mark, rho, itl rho, force, itl force, bookkeeping
-        launches_per_step = 8 if itl.shape[0] else 3
+        launches_per_step = 8 if n_itl else 3
     else:
         launches_per_step = 1
     if rank == 0:
@@ -404,6 +417,10 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
             line["mixed"] = mixed
         if hooks is not None:
             line["hooks"] = hooks
+        if ensemble is not None:
+            line["ensemble"] = ensemble
+        if serving is not None:
+            line["serve"] = serving
         print(json.dumps(line), flush=True)
 
 
@@ -555,12 +572,16 @@ def run_nve(args, mb, world, rank, local, pg) -> None:
             "gpu_launches": None}), flush=True)
 
 
-def run_ensemble(args, mb, world, rank, local, pg) -> None:
-    """512 independent lattices (edges uniform in [8, 40] cells, seed 11; temperature
-    uniform in [300, 1200] K; 0-1% vacancies), mixed precision, every lattice advanced
-    by the same launches of each step (one CUDA graph per step); the autotuner picks
-    between the split kernels and the tile policies of the persistent kernel."""
-    mb.check(mb.lib().mb_env_init(local))
+ENSEMBLE_DESC = ("512 independent periodic BCC Fe lattices, edges uniform in [8, 40] cells (seed 11), "
+                 "300-1200 K, 0-1% vacancies, mixed precision, every lattice advanced by the same launches "
+                 "of each step (one CUDA graph per step)")
+
+
+def ensemble_measure(mb, steps: int, warmup: int, pg=None, autotune: bool = True, clocks_device=None) -> dict:
+    """The batched ensemble: 512 lattices with edges uniform in [8, 40] cells (seed 11),
+    temperature uniform in [300, 1200] K, 0-1% vacancies, mixed precision.  The
+    autotuner picks between the split kernels and the tile policies of the persistent
+    kernel; `steps` launches are timed with CUDA events (max over ranks)."""
     rng = np.random.default_rng(11)
     n_lat = 512
     edges = rng.integers(8, 41, size=(n_lat, 3))
@@ -575,20 +596,19 @@ def run_ensemble(args, mb, world, rank, local, pg) -> None:
         mb.lattice.maxwell_boltzmann(box, None, float(temps[k]), MASS, 5000 + k)
         ens.add(cells, box, steps=0)
         n_atoms += int((box["type"] >= 0).sum())
-    policy, tune_ms = ens.autotune(5)
-    ens.run(max(args.warmup, 3))
-    clocks = ClockSampler(local).start()
+    policy, tune_ms = ens.autotune(5) if autotune else (None, None)
+    ens.run(max(warmup, 3))
+    clocks = ClockSampler(clocks_device).start() if clocks_device is not None else None
     barrier(pg)
-    ms = ens.time(args.steps)
+    ms = ens.time(steps)
     barrier(pg)
-    clk = clocks.stop()
+    clk = clocks.stop() if clocks else None
     ms = reduce_max(pg, ms)
     rho_ms, force_ms, kernels = ens.kernel_times()
     info = ens.info()
     ens.close()
-    value = n_atoms * args.steps * world / (ms * 1e-3)
     peaks = measured_peaks()
-    split = policy == 4
+    split = rho_ms > 0
     if split:
         kname, kbytes, kms = "k_mx_force (mixed force + velocity-Verlet, every lattice)", BYTES_MIXED_FORCE, force_ms
     else:
@@ -601,42 +621,65 @@ def run_ensemble(args, mb, world, rank, local, pg) -> None:
     if split:
         roofline["rho_kernel"] = {"kernel": "k_mx_rho", "launch_ms": rho_ms,
                                   "achieved_gbs": BYTES_MIXED_RHO * n_atoms / (rho_ms * 1e-3) / 1e9}
+    return {"value": n_atoms * steps / (ms * 1e-3), "unit": "atom-steps/s", "ms_per_step": ms / steps,
+            "steps": steps, "lattices": n_lat, "atoms": n_atoms, "roofline": roofline, "gpu_launches": kernels * steps,
+            "kernels": "split (k_mx_rho, k_mx_force, linear item walk)" if split else
+            f"persistent k_ens_step, tile policy {policy}",
+            "autotune_best_ms_5_steps": tune_ms, "clocks": clk,
+            "l2": f"state {info['device_bytes'] / 1e6:.0f} MB > 126 MB L2 (no flush needed)",
+            "dtype": "f32 pairs + two-sum, f64 state", "workload": ENSEMBLE_DESC}
+
+
+def run_ensemble(args, mb, world, rank, local, pg) -> None:
+    mb.check(mb.lib().mb_env_init(local))
+    e = ensemble_measure(mb, args.steps, args.warmup, pg, clocks_device=local)
     if rank == 0:
         print(json.dumps({
-            "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded lattices)",
-            "config": {"workload": "ensemble_512_lattices_8to40c_mixed", "lattices": n_lat, "atoms_per_gpu": n_atoms,
-                       "kernels": "split (k_mx_rho, k_mx_force, linear item walk)" if split else
-                       f"persistent k_ens_step, tile policy {policy}",
-                       "autotune_best_ms_5_steps": tune_ms,
-                       "l2": f"state {info['device_bytes'] / 1e6:.0f} MB > 126 MB L2 (no flush needed)"},
-            "roofline": roofline,
-            "gpu_launches": kernels * args.steps, "clocks": clk, "cpu_baseline": None, "e2e": None}), flush=True)
+            "metric": "atom-steps/s", "value": e["value"] * world, "unit": "atom-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": e["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded lattices)",
+            "config": {"workload": "ensemble_512_lattices_8to40c_mixed", "lattices": e["lattices"],
+                       "atoms_per_gpu": e["atoms"], "kernels": e["kernels"],
+                       "autotune_best_ms_5_steps": e["autotune_best_ms_5_steps"], "l2": e["l2"]},
+            "roofline": e["roofline"], "gpu_launches": e["gpu_launches"], "clocks": e["clocks"],
+            "cpu_baseline": None, "e2e": None}), flush=True)
+
+
+def serve_measure(mb, n_requests: int, max_seconds: float = 600.0, clocks_device=None) -> dict:
+    """Continuous-batching serving of a Poisson request stream (50 req/s, seed 13; atoms
+    log-uniform in [1e3, 2e6], steps uniform in [100, 5000], 300-1200 K, 0-1% vacancies)
+    under a 160 GB HBM admission budget: the first n_requests requests, arriving on the
+    wall clock, each lattice built on a worker thread and uploaded when memory allows."""
+    from misa_b200 import serve
+    reqs = serve.poisson_stream(n_requests, rate=50.0, seed=13)
+    srv = serve.Server(hbm_budget_bytes=160 << 30, chunk=50)
+    clocks = ClockSampler(clocks_device).start() if clocks_device is not None else None
+    stats = srv.serve(reqs, realtime=True, max_seconds=max_seconds)
+    clk = clocks.stop() if clocks else None
+    srv.close()
+    return {"value": stats["atom_steps_per_s"], "unit": "atom-steps/s", "requests": n_requests,
+            "completed": stats["completed"], "rejected": stats["rejected"], "unfinished": stats["unfinished"],
+            "latency_p50_s": stats["latency_p50_s"], "latency_p99_s": stats["latency_p99_s"],
+            "makespan_s": stats["makespan_s"], "admit_stall_s": stats["admit_stall_s"],
+            "gpu_launches": stats["launches"], "clocks": clk, "dtype": "f32 pairs + two-sum, f64 state",
+            "workload": "Poisson 50 req/s (seed 13), atoms log-uniform [1e3, 2e6], steps uniform [100, 5000], "
+                        "300-1200 K, 0-1% vacancies, 160 GB HBM budget, continuous batching"}
 
 
 def run_serve(args, mb, world, rank, local, pg) -> None:
-    """Continuous-batching serving: Poisson arrivals at 50 req/s (seed 13), atoms
-    log-uniform in [1e3, 2e6], steps uniform in [100, 5000], 300-1200 K, 0-1%
-    vacancies, 160 GB HBM admission budget; the first --requests requests."""
-    from misa_b200 import serve
     mb.check(mb.lib().mb_env_init(local))
-    reqs = serve.poisson_stream(args.requests, rate=50.0, seed=13)
-    srv = serve.Server(hbm_budget_bytes=160 << 30, chunk=50)
-    clocks = ClockSampler(local).start()
-    stats = srv.serve(reqs, realtime=True)
-    clk = clocks.stop()
-    srv.close()
+    sv = serve_measure(mb, args.requests, clocks_device=local)
     if rank == 0:
         print(json.dumps({
-            "metric": "atom-steps/s", "value": stats["atom_steps_per_s"] * world, "unit": "atom-steps/s",
-            "n_gpus": world, "steps": stats["launches"], "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+            "metric": "atom-steps/s", "value": sv["value"] * world, "unit": "atom-steps/s",
+            "n_gpus": world, "steps": sv["gpu_launches"], "warmup": 0, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic request stream",
             "config": {"workload": "serve_poisson50_seed13", "requests": args.requests,
-                       "completed": stats["completed"], "rejected": stats["rejected"]},
-            "latency_p50_s": stats["latency_p50_s"], "latency_p99_s": stats["latency_p99_s"],
-            "makespan_s": stats["makespan_s"], "gpu_launches": stats["launches"], "clocks": clk,
-            "cpu_baseline": None, "e2e": None}), flush=True)
+                       "completed": sv["completed"], "rejected": sv["rejected"]},
+            "latency_p50_s": sv["latency_p50_s"], "latency_p99_s": sv["latency_p99_s"],
+            "makespan_s": sv["makespan_s"], "admit_stall_s": sv["admit_stall_s"], "gpu_launches": sv["gpu_launches"],
+            "clocks": sv["clocks"], "cpu_baseline": None, "e2e": None}), flush=True)
 
 
 def main() -> None:
@@ -648,7 +691,12 @@ def main() -> None:
     ap.add_argument("--config", choices=sorted(WORKLOADS) + ["ensemble", "serve", "nve"], default="scale")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
-    ap.add_argument("--requests", type=int, default=32, help="requests served by --config serve")
+    ap.add_argument("--requests", type=int, default=64, help="requests served by --config serve")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default line without the ensemble and serve objects")
+    ap.add_argument("--serve-requests", type=int, default=64, help="requests of the default line's serve object")
+    ap.add_argument("--serve-seconds", type=float, default=90.0,
+                    help="wall-time cap of the default line's serve object")
     ap.add_argument("--nve-steps", type=int, default=10000, help="steps of --config nve")
     ap.add_argument("--check-every", type=int, default=100, help="force / energy check interval of --config nve")
     ap.add_argument("--nve-precision", choices=["mixed", "fp64"], default="mixed", help="path run by --config nve")

@@ -9,6 +9,12 @@ and admits queued requests, so work arriving while others run joins the batch as
 soon as memory frees up.  Per-request completion latency and aggregate
 atom-steps/s are reported.
 
+Request preparation (building the lattice records on the host) runs on worker threads
+as soon as a request is queued, while the device advances the running lattices: the
+loop thread only uploads a prepared lattice, so a large arrival does not hold up the
+launches of the others.  The time the loop thread spends admitting requests between
+chunks is recorded (``admit_stall_s``).
+
 Host-side failure handling: malformed requests are rejected at submission; a
 request larger than the whole budget is rejected instead of queued forever; a
 request can be cancelled while queued or in flight (its slot is freed, the other
@@ -16,6 +22,7 @@ lattices are untouched).
 """
 from __future__ import annotations
 
+import concurrent.futures as cf
 import dataclasses
 import heapq
 import time
@@ -102,7 +109,10 @@ def validate_request(req: Request, budget: int) -> str:
 
 class Server:
     def __init__(self, tables: potential.EamTables | None = None, hbm_budget_bytes: int = 160 << 30,
-                 chunk: int = 50, energy_every: int = 0, keep_results: bool = False):
+                 chunk: int = 50, energy_every: int = 0, keep_results: bool = False, prep_workers: int = 2,
+                 prep_ahead: int = 4):
+        """prep_workers threads build the lattices of up to prep_ahead queued requests
+        ahead of their admission (0 workers: built on the loop thread at admission)."""
         self.tables = tables or potential.fe_analytic()
         self.budget = int(hbm_budget_bytes)
         self.ens = Ensemble(self.tables, lattice_const=A0, mass=MASS, hbm_budget_bytes=self.budget)
@@ -115,8 +125,14 @@ class Server:
         self.rejected: list[Request] = []
         self.t0 = None
         self.launches = 0
+        self.prep_ahead = max(1, prep_ahead)
+        self.pool = cf.ThreadPoolExecutor(max_workers=prep_workers) if prep_workers > 0 else None
+        self.prepared: dict[int, cf.Future] = {}
+        self.admit_stall: list[tuple[int, float]] = []  # (rid, seconds the loop thread spent admitting it)
 
     def close(self):
+        if self.pool is not None:
+            self.pool.shutdown(wait=True, cancel_futures=True)
         self.ens.close()
 
     def now(self) -> float:
@@ -131,33 +147,58 @@ class Server:
             return False
         req.status = "queued"
         self.queue.append(req)
+        self._prefetch()
         return True
+
+    def _prefetch(self) -> None:
+        if self.pool is None:
+            return
+        for req in self.queue[:self.prep_ahead]:
+            if req.rid not in self.prepared:
+                self.prepared[req.rid] = self.pool.submit(build_lattice, req)
 
     def cancel(self, req: Request) -> None:
         if req.status == "queued":
             self.queue.remove(req)
+            fut = self.prepared.pop(req.rid, None)
+            if fut is not None:
+                fut.cancel()
         elif req.status == "running":
             self.ens.remove(req.slot)
             del self.running[req.slot]
         req.status = "cancelled"
 
     def _admit(self) -> None:
+        # first come, first served: a head request whose lattice is still being built
+        # waits (the running lattices keep advancing) unless nothing else runs
         while self.queue:
             req = self.queue[0]
-            box = build_lattice(req)
+            t_in = time.perf_counter()
+            fut = self.prepared.get(req.rid)
+            if fut is None:
+                box = build_lattice(req)
+            elif fut.done() or not self.running:
+                box = fut.result()
+            else:
+                self._prefetch()
+                return
             try:
                 req.slot = self.ens.add(req.cells, box, steps=req.steps)
             except MbError as e:
                 if e.code == MB_ERR_NOMEM and self.running:
-                    return  # wait for memory to free up
+                    return  # wait for memory to free up (the prepared lattice is kept)
                 self.queue.pop(0)
+                self.prepared.pop(req.rid, None)
                 req.status, req.reason = "rejected", str(e)
                 self.rejected.append(req)
                 continue
             self.queue.pop(0)
+            self.prepared.pop(req.rid, None)
             req.status = "running"
             req.admitted = self.now()
             self.running[req.slot] = req
+            self.admit_stall.append((req.rid, time.perf_counter() - t_in))
+            self._prefetch()
 
     def _retire(self) -> None:
         for slot, req in list(self.running.items()):
@@ -201,7 +242,9 @@ class Server:
         for r in self.done:
             work += r.n_atoms * r.steps
         lat = np.array([r.latency for r in self.done]) if self.done else np.zeros(1)
+        stall = np.array([s for _, s in self.admit_stall]) if self.admit_stall else np.zeros(1)
         return {"completed": len(self.done), "rejected": len(self.rejected), "makespan_s": makespan,
                 "atom_steps": work, "atom_steps_per_s": work / makespan if makespan > 0 else 0.0,
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
-                "launches": self.launches}
+                "launches": self.launches, "admit_stall_s": {"max": float(stall.max()), "mean": float(stall.mean())},
+                "unfinished": len(self.queue) + len(self.running)}

@@ -1,6 +1,8 @@
 """Serving loop: request stream, validation, continuous batching, cancellation."""
 from __future__ import annotations
 
+import time
+
 import numpy as np
 import pytest
 
@@ -80,3 +82,22 @@ def test_budget_queues_and_faults_are_contained():
     assert len(finished) + (victim.status == "cancelled") == len(reqs)
     for r in finished[:3]:
         assert np.array_equal(r.result["x"], _alone(r)["x"])
+
+
+@pytest.mark.gpu
+def test_large_admission_is_prepared_off_the_loop_thread():
+    # small lattices run while a 2 M-atom request arrives; its lattice is built on a worker
+    # thread, so the loop thread only uploads it between chunks
+    small = serve.poisson_stream(3, rate=1000.0, seed=21, atoms=(2e3, 2e4), steps=(3000, 3000))
+    big = serve.Request(50, 0.05, serve.cells_for_atoms(2e6), 20, 600.0, 0.005, 77)
+    probe = serve.Request(51, 0.0, big.cells, 20, 600.0, 0.005, 77)
+    t = time.perf_counter()
+    serve.build_lattice(probe)
+    t_build = time.perf_counter() - t
+    srv = serve.Server(chunk=20)
+    stats = srv.serve(small + [big], realtime=True)
+    srv.close()
+    assert stats["completed"] == 4
+    stall = dict(srv.admit_stall)[big.rid]
+    assert big.admitted < max(r.finished for r in small)  # it joined while the others ran
+    assert stall < 0.3 * t_build, (stall, t_build)
