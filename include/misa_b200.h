@@ -246,6 +246,39 @@ int mb_sim_set_conversion(mb_sim *sim, double convert_distance, double recombine
  * dropped (more than 2048 in one step); *n_itl: the current interstitial count. */
 int mb_sim_conversion_stats(mb_sim *sim, int64_t *counters, int32_t *n_itl);
 
+/* ---- one lattice decomposed into z-slabs over several ranks (one GPU each)
+ * The MISA-MD host splits its lattice over MPI ranks and exchanges ghost layers between
+ * the passes: positions before rho, df before force (src/double-buffer/
+ * rho_double_buffer_imp.h:38-39 holds "the lattice atoms array in current MPI process
+ * (including ghost regions)").  A slab sim is one rank's share: box cells
+ * [z_first, z_first + z_count) of cfg->cells_z (x and y whole and periodic), FP64, no
+ * interstitials.  Its x / y ghost images are written on the device as in a whole-lattice
+ * sim; its z ghost layers come from the neighbouring slabs through device buffers the
+ * host moves (NCCL send / recv, a peer copy, ...):
+ *   after mb_sim_upload: codes (what 3) once; every step: positions (what 1), phase 0
+ *   (rho, df), df (what 2), phase 1 (forces, velocity-Verlet, drift).
+ * z_count must be at least the ghost width (2 cells for cutoff + skin = 6.3 A at
+ * a0 = 2.855 A).  Whole-lattice stepping (mb_sim_run, ...) is refused on a slab. */
+int mb_sim_create_slab(const mb_sim_config *cfg, const mb_eam_tables *pot, int32_t z_first, int32_t z_count,
+                       mb_sim **out);
+/* Bytes of one halo message of field `what`: 1 positions (3 doubles per site), 2 df
+ * (1 double), 3 site codes (1 byte); gz whole ext planes of both sublattices. */
+int mb_sim_halo_bytes(mb_sim *sim, int32_t what, int64_t *bytes);
+/* Copy this slab's lowest (side 0, for the slab below) or highest (side 1, for the slab
+ * above) gz box layers of field `what` into device_buf; returns when the copy is done. */
+int mb_sim_halo_pack(mb_sim *sim, int32_t what, int32_t side, void *device_buf);
+/* Fill the bottom (side 0, from the slab below) or top (side 1, from the slab above) gz
+ * ghost layers from device_buf; z positions get z_shift added (+-L_z across the periodic
+ * wrap between the last and the first slab).  Returns when the copy is done. */
+int mb_sim_halo_unpack(mb_sim *sim, int32_t what, int32_t side, const void *device_buf, double z_shift);
+/* Half of a timestep of an FP64 sim without interstitials (a slab, or a whole lattice):
+ * phase 0 rho / df at the current positions, phase 1 forces, the closing half kick of
+ * the previous step and the drift to the next positions.  energy != 0 on both phases of
+ * a step records this sim's (pe, ke) share of it (mb_sim_energies).  Asynchronous. */
+int mb_sim_slab_phase(mb_sim *sim, int32_t phase, int32_t energy);
+/* Drop the recorded energies (they otherwise accumulate across phase-wise steps). */
+int mb_sim_clear_energies(mb_sim *sim);
+
 /* ------------------------------------------- 3. ensembles and serving */
 
 /* Many independent periodic lattices (slots) advanced together, one persistent

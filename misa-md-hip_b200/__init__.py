@@ -85,7 +85,9 @@ class Sim:
 
     def __init__(self, cells, tables: potential.EamTables, lattice_const: float = 2.855, mass: float = 55.845,
                  dt: float = 1.0, cutoff: float | None = None, stencil_skin: float = 0.7,
-                 precision: int = MB_PREC_FP64, max_interstitials: int = 0):
+                 precision: int = MB_PREC_FP64, max_interstitials: int = 0, slab: tuple[int, int] | None = None):
+        """slab = (z_first, z_count): this sim holds only those unit cells along z of the
+        periodic lattice `cells` (one rank of a z-slab decomposition, mb_sim_create_slab)."""
         self.cells = tuple(int(c) for c in cells)
         self.lattice_const = lattice_const
         self.mass = mass
@@ -94,9 +96,15 @@ class Sim:
                                tables.cutoff if cutoff is None else cutoff, stencil_skin, max_interstitials, 0)
         t = tables.as_c()
         h = C.c_void_p()
-        check(lib().mb_sim_create(C.byref(cfg), C.byref(t), C.byref(h)))
+        if slab is None:
+            check(lib().mb_sim_create(C.byref(cfg), C.byref(t), C.byref(h)))
+            nz = self.cells[2]
+        else:
+            check(lib().mb_sim_create_slab(C.byref(cfg), C.byref(t), int(slab[0]), int(slab[1]), C.byref(h)))
+            nz = int(slab[1])
+        self.slab = slab
         self._h = h
-        self.n_box = 2 * self.cells[0] * self.cells[1] * self.cells[2]
+        self.n_box = 2 * self.cells[0] * self.cells[1] * nz
         self.n_itl = 0
         self.max_interstitials = max_interstitials
 
@@ -175,6 +183,26 @@ class Sim:
 
     def set_graphs(self, enable: bool) -> None:
         check(lib().mb_sim_set_graphs(self._h, int(enable)))
+
+    # -- z-slab decomposition (decomp.py drives these)
+    def halo_bytes(self, what: int) -> int:
+        """Bytes of one halo message: what 1 positions, 2 df, 3 site codes."""
+        b = C.c_int64()
+        check(lib().mb_sim_halo_bytes(self._h, what, C.byref(b)))
+        return b.value
+
+    def halo_pack(self, what: int, side: int, device_ptr: int) -> None:
+        check(lib().mb_sim_halo_pack(self._h, what, side, C.c_void_p(device_ptr)))
+
+    def halo_unpack(self, what: int, side: int, device_ptr: int, z_shift: float = 0.0) -> None:
+        check(lib().mb_sim_halo_unpack(self._h, what, side, C.c_void_p(device_ptr), z_shift))
+
+    def phase(self, phase: int, energy: bool = False) -> None:
+        """0: rho / df; 1: forces + velocity-Verlet + drift (mb_sim_slab_phase)."""
+        check(lib().mb_sim_slab_phase(self._h, phase, int(energy)))
+
+    def clear_energies(self) -> None:
+        check(lib().mb_sim_clear_energies(self._h))
 
     def set_conversion(self, convert_distance: float, recombine_distance: float) -> None:
         """Atoms farther than convert_distance from their site join the interstitial

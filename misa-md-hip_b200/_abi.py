@@ -132,6 +132,13 @@ SIGNATURES: dict[str, tuple] = {
     "mb_ensemble_info": (_I, [_P, _PI64, _PI64, _PI64, C.POINTER(C.c_int32)]),
     "mb_ensemble_set_graphs": (_I, [_P, _I]),
     "mb_ensemble_set_wait_limit": (_I, [_P, C.c_int64]),
+    "mb_sim_create_slab": (_I, [C.POINTER(MbSimConfig), C.POINTER(MbEamTables), C.c_int32, C.c_int32,
+                                C.POINTER(_P)]),
+    "mb_sim_halo_bytes": (_I, [_P, C.c_int32, _PI64]),
+    "mb_sim_halo_pack": (_I, [_P, C.c_int32, C.c_int32, C.c_void_p]),
+    "mb_sim_halo_unpack": (_I, [_P, C.c_int32, C.c_int32, C.c_void_p, _D]),
+    "mb_sim_slab_phase": (_I, [_P, C.c_int32, C.c_int32]),
+    "mb_sim_clear_energies": (_I, [_P]),
     "mb_ensemble_set_mode": (_I, [_P, C.c_int32]),
     "mb_ensemble_kernel_times": (_I, [_P, _PF, _PF, C.POINTER(C.c_int32)]),
 }

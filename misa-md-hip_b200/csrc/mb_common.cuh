@@ -92,6 +92,8 @@ struct Geom {
   int gcx, gy, gz; // ghost widths (cells along x)
   int bcx, by, bz; // box size per sublattice
   int images;      // 1: sites write their periodic ghost images (device-resident mode)
+  int zimg;        // with images: 1 also along z; 0 for a z-slab of a larger lattice, whose
+                   // z ghost layers come from the neighbouring slabs
   long long E;     // sites per sublattice array
   double Lx, Ly, Lz;
   double iLx, iLy, iLz; // 1 / L (0 when there is no periodic box)
@@ -213,6 +215,12 @@ int launch_pack_box_ids(const Geom &g, mb_atom_element *aos, const Lattice64 &L,
                         const double *pz, double h, int unkick, const int64_t *ids, cudaStream_t s, int z0 = 0,
                         int z1 = -1);
 int launch_df_from_rho(const Geom &g, const DevPot &pot, const Lattice64 &L, cudaStream_t s);
+// z-slab halo layers (mb_layout.cu): sites of one message, and the pack (box layers ->
+// buf) / unpack (buf -> ghost layers, z positions + z_shift) of one field: what 1 positions
+// (c0, c1, c2), 2 df (c0), 3 site codes.
+long long halo_sites(const Geom &g);
+int launch_halo(const Geom &g, int what, int pack, int side, double *c0, double *c1, double *c2, int8_t *code,
+                void *buf, double z_shift, cudaStream_t s);
 
 // Half-neighbour hook passes (mb_half.cu): a decoded half-stencil offset.
 struct HalfOff {

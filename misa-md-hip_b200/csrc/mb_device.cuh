@@ -83,7 +83,7 @@ template <class Fn>
 __device__ __forceinline__ void for_images(const Geom &g, int s, int cx, int y, int z, Fn fn) {
   const bool xo[3] = {true, cx >= g.bcx - g.gcx, cx < g.gcx};
   const bool yo[3] = {true, y >= g.by - g.gy, y < g.gy};
-  const bool zo[3] = {true, z >= g.bz - g.gz, z < g.gz};
+  const bool zo[3] = {true, g.zimg && z >= g.bz - g.gz, g.zimg && z < g.gz};
   if (!(xo[1] || xo[2] || yo[1] || yo[2] || zo[1] || zo[2])) return;
   const int xs[3] = {cx + g.gcx, cx + g.gcx - g.bcx, cx + g.gcx + g.bcx};
   const int ys[3] = {y + g.gy, y + g.gy - g.by, y + g.gy + g.by};

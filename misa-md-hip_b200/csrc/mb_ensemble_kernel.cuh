@@ -270,6 +270,7 @@ __device__ __forceinline__ Geom lat_geom(const LatDesc &d) {
   g.by = d.by;
   g.bz = d.bz;
   g.images = 1;
+  g.zimg = 1;
   g.E = d.E;
   g.Lx = d.Lx;
   g.Ly = d.Ly;

@@ -236,3 +236,63 @@ int launch_df_from_rho(const Geom &g, const DevPot &pot, const Lattice64 &L, cud
 }
 
 } // namespace mb
+
+// ------------------------------------------------------- z-slab halo layers
+// A z-slab of a larger periodic lattice (one rank of a decomposed run) gets its z ghost
+// layers from the neighbouring slabs.  A message is gz whole ext planes (both
+// sublattices, x and y ghost columns included) of one field, ordered
+// [component][sublattice][layer][y][x]: positions 3 components (double), df 1 (double),
+// site codes 1 (int8).  side 0: my lowest gz box layers (for the slab below, its top
+// ghost) / my bottom ghost layers; side 1: my highest gz box layers / my top ghost.
+// Unpacked z positions get z_shift added (the periodic wrap between the last and the
+// first slab).
+namespace mb {
+
+__global__ void k_halo(const Geom g, int what, int pack, int ez0, double *c0, double *c1, double *c2, int8_t *code,
+                       void *buf, double z_shift) {
+  const long long plane = (long long)g.ey * g.ecx;
+  const long long per_s = plane * g.gz, n = 2 * per_s;
+  const int ncomp = what == 1 ? 3 : 1;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * ncomp;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / n);
+    const long long r = t - (long long)c * n;
+    const int s = (int)(r / per_s);
+    const long long q = r - (long long)s * per_s; // layer-major inside the sublattice
+    const long long idx = (long long)s * g.E + (long long)ez0 * plane + q;
+    if (what == 3) {
+      int8_t *b = static_cast<int8_t *>(buf);
+      if (pack)
+        b[r] = code[idx];
+      else
+        code[idx] = b[r];
+    } else {
+      double *col = c == 0 ? c0 : (c == 1 ? c1 : c2);
+      double *b = static_cast<double *>(buf);
+      if (pack)
+        b[t] = col[idx];
+      else
+        col[idx] = c == 2 ? b[t] + z_shift : b[t];
+    }
+  }
+}
+
+long long halo_sites(const Geom &g) { return 2LL * g.gz * g.ey * g.ecx; }
+
+int launch_halo(const Geom &g, int what, int pack, int side, double *c0, double *c1, double *c2, int8_t *code,
+                void *buf, double z_shift, cudaStream_t s) {
+  if (what < 1 || what > 3) return fail(MB_ERR_ARG, "halo field must be 1 (positions), 2 (df) or 3 (site codes)");
+  if (side != 0 && side != 1) return fail(MB_ERR_ARG, "halo side must be 0 (below) or 1 (above)");
+  if (!buf) return fail(MB_ERR_ARG, "null halo buffer");
+  // ext z of the layers: packing reads box layers, unpacking fills ghost layers
+  const int ez0 = pack ? (side == 0 ? g.gz : g.bz) : (side == 0 ? 0 : g.bz + g.gz);
+  const long long n = halo_sites(g) * (what == 1 ? 3 : 1);
+  long long grid = (n + 255) / 256;
+  if (grid > 8LL * device_sm_count()) grid = 8LL * device_sm_count();
+  k_halo<<<(int)(grid > 0 ? grid : 1), 256, 0, s>>>(g, what, pack, ez0, c0, c1, c2, code, buf,
+                                                     what == 1 ? z_shift : 0.0);
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+} // namespace mb

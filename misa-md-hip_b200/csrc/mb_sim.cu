@@ -65,6 +65,10 @@ struct mb_sim {
   cudaStream_t cp_in = nullptr, cp_out = nullptr;
   cudaEvent_t ev_go = nullptr, ev_in[MB_SLAB_MAX] = {}, ev_out[MB_SLAB_MAX] = {};
   int host_slabs = 0; // 0: automatic (at least 4 MiB of records per slab), 1: one piece
+  // z-slab of a larger periodic lattice (one rank of a decomposed run): box layers
+  // [z_first, z_first + bz) of cells_z; z ghosts filled through mb_sim_halo_*
+  bool slab = false;
+  int z_first = 0;
   // mixed precision: the lattice lives in a one-slot ensemble (mb_ens_host.cu)
   mb_ensemble *ens = nullptr;
   int slot = -1;
@@ -299,9 +303,28 @@ using namespace mb;
 
 extern "C" {
 
+static int create_sim(const mb_sim_config *cfg, const mb_eam_tables *pot, int z_first, int z_count, mb_sim **out);
+
 int mb_sim_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **out) {
+  if (!cfg) return fail(MB_ERR_ARG, "null argument");
+  return create_sim(cfg, pot, 0, cfg->cells_z, out);
+}
+
+int mb_sim_create_slab(const mb_sim_config *cfg, const mb_eam_tables *pot, int32_t z_first, int32_t z_count,
+                       mb_sim **out) {
+  if (!cfg) return fail(MB_ERR_ARG, "null argument");
+  if (cfg->precision != MB_PREC_FP64) return fail(MB_ERR_UNSUPPORTED, "z-slab runs are FP64 only");
+  if (cfg->max_interstitials != 0)
+    return fail(MB_ERR_UNSUPPORTED, "z-slab runs take lattices without interstitials (max_interstitials = 0)");
+  if (z_first < 0 || z_count < 1 || z_first + z_count > cfg->cells_z)
+    return fail(MB_ERR_ARG, "the slab's cells [z_first, z_first + z_count) must lie inside [0, cells_z)");
+  return create_sim(cfg, pot, z_first, z_count, out);
+}
+
+static int create_sim(const mb_sim_config *cfg, const mb_eam_tables *pot, int z_first, int z_count, mb_sim **out) {
   if (!cfg || !pot || !out) return fail(MB_ERR_ARG, "null argument");
   *out = nullptr;
+  const bool slab = z_count != cfg->cells_z;
   if (cfg->cells_x < 1 || cfg->cells_y < 1 || cfg->cells_z < 1) return fail(MB_ERR_ARG, "cells must be >= 1");
   if (!(cfg->lattice_const > 0) || !(cfg->mass > 0) || !(cfg->dt > 0) || !(cfg->cutoff > 0) ||
       cfg->stencil_skin < 0)
@@ -325,6 +348,8 @@ int mb_sim_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **o
 
   mb_sim *s = new mb_sim();
   s->cfg = *cfg;
+  s->slab = slab;
+  s->z_first = z_first;
   int rc = pot_build(pot, &s->pot);
   if (rc != MB_OK) {
     delete s;
@@ -347,7 +372,7 @@ int mb_sim_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **o
   Geom &g = s->g;
   g.bcx = cfg->cells_x;
   g.by = cfg->cells_y;
-  g.bz = cfg->cells_z;
+  g.bz = z_count;
   // a doubled-x reach rx spans floor((s + dx) / 2) columns of the split layout:
   // at most ceil(rx / 2) for either sublattice
   g.gcx = (rx + 1) / 2;
@@ -356,13 +381,15 @@ int mb_sim_create(const mb_sim_config *cfg, const mb_eam_tables *pot, mb_sim **o
   if (g.bcx < g.gcx || g.by < g.gy || g.bz < g.gz) {
     pot_free(s->pot);
     delete s;
-    return fail(MB_ERR_ARG, "box smaller than the ghost width");
+    return fail(MB_ERR_ARG, slab ? "a z-slab must be at least as thick as the ghost width (the stencil's z reach)"
+                                  : "box smaller than the ghost width");
   }
   g.ecx = g.bcx + 2 * g.gcx;
   g.ey = g.by + 2 * g.gy;
   g.ez = g.bz + 2 * g.gz;
   g.E = (long long)g.ecx * g.ey * g.ez;
   g.images = 1;
+  g.zimg = slab ? 0 : 1; // a slab's z ghost layers come from its neighbours (mb_sim_halo_*)
   g.Lx = cfg->cells_x * cfg->lattice_const;
   g.Ly = cfg->cells_y * cfg->lattice_const;
   g.Lz = cfg->cells_z * cfg->lattice_const;
@@ -637,6 +664,7 @@ int mb_sim_download(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl,
 }
 
 int mb_sim_run(mb_sim *s, int32_t nsteps, int32_t energy_every) {
+  if (s && s->slab) return fail(MB_ERR_UNSUPPORTED, "a z-slab steps through mb_sim_slab_phase with halo exchanges");
   if (s && s->ens) {
     MB_TRY(mixed_need_slot(s));
     MB_TRY(mb_ensemble_clear_energies(s->ens, s->slot));
@@ -688,6 +716,7 @@ int mb_sim_energies(mb_sim *s, double *out, int32_t cap, int32_t *n) {
 }
 
 int mb_sim_time_steps(mb_sim *s, int32_t nsteps, float *ms) {
+  if (s && s->slab) return fail(MB_ERR_UNSUPPORTED, "a z-slab steps through mb_sim_slab_phase with halo exchanges");
   if (s && s->ens) {
     MB_TRY(mixed_need_slot(s));
     return mb_ensemble_time(s->ens, nsteps, ms);
@@ -704,6 +733,7 @@ int mb_sim_time_steps(mb_sim *s, int32_t nsteps, float *ms) {
 }
 
 int mb_sim_kernel_times(mb_sim *s, float *rho_ms, float *force_ms) {
+  if (s && s->slab) return fail(MB_ERR_UNSUPPORTED, "a z-slab steps through mb_sim_slab_phase with halo exchanges");
   if (s && s->ens) { // split kernels: each pass timed; persistent kernel: the whole step
     MB_TRY(mixed_need_slot(s));
     return mb_ensemble_kernel_times(s->ens, rho_ms, force_ms, nullptr);
@@ -871,6 +901,7 @@ static int step_host_slabs(mb_sim *s, mb_atom_element *box_atoms, mb_atom_elemen
 }
 
 int mb_sim_step_host(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t n_itl) {
+  if (s && s->slab) return fail(MB_ERR_UNSUPPORTED, "a z-slab steps through mb_sim_slab_phase with halo exchanges");
   if (!s || !box_atoms) return fail(MB_ERR_ARG, "null argument");
   if (s->cfg.precision != MB_PREC_FP64) return fail(MB_ERR_UNSUPPORTED, "host-buffer steps run the FP64 path");
   MB_TRY(ensure_stage(s, (size_t)s->n_box));
@@ -898,6 +929,7 @@ int mb_sim_host_slabs(mb_sim *s, int32_t *n_slabs) {
 }
 
 int mb_sim_set_conversion(mb_sim *s, double convert_distance, double recombine_distance) {
+  if (s && s->slab) return fail(MB_ERR_UNSUPPORTED, "a z-slab steps through mb_sim_slab_phase with halo exchanges");
   if (s && s->ens) {
     MB_TRY(mixed_need_slot(s));
     return mb_ensemble_set_conversion(s->ens, convert_distance, recombine_distance);
@@ -950,6 +982,70 @@ int mb_sim_set_graphs(mb_sim *s, int enable) {
   if (!s) return fail(MB_ERR_ARG, "null sim");
   s->use_graphs = enable != 0;
   if (!s->use_graphs) drop_graph(s);
+  return MB_OK;
+}
+
+// ------------------------------------------------------------------ z-slab runs
+// One rank's share of a lattice decomposed into z-slabs (mb_sim_create_slab): the host
+// moves ghost layers between neighbouring slabs around each pass.
+
+int mb_sim_halo_bytes(mb_sim *s, int32_t what, int64_t *bytes) {
+  if (!s || !bytes || s->ens) return fail(MB_ERR_ARG, "bad arguments");
+  if (what < 1 || what > 3) return fail(MB_ERR_ARG, "halo field must be 1 (positions), 2 (df) or 3 (site codes)");
+  const long long n = halo_sites(s->g);
+  *bytes = (int64_t)(what == 1 ? 3 * n * (long long)sizeof(double) : what == 2 ? n * (long long)sizeof(double) : n);
+  return MB_OK;
+}
+
+static int halo(mb_sim *s, int what, int pack, int side, void *buf, double z_shift) {
+  if (!s || s->ens) return fail(MB_ERR_ARG, "bad arguments");
+  if (!s->slab) return fail(MB_ERR_STATE, "halo layers belong to z-slab runs (mb_sim_create_slab)");
+  double *c0 = what == 1 ? s->pos[s->cur][0] : s->df, *c1 = s->pos[s->cur][1], *c2 = s->pos[s->cur][2];
+  MB_TRY(launch_halo(s->g, what, pack, side, c0, c1, c2, s->code, buf, z_shift, s->stream));
+  MB_CUDA(cudaStreamSynchronize(s->stream));
+  return MB_OK;
+}
+
+int mb_sim_halo_pack(mb_sim *s, int32_t what, int32_t side, void *device_buf) {
+  return halo(s, what, 1, side, device_buf, 0.0);
+}
+
+int mb_sim_halo_unpack(mb_sim *s, int32_t what, int32_t side, const void *device_buf, double z_shift) {
+  return halo(s, what, 0, side, const_cast<void *>(device_buf), z_shift);
+}
+
+int mb_sim_slab_phase(mb_sim *s, int32_t phase, int32_t energy) {
+  if (!s || s->ens) return fail(MB_ERR_ARG, "bad arguments");
+  if (phase != 0 && phase != 1) return fail(MB_ERR_ARG, "phase must be 0 (rho) or 1 (force + integration)");
+  if (s->n_itl > 0 || s->conv_d > 0.0)
+    return fail(MB_ERR_UNSUPPORTED, "phase-wise steps take lattices without interstitials");
+  const DevPot &P = pot_dev(s->pot);
+  Lattice64 L = sim_lattice(s, s->cur);
+  double *ep = energy ? s->epart : nullptr;
+  if (phase == 0) {
+    if (energy) MB_CUDA(cudaMemsetAsync(s->epart, 0, sizeof(double) * energy_partials_needed(), s->stream));
+    MB_TRY(launch_rho64(s->g, s->st, P, L, s->cfg.cutoff * s->cfg.cutoff, ep, energy, 0, s->stream));
+    return MB_OK;
+  }
+  // forces at pos[cur], closing kick of the previous step (once primed), drift to pos[cur ^ 1]
+  const StepParams sp = sim_params(s, s->primed ? 1 : 0, 1);
+  MB_TRY(launch_force64(s->g, s->st, P, L, sp, ep, energy, 0, s->stream));
+  const long long n = s->primed ? s->step + 1 : 0;
+  s->step = n;
+  if (energy) {
+    if (s->n_e == 0) s->e_steps.clear();
+    MB_TRY(record_energy(s));
+  }
+  s->primed = true;
+  s->cur ^= 1;
+  return MB_OK;
+}
+
+int mb_sim_clear_energies(mb_sim *s) {
+  if (!s) return fail(MB_ERR_ARG, "null sim");
+  if (s->ens) return mb_ensemble_clear_energies(s->ens, s->slot);
+  s->n_e = 0;
+  s->e_steps.clear();
   return MB_OK;
 }
 
