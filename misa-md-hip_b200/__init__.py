@@ -204,6 +204,13 @@ class Sim:
     def clear_energies(self) -> None:
         check(lib().mb_sim_clear_energies(self._h))
 
+    def reach(self) -> tuple[float, int]:
+        """(bound on the lattice atoms' displacement from their sites, -1 if unknown;
+        stencil entries the lattice passes walk now) (mb_sim_reach)."""
+        u, n = C.c_double(), C.c_int32()
+        check(lib().mb_sim_reach(self._h, C.byref(u), C.byref(n)))
+        return u.value, n.value
+
     def set_conversion(self, convert_distance: float, recombine_distance: float) -> None:
         """Atoms farther than convert_distance from their site join the interstitial
         list after each step; interstitials within recombine_distance of a vacant site

@@ -20,6 +20,14 @@ __device__ __forceinline__ void spl_locate(double x, double rdx, int n, int &m, 
   p = fmin(pp - (double)mm, 1.0);
   m = mm;
 }
+// spl_locate for x inside the table's range (x < (n - 1) / rdx, which every pair inside
+// a cutoff within the table satisfies): the same m and p there; past the range m is
+// clamped and p is meaningless, for terms the caller masks out.
+__device__ __forceinline__ void spl_locate_in(double x, double rdx, int n, int &m, double &p) {
+  const double pp = x * rdx;
+  m = min((int)pp, n - 2);
+  p = pp - (double)m;
+}
 __device__ __forceinline__ double cubic(const double4 c, double p) { return ((c.w * p + c.z) * p + c.y) * p + c.x; }
 __device__ __forceinline__ double quad(const double4 d, double p) { return (d.z * p + d.y) * p + d.x; }
 __device__ __forceinline__ int pair_idx(int a, int b, int nt) {
@@ -124,6 +132,36 @@ __device__ __forceinline__ double block_sum(double v) {
   if (threadIdx.x == 0)
     for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += red[k];
   return t;
+}
+
+// Deterministic block maximum of non-negative values; result in thread 0.
+__device__ __forceinline__ double block_max(double v) {
+  __shared__ double red_max[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red_max[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t = fmax(t, red_max[k]);
+  return t;
+}
+
+// Raises *umax (bits of a non-negative double) to at least u.
+__device__ __forceinline__ void raise_umax(unsigned long long *umax, double u) {
+  atomicMax(umax, (unsigned long long)__double_as_longlong(u));
+}
+
+// Stencil entries a lattice pass walks: all of them, or (with a displacement bound) only
+// those that can reach inside the cutoff while every atom stays within *umax of its site.
+__device__ __forceinline__ int stencil_in_reach(const StencilSet &st, const unsigned long long *umax) {
+  if (!umax) return st.n;
+  const double u = __longlong_as_double((long long)*umax);
+  int n = st.n_near;
+  while (n < st.n && !(u < st.skip_u[n])) n++;
+  return n;
 }
 
 struct Window {

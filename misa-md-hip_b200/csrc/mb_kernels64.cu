@@ -23,6 +23,7 @@
 //    velocity-Verlet step and drifts to the next positions (double-buffered).
 #include <limits.h>
 #include <stdio.h>
+#include <stdlib.h>
 
 #include "mb_common.cuh"
 #include "mb_device.cuh"
@@ -59,6 +60,42 @@ __device__ __forceinline__ void conv_check(const Geom &g, const StepParams &sp, 
 
 int energy_partials_needed() { return 8 * MB_EPART_CAP; }
 
+// Work items of the lattice passes: 32 consecutive sites (one x chunk) of one row.
+// Rows walk (by == 0): chunk fastest, then y, sublattice, z; a z-slab of the box is a
+// contiguous item range.  Brick walk (by > 0): the items of one brick (one chunk, by rows,
+// bz planes, both sublattices: y fastest, then sublattice, then z) are consecutive, so the
+// warps of a CTA work on neighbouring rows at once and share their neighbour rows in L1.
+struct ItemWalk {
+  int chunks;       // x chunks per row
+  int by, bz;       // brick rows / planes (by == 0: rows walk)
+  int nyb;          // bricks along y
+};
+
+__device__ __forceinline__ bool decode_item(const Geom &g, const ItemWalk &wk, long long w, int &chunk, int &y,
+                                            int &s, int &z) {
+  if (wk.by == 0) {
+    long long t = w;
+    chunk = (int)(t % wk.chunks);
+    t /= wk.chunks;
+    y = (int)(t % g.by);
+    t /= g.by;
+    s = (int)(t & 1);
+    z = (int)(t >> 1);
+    return true;
+  }
+  const int per = 2 * wk.by * wk.bz;
+  const long long b = w / per;
+  const int j = (int)(w - b * per);
+  const int dy = j % wk.by, q = j / wk.by;
+  s = q & 1;
+  const int dz = q >> 1;
+  chunk = (int)(b % wk.chunks);
+  const long long r = b / wk.chunks;
+  y = (int)(r % wk.nyb) * wk.by + dy;
+  z = (int)(r / wk.nyb) * wk.bz + dz;
+  return y < g.by && z < g.bz;
+}
+
 // -------------------------------------------------------------- rho pass
 struct RhoArgs {
   Geom g;
@@ -68,8 +105,8 @@ struct RhoArgs {
   double *e_partial;
   int skip_flagged;
   int m_lo;      // first knot kept in shared memory
-  int chunks;    // 32-site chunks per row
-  long long w0, n_items; // items [w0, n_items): a z-slab of the box (z slowest)
+  ItemWalk walk;
+  long long w0, n_items; // items [w0, n_items): a z-slab of the box (z slowest) or every brick
 };
 
 // One density term of a one-type lattice.  BF (branch-free): the stencil entry lies
@@ -85,7 +122,7 @@ __device__ __forceinline__ double rho_term(const RhoArgs &a, const Lattice64 &L,
   const double r = d2 * rsqrt(d2);
   int m;
   double p;
-  spl_locate(r, a.P.rdr, a.P.nr, m, p);
+  spl_locate_in(r, a.P.rdr, a.P.nr, m, p);
   double4 c;
   if (m >= a.m_lo) {
     const int k = m - a.m_lo, b = (k >> 2) & 1; // halves swapped on every other group of 4 knots
@@ -121,15 +158,13 @@ __global__ void __launch_bounds__(MB_RHO_THREADS, 1)
   const int lane = threadIdx.x & 31;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
   double e_acc = 0.0;
+  // the force passes of this step raise the bound of the drifted positions from zero
+  if (L.umax_next && blockIdx.x == 0 && threadIdx.x == 0) *L.umax_next = 0ull;
+  const int n_use = ONE_TYPE ? stencil_in_reach(st, L.umax) : st.n;
   for (long long w = a.w0 + (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.n_items;
        w += wstride) {
-    long long t = w;
-    const int chunk = (int)(t % a.chunks);
-    t /= a.chunks;
-    const int y = (int)(t % g.by);
-    t /= g.by;
-    const int s = (int)(t & 1);
-    const int z = (int)(t >> 1);
+    int chunk, y, s, z;
+    if (!decode_item(g, a.walk, w, chunk, y, s, z)) continue;
     const int cx = chunk * 32 + lane;
     if (cx >= g.bcx) continue;
     const long long i = ext_index(g, s, cx, y, z);
@@ -148,7 +183,7 @@ __global__ void __launch_bounds__(MB_RHO_THREADS, 1)
       }
       if (k < st.n_near) r0 += rho_term<true>(a, L, s_f2, i + off[k++], xi, yi, zi);
 #pragma unroll 2
-      for (; k < st.n; k++) r1 += rho_term<false>(a, L, s_f2, i + off[k], xi, yi, zi);
+      for (; k < n_use; k++) r1 += rho_term<false>(a, L, s_f2, i + off[k], xi, yi, zi);
       rho = r0 + r1;
     } else {
 #pragma unroll 4
@@ -188,7 +223,7 @@ struct ForceArgs {
   double *e_kin;     // CTA partials of kinetic energy
   int skip_flagged;
   int m_lo;
-  int chunks;
+  ItemWalk walk;
   long long w0, n_items; // items [w0, n_items)
 };
 
@@ -206,7 +241,7 @@ __device__ __forceinline__ void force_term(const ForceArgs &a, const Lattice64 &
   const double dfj = L.df[j];
   int m;
   double p;
-  spl_locate(r, a.P.rdr, a.P.nr, m, p);
+  spl_locate_in(r, a.P.rdr, a.P.nr, m, p);
   double2 c0, c1, c2;
   if (m >= a.m_lo) {
     const double2 *q = s_f1 + (size_t)(m - a.m_lo) * 3;
@@ -248,15 +283,13 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
   const int lane = threadIdx.x & 31;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
   double e_pair = 0.0, e_kin = 0.0;
+  double u2max = 0.0; // squared displacement of the drifted atoms from their sites
+  const bool track_u = L.umax_next && sp.drift;
+  const int n_use = ONE_TYPE ? stencil_in_reach(st, L.umax) : st.n;
   for (long long w = a.w0 + (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.n_items;
        w += wstride) {
-    long long t = w;
-    const int chunk = (int)(t % a.chunks);
-    t /= a.chunks;
-    const int y = (int)(t % g.by);
-    t /= g.by;
-    const int s = (int)(t & 1);
-    const int z = (int)(t >> 1);
+    int chunk, y, s, z;
+    if (!decode_item(g, a.walk, w, chunk, y, s, z)) continue;
     const int cx = chunk * 32 + lane;
     if (cx >= g.bcx) continue;
     const long long i = ext_index(g, s, cx, y, z);
@@ -284,7 +317,7 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
       }
       if (k < st.n_near) force_term<ENERGY, true>(a, L, s_f1, i + off[k++], xi, yi, zi, dfi, fx, fy, fz, ep);
 #pragma unroll 2
-      for (; k < st.n; k++) force_term<ENERGY, false>(a, L, s_f1, i + off[k], xi, yi, zi, dfi, gx, gy, gz, eq);
+      for (; k < n_use; k++) force_term<ENERGY, false>(a, L, s_f1, i + off[k], xi, yi, zi, dfi, gx, gy, gz, eq);
       fx += gx;
       fy += gy;
       fz += gz;
@@ -332,6 +365,12 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
         L.ny[i] = ny;
         L.nz[i] = nz;
         conv_check(g, sp, s, cx, y, z, nx, ny, nz);
+        if (track_u) {
+          double X, Y, Z;
+          site_ideal(s, cx, y, z, sp.a0, X, Y, Z);
+          const double ux = nx - X, uy = ny - Y, uz = nz - Z;
+          u2max = fmax(u2max, ux * ux + uy * uy + uz * uz);
+        }
         if (g.images)
           for_images(g, s, cx, y, z, [&](long long idx, double ox, double oy, double oz) {
             L.nx[idx] = nx + ox;
@@ -351,6 +390,10 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
     const double t2 = block_sum(e_kin);
     if (threadIdx.x == 0) a.e_kin[blockIdx.x] = t2;
   }
+  if (track_u) {
+    const double t = block_max(u2max);
+    if (threadIdx.x == 0) raise_umax(L.umax_next, sqrt(t));
+  }
 }
 
 // ----------------------------------------------------------- launchers
@@ -362,6 +405,42 @@ static int grid_for(long long warps_needed, int threads) {
 }
 
 static const int kSmemCap = 200 * 1024;
+
+// Brick shapes (rows, planes) of the whole-box launches; {0, 0}: rows walk.  The
+// environment variables MB_RHO_BRICK / MB_FORCE_BRICK ("rows,planes") override them.
+static int kRhoBrick[2] = {0, 0}, kForceBrick[2] = {0, 0};
+
+static void brick_override(const char *name, int *shape) {
+  const char *v = getenv(name);
+  int by = 0, bz = 0;
+  if (v && sscanf(v, "%d,%d", &by, &bz) == 2 && by >= 0 && bz >= 0 && by <= 64 && bz <= 64) {
+    shape[0] = by;
+    shape[1] = bz;
+  }
+}
+
+static void set_walk(const Geom &g, int z0, int z1, const int *brick, ItemWalk &wk, long long &w0, long long &n1) {
+  static bool read = false;
+  if (!read) {
+    brick_override("MB_RHO_BRICK", kRhoBrick);
+    brick_override("MB_FORCE_BRICK", kForceBrick);
+    read = true;
+  }
+  wk.chunks = (g.bcx + 31) / 32;
+  const bool whole = z0 == 0 && z1 == g.bz;
+  if (whole && brick[0] > 0 && brick[1] > 0) {
+    wk.by = brick[0];
+    wk.bz = brick[1];
+    wk.nyb = (g.by + wk.by - 1) / wk.by;
+    const long long nzb = (g.bz + wk.bz - 1) / wk.bz;
+    w0 = 0;
+    n1 = (long long)wk.chunks * wk.nyb * nzb * 2 * wk.by * wk.bz;
+    return;
+  }
+  wk.by = wk.bz = wk.nyb = 0;
+  w0 = (long long)wk.chunks * g.by * 2 * z0;
+  n1 = (long long)wk.chunks * g.by * 2 * z1;
+}
 
 // Knots kept in shared memory: those at r >= 0.3 cutoff (lattice neighbours sit near
 // 0.45 cutoff and beyond; closer pairs read the global table), within kSmemCap, so
@@ -384,15 +463,15 @@ int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const L
   a.rc2 = rc2;
   a.e_partial = e_partial;
   a.skip_flagged = skip_flagged;
-  const bool one = pot.n_types == 1;
+  // the one-type kernels locate spline intervals without range clamps: every pair
+  // inside the cutoff must lie inside the table
+  const bool one = pot.n_types == 1 && rc2 <= (double)(pot.nr - 1) * (pot.nr - 1) / (pot.rdr * pot.rdr);
   int nsm = smem_knots(pot, (int)sizeof(double4));
   if (!one) nsm = 0;
   a.m_lo = pot.nr - nsm;
-  a.chunks = (g.bcx + 31) / 32;
   if (z1 < 0) z1 = g.bz;
   if (z0 < 0 || z0 >= z1 || z1 > g.bz) return z0 == z1 ? MB_OK : fail(MB_ERR_ARG, "z-slab outside the box");
-  a.w0 = (long long)a.chunks * g.by * 2 * z0;
-  a.n_items = (long long)a.chunks * g.by * 2 * z1;
+  set_walk(g, z0, z1, kRhoBrick, a.walk, a.w0, a.n_items);
   const size_t smem = (size_t)nsm * sizeof(double4);
   const int grid = grid_for(a.n_items - a.w0, MB_RHO_THREADS);
   static bool attr_done = false;
@@ -426,15 +505,13 @@ int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const
   a.e_pair = e_partial ? e_partial + MB_EPART_CAP : nullptr;
   a.e_kin = e_partial ? e_partial + 2 * MB_EPART_CAP : nullptr;
   a.skip_flagged = skip_flagged;
-  const bool one = pot.n_types == 1;
+  const bool one = pot.n_types == 1 && sp.rc2 <= (double)(pot.nr - 1) * (pot.nr - 1) / (pot.rdr * pot.rdr);
   int nsm = smem_knots(pot, (int)(3 * sizeof(double2)));
   if (!one) nsm = 0;
   a.m_lo = pot.nr - nsm;
-  a.chunks = (g.bcx + 31) / 32;
   if (z1 < 0) z1 = g.bz;
   if (z0 < 0 || z0 >= z1 || z1 > g.bz) return z0 == z1 ? MB_OK : fail(MB_ERR_ARG, "z-slab outside the box");
-  a.w0 = (long long)a.chunks * g.by * 2 * z0;
-  a.n_items = (long long)a.chunks * g.by * 2 * z1;
+  set_walk(g, z0, z1, kForceBrick, a.walk, a.w0, a.n_items);
   const size_t smem = (size_t)nsm * 3 * sizeof(double2);
   const int grid = grid_for(a.n_items - a.w0, MB_FORCE_THREADS);
   static bool attr_done = false;
@@ -701,6 +778,12 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
             L.ny[i] = ny;
             L.nz[i] = nz;
             conv_check(g, sp, s, cx, y, z, nx, ny, nz);
+            if (L.umax_next) {
+              double X, Y, Z;
+              site_ideal(s, cx, y, z, sp.a0, X, Y, Z);
+              const double ux = nx - X, uy = ny - Y, uz = nz - Z;
+              raise_umax(L.umax_next, sqrt(ux * ux + uy * uy + uz * uz));
+            }
             if (g.images)
               for_images(g, s, cx, y, z, [&](long long idx, double ox, double oy, double oz) {
                 L.nx[idx] = nx + ox;
