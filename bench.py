@@ -682,13 +682,65 @@ def run_serve(args, mb, world, rank, local, pg) -> None:
             "clocks": sv["clocks"], "cpu_baseline": None, "e2e": None}), flush=True)
 
 
+def run_decomp(args, mb, world, rank, local, pg) -> None:
+    """One 128^3-cell lattice (0.5% vacancies, seed 7, 300 K; no interstitials: slabs hold
+    none) split into z-slabs over the N ranks (strong scaling): every step exchanges the
+    ghost layers of positions and of df with the neighbouring ranks (NCCL point-to-point
+    on device buffers, misa_b200.decomp) around the rho and force phases.  Timed on the
+    wall clock between synchronised points (exchanges and their host synchronisations
+    included), max over ranks."""
+    import torch
+
+    from misa_b200 import decomp
+    mb.check(mb.lib().mb_env_init(local))
+    wl = dict(WORKLOADS["scale"], n_itl=0)
+    box, _ = build_state(mb, wl)
+    n_atoms = int((box["type"] >= 0).sum())
+    dev = torch.device("cuda", local) if torch.cuda.is_available() else None
+    bufs = lambda n: torch.empty(n, dtype=torch.uint8, device=dev)  # noqa: E731
+    r = decomp.SlabRank(wl["cells"], mb.potential.fe_analytic(), rank, world, bufs, lattice_const=A0, mass=MASS,
+                        dt=DT, cutoff=RC, stencil_skin=SKIN)
+    ex = decomp.TorchExchange(pg, rank, world) if world > 1 else None
+    sync = torch.cuda.synchronize if dev is not None else None
+    try:
+        r.upload(box)
+        decomp.exchange_codes([r], ex, sync)
+        for _ in range(max(args.warmup, 3)):
+            decomp.step_all([r], ex, sync=sync)
+        r.sim.sync()
+        clocks = ClockSampler(local).start()
+        barrier(pg)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            decomp.step_all([r], ex, sync=sync)
+        r.sim.sync()
+        dt = time.perf_counter() - t0
+        barrier(pg)
+        clk = clocks.stop()
+    finally:
+        r.close()
+    dt = reduce_max(pg, dt)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "atom-steps/s", "value": n_atoms * args.steps / dt, "unit": "atom-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded lattice, analytic tabulated potential)",
+            "config": {"workload": "fe_bcc_128c_vac0.5pct_300K_fp64_zslabs", "cells": list(wl["cells"]),
+                       "atoms": n_atoms, "slabs": r.parts,
+                       "timing": "wall clock between synchronised points, ghost-layer exchanges included"},
+            # rho and force per step, plus 4 halo packs and 4 unpacks when the slabs exchange
+            "gpu_launches": (2 + (8 if world > 1 else 0)) * args.steps, "clocks": clk, "cpu_baseline": None,
+            "e2e": None}), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=sorted(WORKLOADS) + ["ensemble", "serve", "nve"], default="scale")
+    ap.add_argument("--config", choices=sorted(WORKLOADS) + ["ensemble", "serve", "nve", "decomp"], default="scale")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     ap.add_argument("--requests", type=int, default=64, help="requests served by --config serve")
@@ -728,6 +780,8 @@ def main() -> None:
             run_serve(args, mb, world, rank, local, pg)
         elif args.config == "nve":
             run_nve(args, mb, world, rank, local, pg)
+        elif args.config == "decomp":
+            run_decomp(args, mb, world, rank, local, pg)
         else:
             run_ours(args, mb, wl, world, rank, local, pg)
     finally:

@@ -204,6 +204,10 @@ class Sim:
     def clear_energies(self) -> None:
         check(lib().mb_sim_clear_energies(self._h))
 
+    def sync(self) -> None:
+        """Wait for the sim's queued device work (mb_sim_sync)."""
+        check(lib().mb_sim_sync(self._h))
+
     def reach(self) -> tuple[float, int]:
         """(bound on the lattice atoms' displacement from their sites, -1 if unknown;
         stencil entries the lattice passes walk now) (mb_sim_reach)."""
