@@ -4,6 +4,8 @@
 // serving loop builds continuous batching on.
 #include <cudaTypedefs.h>
 #include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -535,7 +537,7 @@ static int rebuild(mb_ensemble *e) {
       }
       first[nl] = (unsigned)n_items;
     } else {
-      n_items = (unsigned long long)W.n_units * MX_BRICK_ITEMS;
+      n_items = (unsigned long long)W.n_units * W.bitems;
     }
       if (n_items >= (1ull << 31)) return fail(MB_ERR_ARG, "too many sites for the 32-bit item walk");
     W.n_items = (unsigned)n_items;
@@ -639,11 +641,23 @@ static const char *mx_stencil(const mb_ensemble *e, const LatDesc &d, MxStencil 
   if (S.n_odd == 0 || S.n_even == 0) return "split stencil has an empty branch-free class";
   pad(S.odd, S.n_odd);
   pad(S.even, S.n_even);
-  // brick walk
-  const unsigned chunks = (unsigned)((d.bcx + 31) / 32), nyb = (unsigned)((d.by + MX_BY - 1) / MX_BY),
-                 nzb = (unsigned)((d.bz + MX_BZ - 1) / MX_BZ);
+  // brick walk (shape MX_BY x MX_BZ; the environment variable MB_MX_BRICK = "rows,planes"
+  // overrides it, for tuning)
+  unsigned bby = MX_BY, bbz = MX_BZ;
+  if (const char *v = getenv("MB_MX_BRICK")) {
+    unsigned a = 0, b = 0;
+    if (sscanf(v, "%u,%u", &a, &b) == 2 && a >= 1 && b >= 1 && a <= 32 && b <= 32) {
+      bby = a;
+      bbz = b;
+    }
+  }
+  const unsigned chunks = (unsigned)((d.bcx + 31) / 32), nyb = (unsigned)((d.by + bby - 1) / bby),
+                 nzb = (unsigned)((d.bz + bbz - 1) / bbz);
   const unsigned long long units = (unsigned long long)chunks * nyb * nzb;
-  if (units * MX_BRICK_ITEMS >= (1ull << 31)) return "lattice too large for the 32-bit brick walk";
+  if (units * 2 * bby * bbz >= (1ull << 31)) return "lattice too large for the 32-bit brick walk";
+  S.walk.by = bby;
+  S.walk.bz = bbz;
+  S.walk.bitems = 2 * bby * bbz;
   S.walk.chunks = chunks;
   S.walk.m_chunks = 0xFFFFFFFFu / chunks;
   S.walk.nyb = nyb;

@@ -134,10 +134,10 @@ struct MxEntry {
 // walks one contiguous range of the concatenated items.
 #define MX_BY 8
 #define MX_BZ 8
-#define MX_BRICK_ITEMS (2 * MX_BY * MX_BZ)
 struct MxWalk {
   int linear;                // 0: bricks of lattice `lat`; 1: linear items over every lattice
   unsigned chunks, m_chunks; // x chunks per row and floor((2^32 - 1) / chunks)
+  unsigned by, bz, bitems;   // brick rows, planes and items (2 by bz; MX_BY, MX_BZ unless overridden)
   unsigned nyb, m_nyb;       // y bricks
   unsigned n_units;          // bricks
   // linear walk: item = 32 consecutive sites of one (z, sublattice) plane of a lattice,

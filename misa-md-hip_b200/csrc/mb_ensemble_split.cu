@@ -37,15 +37,15 @@ __device__ __forceinline__ unsigned fdiv(unsigned n, unsigned d, unsigned m, uns
   return q;
 }
 
-// Item it (0 .. MX_BRICK_ITEMS - 1) of brick `unit`: a row chunk of 32 sites, lane = x.
+// Item it (0 .. W.bitems - 1) of brick `unit`: a row chunk of 32 sites, lane = x.
 __device__ __forceinline__ bool mx_site(const LatDesc &d, const MxWalk &W, unsigned unit, unsigned it, int lane,
                                         int &s, int &cx, int &y, int &z, long long &i) {
   unsigned chunk, yb;
   const unsigned t = fdiv(unit, W.chunks, W.m_chunks, chunk);
   const unsigned zb = fdiv(t, W.nyb, W.m_nyb, yb);
-  y = (int)(yb * MX_BY + it % MX_BY);
-  s = (int)((it / MX_BY) & 1u);
-  z = (int)(zb * MX_BZ + it / (2 * MX_BY));
+  y = (int)(yb * W.by + it % W.by);
+  s = (int)((it / W.by) & 1u);
+  z = (int)(zb * W.bz + it / (2 * W.by));
   cx = (int)chunk * 32 + lane;
   if (cx >= d.bcx || y >= d.by || z >= d.bz) return false;
   i = (long long)s * d.E + ((long long)(z + 2) * d.ey + y + 2) * d.ecx + cx + 2;
@@ -125,7 +125,7 @@ __device__ __forceinline__ bool mx_locate(const EnsParams &P, const MxWalk &W, i
                                           MxAt &at, int &s, int &cx, int &y, int &z, long long &i) {
   if constexpr (WALK == 0) {
     at.l = lat;
-    return mx_site(P.lats[lat], W, item / MX_BRICK_ITEMS, item % MX_BRICK_ITEMS, lane, s, cx, y, z, i);
+    return mx_site(P.lats[lat], W, item / W.bitems, item % W.bitems, lane, s, cx, y, z, i);
   } else {
     if (item < at.lo || item >= at.hi) { // binary search of the owning lattice
       int a = 0, b = W.n_lats;
@@ -167,12 +167,12 @@ __device__ __forceinline__ void mx_items(const MxWalk &W, unsigned &first, unsig
 }
 
 // Brick walk: the k-th item of this block (k = warp, warp + warps, ...) is item it of
-// brick blockIdx.x + (k / MX_BRICK_ITEMS) * grid.  Returns the walk item or ~0u at the end.
+// brick blockIdx.x + (k / W.bitems) * grid.  Returns the walk item or ~0u at the end.
 template <int WALK>
 __device__ __forceinline__ unsigned mx_next(const MxWalk &W, unsigned k, unsigned first, unsigned count) {
   if constexpr (WALK == 0) {
-    const unsigned unit = blockIdx.x + (k / MX_BRICK_ITEMS) * gridDim.x;
-    return unit < W.n_units ? unit * MX_BRICK_ITEMS + k % MX_BRICK_ITEMS : ~0u;
+    const unsigned unit = blockIdx.x + (k / W.bitems) * gridDim.x;
+    return unit < W.n_units ? unit * W.bitems + k % W.bitems : ~0u;
   } else {
     return k < count ? first + k : ~0u;
   }
