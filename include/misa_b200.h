@@ -278,13 +278,6 @@ int mb_sim_halo_unpack(mb_sim *sim, int32_t what, int32_t side, const void *devi
 int mb_sim_slab_phase(mb_sim *sim, int32_t phase, int32_t energy);
 /* Drop the recorded energies (they otherwise accumulate across phase-wise steps). */
 int mb_sim_clear_energies(mb_sim *sim);
-/* FP64 device-resident runs bound the largest displacement of a lattice atom from its
- * site after every drift; the lattice passes then walk only the stencil entries that can
- * still reach inside the cutoff (ordered by ideal distance R_k, entry k is left out
- * while 2 * umax < R_k - cutoff: every result is the same as with the whole stencil).
- * *umax: the bound at the current positions (-1 when unknown: after an upload, a
- * host-buffer step, with conversions); *entries: the stencil entries walked now. */
-int mb_sim_reach(mb_sim *sim, double *umax, int32_t *entries);
 
 /* ------------------------------------------- 3. ensembles and serving */
 

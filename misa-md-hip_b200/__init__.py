@@ -208,12 +208,6 @@ class Sim:
         """Wait for the sim's queued device work (mb_sim_sync)."""
         check(lib().mb_sim_sync(self._h))
 
-    def reach(self) -> tuple[float, int]:
-        """(bound on the lattice atoms' displacement from their sites, -1 if unknown;
-        stencil entries the lattice passes walk now) (mb_sim_reach)."""
-        u, n = C.c_double(), C.c_int32()
-        check(lib().mb_sim_reach(self._h, C.byref(u), C.byref(n)))
-        return u.value, n.value
 
     def set_conversion(self, convert_distance: float, recombine_distance: float) -> None:
         """Atoms farther than convert_distance from their site join the interstitial

@@ -139,7 +139,6 @@ SIGNATURES: dict[str, tuple] = {
     "mb_sim_halo_unpack": (_I, [_P, C.c_int32, C.c_int32, C.c_void_p, _D]),
     "mb_sim_slab_phase": (_I, [_P, C.c_int32, C.c_int32]),
     "mb_sim_clear_energies": (_I, [_P]),
-    "mb_sim_reach": (_I, [_P, _PD, C.POINTER(C.c_int32)]),
     "mb_ensemble_set_mode": (_I, [_P, C.c_int32]),
     "mb_ensemble_kernel_times": (_I, [_P, _PF, _PF, C.POINTER(C.c_int32)]),
 }

@@ -103,10 +103,6 @@ struct StencilSet {
   int n;                          // entries per parity (equal for both)
   int n_near;                     // leading entries inside the cutoff at the ideal lattice (0: unknown)
   int off[2][MB_MAX_STENCIL];     // [sublattice] split-layout linear offsets
-  // Entries ordered by ideal distance R_k: while every lattice atom lies closer than
-  // skip_u[k] = (R_k - cutoff) / 2 to its site, entry k and all later ones are out of the
-  // cutoff for every site and can be left out (-1: never)
-  double skip_u[MB_MAX_STENCIL];
 };
 
 // Convert reference-style doubled-x linear offsets to split-layout offsets.
@@ -120,8 +116,6 @@ int stencil_generate(double a0, double reach, int ext_x, int ext_y, int64_t *eve
                      int *reach_x, int *reach_y, int *reach_z);
 int stencil_sort_by_distance(double a0, double cutoff, int ext_x, int ext_y, int64_t *even, int64_t *odd, int n,
                              int *n_near);
-// skip_u of a distance-ordered stencil (see StencilSet)
-int stencil_skip_radii(double a0, double cutoff, int ext_x, int ext_y, const int64_t *even, int n, StencilSet *st);
 
 // ------------------------------------------------------ kernel arguments
 struct Lattice64 {
@@ -132,11 +126,6 @@ struct Lattice64 {
   double *vx, *vy, *vz; // velocities (box sites used)
   double *fx, *fy, *fz; // forces (box sites used)
   double *nx, *ny, *nz; // positions written by the drift (ext) or nullptr
-  // largest displacement of a lattice atom from its site, as the bits of a non-negative
-  // double (they order like the values): umax for px/py/pz (read; all ones = unknown),
-  // umax_next for nx/ny/nz (reset by the density pass, raised by the force passes); both
-  // null: the whole stencil is walked
-  unsigned long long *umax, *umax_next;
 };
 
 struct Itl64 {

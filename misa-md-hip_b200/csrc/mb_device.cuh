@@ -134,36 +134,6 @@ __device__ __forceinline__ double block_sum(double v) {
   return t;
 }
 
-// Deterministic block maximum of non-negative values; result in thread 0.
-__device__ __forceinline__ double block_max(double v) {
-  __shared__ double red_max[32];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) red_max[w] = v;
-  __syncthreads();
-  double t = 0.0;
-  if (threadIdx.x == 0)
-    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t = fmax(t, red_max[k]);
-  return t;
-}
-
-// Raises *umax (bits of a non-negative double) to at least u.
-__device__ __forceinline__ void raise_umax(unsigned long long *umax, double u) {
-  atomicMax(umax, (unsigned long long)__double_as_longlong(u));
-}
-
-// Stencil entries a lattice pass walks: all of them, or (with a displacement bound) only
-// those that can reach inside the cutoff while every atom stays within *umax of its site.
-__device__ __forceinline__ int stencil_in_reach(const StencilSet &st, const unsigned long long *umax) {
-  if (!umax) return st.n;
-  const double u = __longlong_as_double((long long)*umax);
-  int n = st.n_near;
-  while (n < st.n && !(u < st.skip_u[n])) n++;
-  return n;
-}
-
 struct Window {
   int gx0, gy0, gz0, nx, ny, nz;
 };

@@ -74,7 +74,6 @@ int stencil_from_linear(const int64_t *even, size_t n_even, const int64_t *odd, 
   if (n_even > MB_MAX_STENCIL) return fail(MB_ERR_ARG, "stencil longer than MB_MAX_STENCIL");
   out->n = (int)n_even;
   out->n_near = 0;
-  for (int k = 0; k < MB_MAX_STENCIL; k++) out->skip_u[k] = -1.0;
   const long long plane = (long long)ext_x * ext_y;
   for (int s = 0; s < 2; s++) {
     const int64_t *src = parity_of_sublattice[s] ? odd : even;
@@ -123,24 +122,6 @@ int stencil_sort_by_distance(double a0, double cutoff, int ext_x, int ext_y, int
   }
   if (near[0] != near[1]) return fail(MB_ERR_STATE, "even and odd stencils differ inside the cutoff");
   *n_near = near[0];
-  return MB_OK;
-}
-
-int stencil_skip_radii(double a0, double cutoff, int ext_x, int ext_y, const int64_t *even, int n, StencilSet *st) {
-  const long long plane = (long long)ext_x * ext_y;
-  double prev = 0.0;
-  for (int k = 0; k < n; k++) {
-    const long long o = even[k];
-    const long long dz = round_div(o, plane), rem = o - dz * plane, dy = round_div(rem, ext_x), dx = rem - dy * ext_x;
-    const int npar = (int)(dx & 1);
-    const double ox = 0.5 * dx, oy = dy + 0.5 * npar, oz = dz + 0.5 * npar;
-    const double R = a0 * sqrt(ox * ox + oy * oy + oz * oz);
-    if (R < prev) return fail(MB_ERR_STATE, "stencil not ordered by distance");
-    prev = R;
-    // a pair of this entry is at least R - |u_i| - |u_j| apart; keep a relative margin
-    // for the rounding of positions and of the bound itself
-    st->skip_u[k] = R > cutoff ? 0.5 * (R - cutoff) * (1.0 - 1e-9) : -1.0;
-  }
   return MB_OK;
 }
 

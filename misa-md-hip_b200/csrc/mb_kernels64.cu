@@ -158,9 +158,6 @@ __global__ void __launch_bounds__(MB_RHO_THREADS, 1)
   const int lane = threadIdx.x & 31;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
   double e_acc = 0.0;
-  // the force passes of this step raise the bound of the drifted positions from zero
-  if (L.umax_next && blockIdx.x == 0 && threadIdx.x == 0) *L.umax_next = 0ull;
-  const int n_use = ONE_TYPE ? stencil_in_reach(st, L.umax) : st.n;
   for (long long w = a.w0 + (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.n_items;
        w += wstride) {
     int chunk, y, s, z;
@@ -183,7 +180,7 @@ __global__ void __launch_bounds__(MB_RHO_THREADS, 1)
       }
       if (k < st.n_near) r0 += rho_term<true>(a, L, s_f2, i + off[k++], xi, yi, zi);
 #pragma unroll 2
-      for (; k < n_use; k++) r1 += rho_term<false>(a, L, s_f2, i + off[k], xi, yi, zi);
+      for (; k < st.n; k++) r1 += rho_term<false>(a, L, s_f2, i + off[k], xi, yi, zi);
       rho = r0 + r1;
     } else {
 #pragma unroll 4
@@ -283,9 +280,6 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
   const int lane = threadIdx.x & 31;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
   double e_pair = 0.0, e_kin = 0.0;
-  double u2max = 0.0; // squared displacement of the drifted atoms from their sites
-  const bool track_u = L.umax_next && sp.drift;
-  const int n_use = ONE_TYPE ? stencil_in_reach(st, L.umax) : st.n;
   for (long long w = a.w0 + (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.n_items;
        w += wstride) {
     int chunk, y, s, z;
@@ -317,7 +311,7 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
       }
       if (k < st.n_near) force_term<ENERGY, true>(a, L, s_f1, i + off[k++], xi, yi, zi, dfi, fx, fy, fz, ep);
 #pragma unroll 2
-      for (; k < n_use; k++) force_term<ENERGY, false>(a, L, s_f1, i + off[k], xi, yi, zi, dfi, gx, gy, gz, eq);
+      for (; k < st.n; k++) force_term<ENERGY, false>(a, L, s_f1, i + off[k], xi, yi, zi, dfi, gx, gy, gz, eq);
       fx += gx;
       fy += gy;
       fz += gz;
@@ -365,12 +359,6 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
         L.ny[i] = ny;
         L.nz[i] = nz;
         conv_check(g, sp, s, cx, y, z, nx, ny, nz);
-        if (track_u) {
-          double X, Y, Z;
-          site_ideal(s, cx, y, z, sp.a0, X, Y, Z);
-          const double ux = nx - X, uy = ny - Y, uz = nz - Z;
-          u2max = fmax(u2max, ux * ux + uy * uy + uz * uz);
-        }
         if (g.images)
           for_images(g, s, cx, y, z, [&](long long idx, double ox, double oy, double oz) {
             L.nx[idx] = nx + ox;
@@ -390,10 +378,6 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
     const double t2 = block_sum(e_kin);
     if (threadIdx.x == 0) a.e_kin[blockIdx.x] = t2;
   }
-  if (track_u) {
-    const double t = block_max(u2max);
-    if (threadIdx.x == 0) raise_umax(L.umax_next, sqrt(t));
-  }
 }
 
 // ----------------------------------------------------------- launchers
@@ -405,6 +389,14 @@ static int grid_for(long long warps_needed, int threads) {
 }
 
 static const int kSmemCap = 200 * 1024;
+
+// The one-type kernels locate spline intervals without range clamps (spl_locate_in):
+// every pair inside the cutoff must lie inside the r table, up to the rounding of its end
+// (a pair that far out takes the last interval at p a few ulps past 1).
+static bool cutoff_in_table(const DevPot &pot, double rc2) {
+  const double end = (double)(pot.nr - 1) / pot.rdr;
+  return rc2 <= end * end * (1.0 + 1e-12);
+}
 
 // Brick shapes (rows, planes) of the whole-box launches; {0, 0}: rows walk.  The
 // environment variables MB_RHO_BRICK / MB_FORCE_BRICK ("rows,planes") override them.
@@ -463,9 +455,7 @@ int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const L
   a.rc2 = rc2;
   a.e_partial = e_partial;
   a.skip_flagged = skip_flagged;
-  // the one-type kernels locate spline intervals without range clamps: every pair
-  // inside the cutoff must lie inside the table
-  const bool one = pot.n_types == 1 && rc2 <= (double)(pot.nr - 1) * (pot.nr - 1) / (pot.rdr * pot.rdr);
+  const bool one = pot.n_types == 1 && cutoff_in_table(pot, rc2);
   int nsm = smem_knots(pot, (int)sizeof(double4));
   if (!one) nsm = 0;
   a.m_lo = pot.nr - nsm;
@@ -505,7 +495,7 @@ int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const
   a.e_pair = e_partial ? e_partial + MB_EPART_CAP : nullptr;
   a.e_kin = e_partial ? e_partial + 2 * MB_EPART_CAP : nullptr;
   a.skip_flagged = skip_flagged;
-  const bool one = pot.n_types == 1 && sp.rc2 <= (double)(pot.nr - 1) * (pot.nr - 1) / (pot.rdr * pot.rdr);
+  const bool one = pot.n_types == 1 && cutoff_in_table(pot, sp.rc2);
   int nsm = smem_knots(pot, (int)(3 * sizeof(double2)));
   if (!one) nsm = 0;
   a.m_lo = pot.nr - nsm;
@@ -778,12 +768,6 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
             L.ny[i] = ny;
             L.nz[i] = nz;
             conv_check(g, sp, s, cx, y, z, nx, ny, nz);
-            if (L.umax_next) {
-              double X, Y, Z;
-              site_ideal(s, cx, y, z, sp.a0, X, Y, Z);
-              const double ux = nx - X, uy = ny - Y, uz = nz - Z;
-              raise_umax(L.umax_next, sqrt(ux * ux + uy * uy + uz * uz));
-            }
             if (g.images)
               for_images(g, s, cx, y, z, [&](long long idx, double ox, double oy, double oz) {
                 L.nx[idx] = nx + ox;

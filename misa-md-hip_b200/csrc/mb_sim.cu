@@ -69,10 +69,6 @@ struct mb_sim {
   // [z_first, z_first + bz) of cells_z; z ghosts filled through mb_sim_halo_*
   bool slab = false;
   int z_first = 0;
-  // largest displacement of a lattice atom from its site, per position buffer (bits of a
-  // double; all ones = unknown): the lattice passes of device-resident steps leave out
-  // the stencil entries it puts out of reach (see StencilSet::skip_u)
-  unsigned long long *d_umax = nullptr;
   // mixed precision: the lattice lives in a one-slot ensemble (mb_ens_host.cu)
   mb_ensemble *ens = nullptr;
   int slot = -1;
@@ -109,24 +105,6 @@ Lattice64 sim_lattice(mb_sim *s, int which) {
   L.fy = s->f[1];
   L.fz = s->f[2];
   return L;
-}
-
-// The lattice view of a device-resident step: with the displacement bound, unless
-// conversions can place atoms on sites behind the force passes' backs (their recombined
-// atoms would not be counted) or the slab's ghost atoms belong to other ranks.
-static Lattice64 sim_lattice_step(mb_sim *s, int which) {
-  Lattice64 L = sim_lattice(s, which);
-  if (s->d_umax && !s->slab && !(s->conv_d > 0.0)) {
-    L.umax = s->d_umax + which;
-    L.umax_next = s->d_umax + (which ^ 1);
-  }
-  return L;
-}
-
-// Positions changed outside the device-resident step: the bounds are unknown again.
-static int forget_umax(mb_sim *s) {
-  if (s->d_umax) MB_CUDA(cudaMemsetAsync(s->d_umax, 0xff, 2 * sizeof(unsigned long long), s->stream));
-  return MB_OK;
 }
 
 Itl64 sim_itl(mb_sim *s, int which) {
@@ -182,7 +160,7 @@ static bool itl_active(const mb_sim *s) { return s->n_itl > 0 || s->conv_d > 0.0
 // One FP64 step at positions pos[cur] (forces, closing kick, drift to pos[cur^1]).
 static int step64(mb_sim *s, int energy, int kick_pre, int drift, int timed) {
   const DevPot &P = pot_dev(s->pot);
-  Lattice64 L = sim_lattice_step(s, s->cur);
+  Lattice64 L = sim_lattice(s, s->cur);
   Itl64 I = sim_itl(s, s->cur);
   StepParams sp = sim_params(s, kick_pre, drift);
   double *ep = energy ? s->epart : nullptr;
@@ -435,8 +413,6 @@ static int create_sim(const mb_sim_config *cfg, const mb_eam_tables *pot, int z_
     rc = stencil_sort_by_distance(cfg->lattice_const, cfg->cutoff, s->ext_x, s->ext_y, even, odd, n, &n_near);
   if (rc == MB_OK) rc = stencil_from_linear(even, n, odd, n, s->ext_x, s->ext_y, g, par, &s->st);
   s->st.n_near = n_near;
-  if (rc == MB_OK && pot->n_types == 1)
-    rc = stencil_skip_radii(cfg->lattice_const, cfg->cutoff, s->ext_x, s->ext_y, even, n, &s->st);
   if (rc != MB_OK) {
     pot_free(s->pot);
     delete s;
@@ -470,8 +446,6 @@ static int create_sim(const mb_sim_config *cfg, const mb_eam_tables *pot, int z_
   if ((rc = dalloc(s, (void **)&s->id, (size_t)s->n_box * sizeof(int64_t))) != MB_OK) return cleanup(rc);
   if ((rc = dalloc(s, (void **)&s->epart, sizeof(double) * energy_partials_needed())) != MB_OK) return cleanup(rc);
   if ((rc = dalloc(s, (void **)&s->bad, sizeof(int))) != MB_OK) return cleanup(rc);
-  if ((rc = dalloc(s, (void **)&s->d_umax, 2 * sizeof(unsigned long long))) != MB_OK) return cleanup(rc);
-  if ((rc = forget_umax(s)) != MB_OK) return cleanup(rc);
   s->cap_itl = cfg->max_interstitials;
   const int ci = std::max(1, s->cap_itl);
   for (int b = 0; b < 2; b++)
@@ -520,8 +494,7 @@ int mb_sim_destroy(mb_sim *s) {
   drop_graph(s);
   if (s->ens) mb_ensemble_destroy(s->ens);
   void *ptrs[] = {s->code, s->df, s->rho, s->id, s->epart, s->eout, s->stage, s->bad, s->irho, s->idf, s->itype,
-                  s->iid, s->flag_list, s->flag_count, s->d_nitl, s->d_cand, s->d_cand_n, s->d_conv_counters,
-                  s->d_umax};
+                  s->iid, s->flag_list, s->flag_count, s->d_nitl, s->d_cand, s->d_cand_n, s->d_conv_counters};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int b = 0; b < 2; b++)
@@ -650,7 +623,6 @@ int mb_sim_upload(mb_sim *s, const mb_atom_element *box_atoms, const mb_atom_ele
   s->n_e = 0;
   s->e_steps.clear();
   MB_TRY(ensure_stage(s, (size_t)s->n_box));
-  MB_TRY(forget_umax(s));
   MB_CUDA(cudaMemcpyAsync(s->stage, box_atoms, (size_t)s->n_box * sizeof(mb_atom_element), cudaMemcpyHostToDevice,
                           s->stream));
   MB_CUDA(cudaMemsetAsync(s->bad, 0, sizeof(int), s->stream));
@@ -933,7 +905,6 @@ int mb_sim_step_host(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl
   if (!s || !box_atoms) return fail(MB_ERR_ARG, "null argument");
   if (s->cfg.precision != MB_PREC_FP64) return fail(MB_ERR_UNSUPPORTED, "host-buffer steps run the FP64 path");
   MB_TRY(ensure_stage(s, (size_t)s->n_box));
-  MB_TRY(forget_umax(s));
   drop_graph(s);
   s->cur = 0;
   s->primed = false;
@@ -973,7 +944,6 @@ int mb_sim_set_conversion(mb_sim *s, double convert_distance, double recombine_d
   s->conv_d = convert_distance;
   s->rec_d = convert_distance > 0 ? recombine_distance : 0.0;
   drop_graph(s); // the captured step pair changes
-  MB_TRY(forget_umax(s)); // bounds are not kept while conversions run
   return MB_OK;
 }
 
@@ -1051,7 +1021,6 @@ int mb_sim_slab_phase(mb_sim *s, int32_t phase, int32_t energy) {
     return fail(MB_ERR_UNSUPPORTED, "phase-wise steps take lattices without interstitials");
   const DevPot &P = pot_dev(s->pot);
   Lattice64 L = sim_lattice(s, s->cur);
-  MB_TRY(forget_umax(s)); // phase-wise steps keep no displacement bound
   double *ep = energy ? s->epart : nullptr;
   if (phase == 0) {
     if (energy) MB_CUDA(cudaMemsetAsync(s->epart, 0, sizeof(double) * energy_partials_needed(), s->stream));
@@ -1069,25 +1038,6 @@ int mb_sim_slab_phase(mb_sim *s, int32_t phase, int32_t energy) {
   }
   s->primed = true;
   s->cur ^= 1;
-  return MB_OK;
-}
-
-int mb_sim_reach(mb_sim *s, double *umax, int32_t *entries) {
-  if (!s || s->ens) return fail(MB_ERR_ARG, "bad arguments");
-  unsigned long long bits = ~0ull;
-  MB_CUDA(cudaStreamSynchronize(s->stream));
-  if (s->d_umax && !s->slab && !(s->conv_d > 0.0))
-    MB_CUDA(cudaMemcpy(&bits, s->d_umax + s->cur, sizeof(bits), cudaMemcpyDeviceToHost));
-  double u;
-  memcpy(&u, &bits, sizeof(u));
-  const bool known = bits != ~0ull;
-  int n = s->st.n;
-  if (known) {
-    n = s->st.n_near;
-    while (n < s->st.n && !(u < s->st.skip_u[n])) n++;
-  }
-  if (umax) *umax = known ? u : -1.0;
-  if (entries) *entries = n;
   return MB_OK;
 }
 

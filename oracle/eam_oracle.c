@@ -220,6 +220,16 @@ int orc_stencil_build(const orc_domain *d, double a0, double reach, int64_t *eve
 
 /* ------------------------------------------------------- reference passes */
 
+/* Neumaier's compensated summation: *s + *c carries the sum of every x added. */
+static inline void neumaier(double *s, double *c, double x) {
+  const double t = *s + x;
+  if (fabs(*s) >= fabs(x))
+    *c += (*s - t) + x;
+  else
+    *c += (x - t) + *s;
+  *s = t;
+}
+
 static inline int64_t site_linear(const orc_domain *d, int64_t x, int64_t y, int64_t z) {
   return ((z + d->ghost_size_z) * d->ext_size_y + y + d->ghost_size_y) * d->ext_size_x + x + d->ghost_size_x;
 }
@@ -514,9 +524,15 @@ void orc_compute_forces(const orc_pot *p, const orc_domain *d, orc_atom *atoms, 
   free(win);
 
   if (e_out) {
-    double pe = 0.0, ke = 0.0;
-#pragma omp parallel for schedule(static) collapse(2) reduction(+ : pe, ke)
-    for (int64_t z = 0; z < d->box_size_z; z++)
+    /* Energies are sums of millions of terms: each z layer is summed with Neumaier's
+     * compensated summation, then the layers in order, so the totals carry about one
+     * rounding of the result whatever the thread count (a plain OpenMP reduction leaves
+     * ~1e-11 eV/atom of rounding at 4 M atoms). */
+    const int64_t nzl = d->box_size_z;
+    double *lay = (double *)calloc((size_t)(4 * nzl), sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int64_t z = 0; z < nzl; z++) {
+      double sp = 0.0, cp = 0.0, sk = 0.0, ck = 0.0;
       for (int64_t y = 0; y < d->box_size_y; y++)
         for (int64_t x = 0; x < d->box_size_x; x++) {
           const int64_t i = site_linear(d, x, y, z);
@@ -534,14 +550,29 @@ void orc_compute_forces(const orc_pot *p, const orc_domain *d, orc_atom *atoms, 
             if (d2 >= rc2) continue;
             e += 0.5 * orc_phi_of_r(p, a->type, b->type, sqrt(d2));
           }
-          pe += e;
-          ke += 0.5 * mp->mass * (a->v[0] * a->v[0] + a->v[1] * a->v[1] + a->v[2] * a->v[2]);
+          neumaier(&sp, &cp, e);
+          neumaier(&sk, &ck, 0.5 * mp->mass * (a->v[0] * a->v[0] + a->v[1] * a->v[1] + a->v[2] * a->v[2]));
         }
+      lay[4 * z + 0] = sp;
+      lay[4 * z + 1] = cp;
+      lay[4 * z + 2] = sk;
+      lay[4 * z + 3] = ck;
+    }
+    double pe = 0.0, cpe = 0.0, ke = 0.0, cke = 0.0;
+    for (int64_t z = 0; z < nzl; z++) {
+      neumaier(&pe, &cpe, lay[4 * z + 0]);
+      neumaier(&pe, &cpe, lay[4 * z + 1]);
+      neumaier(&ke, &cke, lay[4 * z + 2]);
+      neumaier(&ke, &cke, lay[4 * z + 3]);
+    }
+    free(lay);
     for (int I = 0; I < n_itl; I++) {
       const orc_atom *a = itl + I;
-      pe += orc_F_of_rho(p, a->type, a->rho);
-      ke += 0.5 * mp->mass * (a->v[0] * a->v[0] + a->v[1] * a->v[1] + a->v[2] * a->v[2]);
+      neumaier(&pe, &cpe, orc_F_of_rho(p, a->type, a->rho));
+      neumaier(&ke, &cke, 0.5 * mp->mass * (a->v[0] * a->v[0] + a->v[1] * a->v[1] + a->v[2] * a->v[2]));
     }
+    pe += cpe;
+    ke += cke;
     e_out->pe = pe + pe_pair_itl;
     e_out->ke = ke * ORC_MVV2E;
   }

@@ -63,7 +63,9 @@ def test_fe20_600K_every_step_of_100_matches_oracle():
         sim.run(0, energy_every=1)  # forces and energies at the start
         e0 = sim.energies()
         bg, _ = sim.download()
-        _compare(bg, None, ref.box(), None, what=("f",))
+        # the start is the perfect lattice: every force vanishes by symmetry (both paths
+        # leave rounding noise only), so the relative comparison starts at step 1
+        assert np.abs(bg["f"]).max() < 1e-12 and np.abs(ref.box()["f"]).max() < 1e-12
         assert abs(e0[-1, 1] - ref.pe) / n < E_TOL and abs(e0[-1, 2] - ref.ke) / n < E_TOL
         worst = 0.0
         for step in range(1, 101):

@@ -86,9 +86,9 @@ def test_budget_queues_and_faults_are_contained():
 
 @pytest.mark.gpu
 def test_large_admission_is_prepared_off_the_loop_thread():
-    # small lattices run while a 2 M-atom request arrives; its lattice is built on a worker
-    # thread, so the loop thread only uploads it between chunks
-    small = serve.poisson_stream(3, rate=1000.0, seed=21, atoms=(2e3, 2e4), steps=(3000, 3000))
+    # small lattices run for many steps while a 2 M-atom request arrives; its lattice is
+    # built on a worker thread, so the loop thread only uploads it between chunks
+    small = serve.poisson_stream(3, rate=1000.0, seed=21, atoms=(2e4, 5e4), steps=(40000, 40000))
     big = serve.Request(50, 0.05, serve.cells_for_atoms(2e6), 20, 600.0, 0.005, 77)
     probe = serve.Request(51, 0.0, big.cells, 20, 600.0, 0.005, 77)
     t = time.perf_counter()
@@ -99,5 +99,5 @@ def test_large_admission_is_prepared_off_the_loop_thread():
     srv.close()
     assert stats["completed"] == 4
     stall = dict(srv.admit_stall)[big.rid]
-    assert big.admitted < max(r.finished for r in small)  # it joined while the others ran
     assert stall < 0.3 * t_build, (stall, t_build)
+    assert big.admitted < max(r.finished for r in small)  # it joined while the others ran
