@@ -92,6 +92,18 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
+def ncu_l1tex(kernel: str) -> dict | None:
+    """L1TEX data-stage throughput (% of peak) of `kernel` from the committed ncu summary:
+    the on-chip resource the lattice passes are bound by (their DRAM traffic is at or below
+    the algorithmic bytes)."""
+    p = ROOT / "profiles" / "traffic.json"
+    try:
+        d = json.loads(p.read_text())[kernel]
+        return {"frac": d["l1tex_throughput_pct"] / 100.0, "source": d["source"]}
+    except Exception:
+        return None
+
+
 def ncu_traffic(kernel: str, n_atoms: int) -> float | None:
     """DRAM bytes per launch of `kernel` from the committed ncu summary, scaled from the
     profiled atom count to n_atoms (traffic grows in proportion to the lattice)."""
@@ -335,6 +347,7 @@ def run_ours(args, mb, wl, world, rank, local, pg) -> None:
                 "frac": kflops * n_atoms / (kms * 1e-3) / 1e12 / fpeak,
                 "peak_source": "measured FMA-chain probe (mb_measure_fma_peaks)"},
         "fp64_peak_tflops": f64.value, "fp32_peak_tflops": f32.value,
+        "l1tex": ncu_l1tex(kname.split()[0]),
     }
     if rho_ms > 0:
         rb = BYTES_RHO if precision == mb.MB_PREC_FP64 else BYTES_MIXED_RHO
