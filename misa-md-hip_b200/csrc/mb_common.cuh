@@ -10,6 +10,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <string>
@@ -31,6 +32,17 @@ __device__ __forceinline__ double4 ldg4(const double4 *p) {
   const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
   return make_double4(a.x, a.y, b.x, b.y);
 }
+
+// ----------------------------------------------------------------- tracing
+// NVTX range around an entry point's work (shows in Nsight timelines; costs nothing
+// when no tool is attached).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
+#define MB_RANGE(name) ::mb::NvtxRange mb_nvtx_range_(name)
 
 // ---------------------------------------------------------------- errors
 void set_error(const std::string &msg);

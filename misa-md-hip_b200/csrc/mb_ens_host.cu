@@ -917,6 +917,7 @@ int mb_ensemble_lattice_bytes(const mb_lattice_spec *spec, int64_t *bytes) {
 
 int mb_ensemble_add(mb_ensemble *e, const mb_lattice_spec *spec, const mb_atom_element *box,
                     const mb_atom_element *itl, int32_t n_itl, int64_t steps, int32_t *slot_out) {
+  MB_RANGE("mb_ensemble_add");
   if (!e || !spec || !box || !slot_out) return fail(MB_ERR_ARG, "null argument");
   std::lock_guard<std::mutex> lk(e->mu);
   const int cx = spec->cells_x, cy = spec->cells_y, cz = spec->cells_z;
@@ -1094,6 +1095,7 @@ int mb_ensemble_set_steps(mb_ensemble *e, int32_t slot, int64_t steps_target) {
 }
 
 int mb_ensemble_advance(mb_ensemble *e, int32_t max_launches, int32_t energy_every, int32_t *launches) {
+  MB_RANGE("mb_ensemble_advance");
   if (!e || max_launches < 0 || energy_every < 0) return fail(MB_ERR_ARG, "bad arguments");
   std::lock_guard<std::mutex> lk(e->mu);
   long long n = 0;
@@ -1103,6 +1105,7 @@ int mb_ensemble_advance(mb_ensemble *e, int32_t max_launches, int32_t energy_eve
 }
 
 int mb_ensemble_run(mb_ensemble *e, int32_t nsteps, int32_t energy_every) {
+  MB_RANGE("mb_ensemble_run");
   if (!e || nsteps < 0 || energy_every < 0) return fail(MB_ERR_ARG, "bad arguments");
   std::lock_guard<std::mutex> lk(e->mu);
   MB_TRY(sync_desc(e));

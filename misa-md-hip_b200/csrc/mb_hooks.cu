@@ -397,6 +397,7 @@ int mb_pot_init(const mb_eam_tables *t) {
 }
 
 int mb_eam_rho_calc(mb_atom_element *atoms, double cutoff_radius) {
+  MB_RANGE("mb_eam_rho_calc");
   std::lock_guard<std::mutex> lk(g_mu);
   HookCtx &c = g_ctx;
   if (!(cutoff_radius > 0)) return fail(MB_ERR_ARG, "cutoff must be > 0");
@@ -407,6 +408,7 @@ int mb_eam_rho_calc(mb_atom_element *atoms, double cutoff_radius) {
 }
 
 int mb_eam_df_calc(mb_atom_element *atoms, double cutoff_radius) {
+  MB_RANGE("mb_eam_df_calc");
   // Full-neighbour mode: df already came out of the rho pass
   // (src/hip_arch_acc_imp.cpp:184-186 returns at once).  Half-neighbour mode: the
   // host has added the ghost shares of rho to their owners; df = F'(rho) of the box
@@ -429,6 +431,7 @@ int mb_eam_df_from_rho(mb_atom_element *atoms) {
 }
 
 int mb_eam_force_calc(mb_atom_element *atoms, double cutoff_radius) {
+  MB_RANGE("mb_eam_force_calc");
   std::lock_guard<std::mutex> lk(g_mu);
   HookCtx &c = g_ctx;
   if (!(cutoff_radius > 0)) return fail(MB_ERR_ARG, "cutoff must be > 0");

@@ -613,6 +613,7 @@ static int download_itl(mb_sim *s, mb_atom_element *itl, int which, int unkick) 
 }
 
 int mb_sim_upload(mb_sim *s, const mb_atom_element *box_atoms, const mb_atom_element *itl, int32_t n_itl) {
+  MB_RANGE("mb_sim_upload");
   if (s && s->ens) return box_atoms ? mixed_upload(s, box_atoms, itl, n_itl) : fail(MB_ERR_ARG, "null argument");
   if (!s || !box_atoms) return fail(MB_ERR_ARG, "null argument");
   MB_CUDA(cudaStreamSynchronize(s->stream));
@@ -643,6 +644,7 @@ int mb_sim_upload(mb_sim *s, const mb_atom_element *box_atoms, const mb_atom_ele
 }
 
 int mb_sim_download(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t *n_itl) {
+  MB_RANGE("mb_sim_download");
   if (s && s->ens) {
     MB_TRY(mixed_need_slot(s));
     return mb_ensemble_download(s->ens, s->slot, box_atoms, itl, n_itl);
@@ -664,6 +666,7 @@ int mb_sim_download(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl,
 }
 
 int mb_sim_run(mb_sim *s, int32_t nsteps, int32_t energy_every) {
+  MB_RANGE("mb_sim_run");
   if (s && s->slab) return fail(MB_ERR_UNSUPPORTED, "a z-slab steps through mb_sim_slab_phase with halo exchanges");
   if (s && s->ens) {
     MB_TRY(mixed_need_slot(s));
@@ -901,6 +904,7 @@ static int step_host_slabs(mb_sim *s, mb_atom_element *box_atoms, mb_atom_elemen
 }
 
 int mb_sim_step_host(mb_sim *s, mb_atom_element *box_atoms, mb_atom_element *itl, int32_t n_itl) {
+  MB_RANGE("mb_sim_step_host");
   if (s && s->slab) return fail(MB_ERR_UNSUPPORTED, "a z-slab steps through mb_sim_slab_phase with halo exchanges");
   if (!s || !box_atoms) return fail(MB_ERR_ARG, "null argument");
   if (s->cfg.precision != MB_PREC_FP64) return fail(MB_ERR_UNSUPPORTED, "host-buffer steps run the FP64 path");
@@ -1015,6 +1019,7 @@ int mb_sim_halo_unpack(mb_sim *s, int32_t what, int32_t side, const void *device
 }
 
 int mb_sim_slab_phase(mb_sim *s, int32_t phase, int32_t energy) {
+  MB_RANGE("mb_sim_slab_phase");
   if (!s || s->ens) return fail(MB_ERR_ARG, "bad arguments");
   if (phase != 0 && phase != 1) return fail(MB_ERR_ARG, "phase must be 0 (rho) or 1 (force + integration)");
   if (s->n_itl > 0 || s->conv_d > 0.0)

@@ -19,6 +19,12 @@ Host-side failure handling: malformed requests are rejected at submission; a
 request larger than the whole budget is rejected instead of queued forever; a
 request can be cancelled while queued or in flight (its slot is freed, the other
 lattices are untouched).
+
+Checkpoint / resume: ``checkpoint(req)`` reads a running request's state (positions,
+velocities, forces of its lattice at its current step) back to the host;
+``preempt(req)`` does that, frees its slot and puts it back at the head of the queue,
+so that it resumes from the saved state with its remaining steps when memory allows
+(e.g. to make room for a more urgent lattice).
 """
 from __future__ import annotations
 
@@ -54,6 +60,9 @@ class Request:
     reason: str = ""
     result: np.ndarray | None = None
     energies: np.ndarray | None = None
+    # checkpoint / resume
+    snapshot: np.ndarray | None = None  # box records of the last checkpoint
+    steps_before: int = 0               # steps done before the current admission
 
     @property
     def latency(self) -> float:
@@ -154,8 +163,27 @@ class Server:
         if self.pool is None:
             return
         for req in self.queue[:self.prep_ahead]:
-            if req.rid not in self.prepared:
+            if req.rid not in self.prepared and req.snapshot is None:
                 self.prepared[req.rid] = self.pool.submit(build_lattice, req)
+
+    def checkpoint(self, req: Request) -> tuple[np.ndarray, int]:
+        """A running request's lattice at its current step and the steps it has done."""
+        if req.status != "running":
+            raise ValueError("only a running request can be checkpointed")
+        done, _, _ = self.ens.status(req.slot)
+        box = self.ens.download(req.slot)[0]
+        return box, req.steps_before + int(done)
+
+    def preempt(self, req: Request) -> None:
+        """Checkpoint a running request, free its slot and queue it first: it resumes
+        from the checkpoint with its remaining steps."""
+        box, done = self.checkpoint(req)
+        self.ens.remove(req.slot)
+        del self.running[req.slot]
+        req.slot = -1
+        req.snapshot, req.steps_before = box, done
+        req.status = "queued"
+        self.queue.insert(0, req)
 
     def cancel(self, req: Request) -> None:
         if req.status == "queued":
@@ -175,7 +203,9 @@ class Server:
             req = self.queue[0]
             t_in = time.perf_counter()
             fut = self.prepared.get(req.rid)
-            if fut is None:
+            if req.snapshot is not None:
+                box = req.snapshot  # resuming from a checkpoint
+            elif fut is None:
                 box = build_lattice(req)
             elif fut.done() or not self.running:
                 box = fut.result()
@@ -183,7 +213,7 @@ class Server:
                 self._prefetch()
                 return
             try:
-                req.slot = self.ens.add(req.cells, box, steps=req.steps)
+                req.slot = self.ens.add(req.cells, box, steps=req.steps - req.steps_before)
             except MbError as e:
                 if e.code == MB_ERR_NOMEM and self.running:
                     return  # wait for memory to free up (the prepared lattice is kept)
@@ -194,6 +224,7 @@ class Server:
                 continue
             self.queue.pop(0)
             self.prepared.pop(req.rid, None)
+            req.snapshot = None
             req.status = "running"
             req.admitted = self.now()
             self.running[req.slot] = req

@@ -101,3 +101,28 @@ def test_large_admission_is_prepared_off_the_loop_thread():
     stall = dict(srv.admit_stall)[big.rid]
     assert stall < 0.3 * t_build, (stall, t_build)
     assert big.admitted < max(r.finished for r in small)  # it joined while the others ran
+
+
+@pytest.mark.gpu
+def test_preempted_request_resumes_from_its_checkpoint():
+    req = serve.Request(0, 0.0, (10, 10, 10), 300, 900.0, 0.005, 5)
+    alone = _alone(serve.Request(0, 0.0, (10, 10, 10), 300, 900.0, 0.005, 5))
+    srv = serve.Server(chunk=25, keep_results=True)
+    hit = []
+
+    def tick(s):
+        if not hit and req.status == "running":
+            box, done = s.checkpoint(req)
+            assert box.shape[0] == 2 * 10 ** 3
+            if done >= 100:
+                s.preempt(req)
+                hit.append(req.steps_before)
+
+    stats = srv.serve([req], realtime=False, on_tick=tick)
+    srv.close()
+    assert stats["completed"] == 1 and req.status == "done"
+    assert hit and 100 <= hit[0] < 300
+    # resumed from positions, velocities and forces read back mid-run: the same
+    # trajectory up to the rounding of the read-back state
+    assert np.max(np.abs(req.result["x"] - alone["x"])) < 1e-8
+    assert np.max(np.abs(req.result["v"] - alone["v"])) < 1e-10
