@@ -174,9 +174,6 @@ int mb_spline_coeffs(const double *y, int n, double dx, double *coef7);
  * copies that did not overlap it. */
 int mb_hook_last_timing(float *kernel_ms, float *copy_ms);
 
-/* Throughput of dependent-free FMA chains on the CUDA cores of the current device
- * (TFLOP/s, FMA = 2 flops): the FP64 and FP32 roofline denominators. */
-int mb_measure_fma_peaks(double *fp64_tflops, double *fp32_tflops);
 
 /* ---------------------------------------- 2. device-resident simulation */
 

@@ -92,7 +92,6 @@ SIGNATURES: dict[str, tuple] = {
     "mb_cli_set_batches": (_I, [C.c_uint]),
     "mb_cli_batches": (C.c_uint, []),
     "mb_hook_last_timing": (_I, [_PF, _PF]),
-    "mb_measure_fma_peaks": (_I, [_PD, _PD]),
     "mb_spline_coeffs": (_I, [_PD, _I, _D, _PD]),
     "mb_stencil_linear": (_I, [_D, _D, _I, _I, _PI64, _PI64, _I, _PI]),
     "mb_sim_create": (_I, [C.POINTER(MbSimConfig), C.POINTER(MbEamTables), C.POINTER(_P)]),

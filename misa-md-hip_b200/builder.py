@@ -15,6 +15,8 @@ PKG = pathlib.Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libmisa_b200.so"
+PROBE_SRC = PKG / "probe" / "fma_probe.cu"
+PROBE_LIB = PKG / "libmb_probe.so"  # the benchmark's FMA-peak probe (not part of the plugin)
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -66,6 +68,13 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    if force or _stale(PROBE_LIB, [PROBE_SRC]):
+        cmd = [nvcc, *flags, "-shared", "-o", str(PROBE_LIB), str(PROBE_SRC)]
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"probe build failed:\n{r.stdout}\n{r.stderr}")
     return LIB
 
 
