@@ -184,10 +184,19 @@ __host__ __device__ __forceinline__ void site_ideal(int s, int cx, int y, int z,
 // [z0, z1): the box layers a launch covers (z1 < 0: up to the last layer).  The
 // interstitial passes then take the flagged sites in those layers and the
 // interstitials whose wrapped z lies in them.
+// outer: per-item masks of the outer stencil entries (beyond the cutoff at the ideal
+// lattice) that some site of the item has inside the cutoff, one uint2 per item of the
+// box (items_per_box).  The density pass writes them; a force pass given them walks only
+// those entries, so it must run on the positions of the density pass that wrote them
+// (null: the force pass walks every entry).
 int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, double rc2,
-                 double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0 = 0, int z1 = -1);
+                 double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0 = 0, int z1 = -1,
+                 uint2 *outer = nullptr);
 int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const StepParams &sp,
-                   double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0 = 0, int z1 = -1);
+                   double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0 = 0, int z1 = -1,
+                   const uint2 *outer = nullptr);
+// Work items (32-site row chunks) of the whole box: the length of the outer masks.
+inline long long items_per_box(const Geom &g) { return (long long)((g.bcx + 31) / 32) * g.by * 2 * g.bz; }
 int launch_itl_mark64(const Geom &g, const Lattice64 &L, const Itl64 &I, cudaStream_t s);
 // Flags the sites of layers [z0, z1) near an interstitial, without clearing or
 // resetting the list first.

@@ -96,6 +96,12 @@ __device__ __forceinline__ bool decode_item(const Geom &g, const ItemWalk &wk, l
   return y < g.by && z < g.bz;
 }
 
+// Index of an item in rows-walk order, whatever walk a launch takes: the key of the
+// per-item outer-entry masks, which the density pass writes and the force pass reads.
+__device__ __forceinline__ long long item_id(const Geom &g, const ItemWalk &wk, int chunk, int y, int s, int z) {
+  return ((long long)(2 * z + s) * g.by + y) * wk.chunks + chunk;
+}
+
 // -------------------------------------------------------------- rho pass
 struct RhoArgs {
   Geom g;
@@ -107,6 +113,9 @@ struct RhoArgs {
   int m_lo;      // first knot kept in shared memory
   ItemWalk walk;
   long long w0, n_items; // items [w0, n_items): a z-slab of the box (z slowest) or every brick
+  uint2 *outer;  // per item: bit b set when a lane has stencil entry n_near + b inside the cutoff (or null)
+  double rc2m;   // the squared cutoff of those bits, a hair above rc2 (robust to the FMA contraction
+                 // of either pass)
 };
 
 // One density term of a one-type lattice.  BF (branch-free): the stencil entry lies
@@ -114,10 +123,11 @@ struct RhoArgs {
 // value is masked instead of branched around, which lets iterations overlap.
 template <bool BF>
 __device__ __forceinline__ double rho_term(const RhoArgs &a, const Lattice64 &L, const double2 *s_f2, long long j,
-                                           double xi, double yi, double zi) {
+                                           double xi, double yi, double zi, bool *near = nullptr) {
   const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
   const double d2 = dx * dx + dy * dy + dz * dz;
   const bool in = d2 < a.rc2;
+  if (!BF) *near = d2 < a.rc2m;
   if (!BF && !in) return 0.0;
   const double r = d2 * rsqrt(d2);
   int m;
@@ -133,6 +143,62 @@ __device__ __forceinline__ double rho_term(const RhoArgs &a, const Lattice64 &L,
   }
   const double v = cubic(c, p);
   return (BF && !in) ? 0.0 : v;
+}
+
+// Density, df = F'(rho) and its ghost images of one lattice site (a lane of an item);
+// returns the bits of the outer stencil entries (n_near + b) the site has inside the
+// cutoff (one-type walk only).
+template <bool ENERGY, bool ONE_TYPE>
+__device__ __forceinline__ unsigned long long rho_site(const StencilSet &st, const RhoArgs &a, const double2 *s_f2,
+                                                       int s, int cx, int y, int z, double &e_acc) {
+  const Geom &g = a.g;
+  const Lattice64 &L = a.L;
+  const DevPot &P = a.P;
+  const long long i = ext_index(g, s, cx, y, z);
+  const int code = L.code[i];
+  if (code < 0 || (a.skip_flagged && (code & MB_FLAG_ITL))) return 0;
+  const int ti = code & 0x3F;
+  const double xi = L.px[i], yi = L.py[i], zi = L.pz[i];
+  const int *off = st.off[s];
+  double rho = 0.0;
+  unsigned long long near = 0;
+  if (ONE_TYPE) {
+    double r0 = 0.0, r1 = 0.0;
+    int k = 0;
+    for (; k + 1 < st.n_near; k += 2) {
+      r0 += rho_term<true>(a, L, s_f2, i + off[k], xi, yi, zi);
+      r1 += rho_term<true>(a, L, s_f2, i + off[k + 1], xi, yi, zi);
+    }
+    if (k < st.n_near) r0 += rho_term<true>(a, L, s_f2, i + off[k++], xi, yi, zi);
+#pragma unroll 2
+    for (; k < st.n; k++) {
+      bool in;
+      r1 += rho_term<false>(a, L, s_f2, i + off[k], xi, yi, zi, &in);
+      near |= (unsigned long long)in << ((k - st.n_near) & 63);
+    }
+    rho = r0 + r1;
+  } else {
+#pragma unroll 4
+    for (int k = 0; k < st.n; k++) {
+      const long long j = i + off[k];
+      const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (d2 < a.rc2) {
+        const double r = d2 * rsqrt(d2);
+        int m;
+        double p;
+        spl_locate(r, P.rdr, P.nr, m, p);
+        const int tj = L.code[j] & 0x3F;
+        rho += cubic(ldg4(&P.f_val[(size_t)tj * P.nr + m]), p);
+      }
+    }
+  }
+  const double df = dF64(P, ti, rho);
+  L.df[i] = df;
+  if (L.rho) L.rho[i] = rho;
+  if (g.images) for_images(g, s, cx, y, z, [&](long long idx, double, double, double) { L.df[idx] = df; });
+  if (ENERGY) e_acc += F64(P, ti, rho);
+  return near;
 }
 
 template <bool ENERGY, bool ONE_TYPE>
@@ -154,55 +220,21 @@ __global__ void __launch_bounds__(MB_RHO_THREADS, 1)
   __syncthreads();
 
   const Geom &g = a.g;
-  const Lattice64 &L = a.L;
   const int lane = threadIdx.x & 31;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
   double e_acc = 0.0;
   for (long long w = a.w0 + (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.n_items;
        w += wstride) {
     int chunk, y, s, z;
-    if (!decode_item(g, a.walk, w, chunk, y, s, z)) continue;
+    if (!decode_item(g, a.walk, w, chunk, y, s, z)) continue; // the same for the whole warp
     const int cx = chunk * 32 + lane;
-    if (cx >= g.bcx) continue;
-    const long long i = ext_index(g, s, cx, y, z);
-    const int code = L.code[i];
-    if (code < 0 || (a.skip_flagged && (code & MB_FLAG_ITL))) continue;
-    const int ti = code & 0x3F;
-    const double xi = L.px[i], yi = L.py[i], zi = L.pz[i];
-    const int *off = st.off[s];
-    double rho = 0.0;
-    if (ONE_TYPE) {
-      double r0 = 0.0, r1 = 0.0;
-      int k = 0;
-      for (; k + 1 < st.n_near; k += 2) {
-        r0 += rho_term<true>(a, L, s_f2, i + off[k], xi, yi, zi);
-        r1 += rho_term<true>(a, L, s_f2, i + off[k + 1], xi, yi, zi);
-      }
-      if (k < st.n_near) r0 += rho_term<true>(a, L, s_f2, i + off[k++], xi, yi, zi);
-#pragma unroll 2
-      for (; k < st.n; k++) r1 += rho_term<false>(a, L, s_f2, i + off[k], xi, yi, zi);
-      rho = r0 + r1;
-    } else {
-#pragma unroll 4
-      for (int k = 0; k < st.n; k++) {
-        const long long j = i + off[k];
-        const double dx = xi - L.px[j], dy = yi - L.py[j], dz = zi - L.pz[j];
-        const double d2 = dx * dx + dy * dy + dz * dz;
-        if (d2 < a.rc2) {
-          const double r = d2 * rsqrt(d2);
-          int m;
-          double p;
-          spl_locate(r, P.rdr, P.nr, m, p);
-          const int tj = L.code[j] & 0x3F;
-          rho += cubic(ldg4(&P.f_val[(size_t)tj * P.nr + m]), p);
-        }
-      }
+    unsigned long long near = 0; // outer stencil entries this lane has inside the cutoff
+    if (cx < g.bcx) near = rho_site<ENERGY, ONE_TYPE>(st, a, s_f2, s, cx, y, z, e_acc);
+    if (ONE_TYPE && a.outer) {
+      const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)near);
+      const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(near >> 32));
+      if (lane == 0) a.outer[item_id(g, a.walk, chunk, y, s, z)] = make_uint2(lo, hi);
     }
-    const double df = dF64(P, ti, rho);
-    L.df[i] = df;
-    if (L.rho) L.rho[i] = rho;
-    if (g.images) for_images(g, s, cx, y, z, [&](long long idx, double, double, double) { L.df[idx] = df; });
-    if (ENERGY) e_acc += F64(P, ti, rho);
   }
   if (ENERGY) {
     const double t = block_sum(e_acc);
@@ -222,6 +254,8 @@ struct ForceArgs {
   int m_lo;
   ItemWalk walk;
   long long w0, n_items; // items [w0, n_items)
+  const uint2 *outer;    // per item: the outer stencil entries the density pass of these
+                         // positions found inside the cutoff (or null: walk them all)
 };
 
 // One force term of a one-type lattice (see rho_term for BF).
@@ -284,6 +318,15 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
        w += wstride) {
     int chunk, y, s, z;
     if (!decode_item(g, a.walk, w, chunk, y, s, z)) continue;
+    // outer entries (n_near + b) that no lane of this item has inside the cutoff are not
+    // walked: they contribute nothing.  Without masks the same loop walks every outer
+    // entry, so both give bitwise the same forces.
+    const int n_outer = st.n - st.n_near;
+    unsigned long long outer = n_outer >= 64 ? ~0ull : (1ull << n_outer) - 1;
+    if (ONE_TYPE && a.outer) {
+      const uint2 m2 = a.outer[item_id(g, a.walk, chunk, y, s, z)];
+      outer = (unsigned long long)m2.x | ((unsigned long long)m2.y << 32);
+    }
     const int cx = chunk * 32 + lane;
     if (cx >= g.bcx) continue;
     const long long i = ext_index(g, s, cx, y, z);
@@ -310,8 +353,16 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
         force_term<ENERGY, true>(a, L, s_f1, i + off[k + 1], xi, yi, zi, dfi, gx, gy, gz, eq);
       }
       if (k < st.n_near) force_term<ENERGY, true>(a, L, s_f1, i + off[k++], xi, yi, zi, dfi, fx, fy, fz, ep);
+      if (n_outer <= 64) {
+        // set bits in ascending k, the order of the full walk
+        for (unsigned long long m = outer; m; m &= m - 1) {
+          const int kk = st.n_near + __ffsll((long long)m) - 1;
+          force_term<ENERGY, false>(a, L, s_f1, i + off[kk], xi, yi, zi, dfi, gx, gy, gz, eq);
+        }
+      } else {
 #pragma unroll 2
-      for (; k < st.n; k++) force_term<ENERGY, false>(a, L, s_f1, i + off[k], xi, yi, zi, dfi, gx, gy, gz, eq);
+        for (; k < st.n; k++) force_term<ENERGY, false>(a, L, s_f1, i + off[k], xi, yi, zi, dfi, gx, gy, gz, eq);
+      }
       fx += gx;
       fy += gy;
       fz += gz;
@@ -449,16 +500,21 @@ static int smem_knots(const DevPot &pot, int bytes_per_knot) {
   return n;
 }
 
+// Per-item outer-entry masks fit in 64 bits.
+static bool outer_masks_fit(const StencilSet &st) { return st.n - st.n_near <= 64; }
+
 int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, double rc2,
-                 double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0, int z1) {
+                 double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0, int z1, uint2 *outer) {
   RhoArgs a;
   a.g = g;
   a.P = pot;
   a.L = L;
   a.rc2 = rc2;
+  a.rc2m = rc2 * (1.0 + 1e-9);
   a.e_partial = e_partial;
   a.skip_flagged = skip_flagged;
   const bool one = pot.n_types == 1 && cutoff_in_table(pot, rc2);
+  a.outer = one && outer_masks_fit(st) ? outer : nullptr;
   int nsm = smem_knots(pot, (int)sizeof(double4));
   if (!one) nsm = 0;
   a.m_lo = pot.nr - nsm;
@@ -489,7 +545,8 @@ int launch_rho64(const Geom &g, const StencilSet &st, const DevPot &pot, const L
 }
 
 int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const Lattice64 &L, const StepParams &sp,
-                   double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0, int z1) {
+                   double *e_partial, int energy, int skip_flagged, cudaStream_t s, int z0, int z1,
+                   const uint2 *outer) {
   ForceArgs a;
   a.g = g;
   a.P = pot;
@@ -499,6 +556,7 @@ int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const
   a.e_kin = e_partial ? e_partial + 2 * MB_EPART_CAP : nullptr;
   a.skip_flagged = skip_flagged;
   const bool one = pot.n_types == 1 && cutoff_in_table(pot, sp.rc2);
+  a.outer = one && outer_masks_fit(st) ? outer : nullptr;
   int nsm = smem_knots(pot, (int)(3 * sizeof(double2)));
   if (!one) nsm = 0;
   a.m_lo = pot.nr - nsm;

@@ -32,6 +32,11 @@ struct mb_sim {
   int8_t *code = nullptr;
   double *df = nullptr, *rho = nullptr, *v[3] = {}, *f[3] = {};
   int64_t *id = nullptr;
+  // per-item masks of the outer stencil entries in the cutoff: written by each density
+  // pass, read by the force pass at the same positions (outer_ok: the phase-wise steps of
+  // a z-slab wrote them at the current positions)
+  uint2 *outer = nullptr;
+  bool outer_ok = false;
   // interstitials
   int n_itl = 0, cap_itl = 0, cap_flag = 0;
   double *ipos[2][3] = {}, *iv[3] = {}, *ifr[3] = {}, *irho = nullptr, *idf = nullptr;
@@ -168,11 +173,11 @@ static int step64(mb_sim *s, int energy, int kick_pre, int drift, int timed) {
   const int itl = itl_active(s);
   if (itl) MB_TRY(launch_itl_mark64(s->g, L, I, s->stream));
   if (timed) MB_CUDA(cudaEventRecord(s->ev[4], s->stream));
-  MB_TRY(launch_rho64(s->g, s->st, P, L, sp.rc2, ep, energy, itl, s->stream));
+  MB_TRY(launch_rho64(s->g, s->st, P, L, sp.rc2, ep, energy, itl, s->stream, 0, -1, s->outer));
   if (timed) MB_CUDA(cudaEventRecord(s->ev[5], s->stream));
   if (itl) MB_TRY(launch_itl_rho64(s->g, s->st, P, L, I, sp.rc2, ep, energy, s->stream));
   if (timed) MB_CUDA(cudaEventRecord(s->ev[6], s->stream));
-  MB_TRY(launch_force64(s->g, s->st, P, L, sp, ep, energy, itl, s->stream));
+  MB_TRY(launch_force64(s->g, s->st, P, L, sp, ep, energy, itl, s->stream, 0, -1, s->outer));
   if (timed) MB_CUDA(cudaEventRecord(s->ev[7], s->stream));
   if (itl) MB_TRY(launch_itl_force64(s->g, s->st, P, L, I, sp, ep, energy, s->stream));
   if (sp.conv2 > 0.0)
@@ -438,6 +443,8 @@ static int create_sim(const mb_sim_config *cfg, const mb_eam_tables *pot, int z_
   if (fp64) {
     if ((rc = dalloc(s, (void **)&s->df, ne * sizeof(double))) != MB_OK) return cleanup(rc);
     if ((rc = dalloc(s, (void **)&s->rho, ne * sizeof(double))) != MB_OK) return cleanup(rc);
+    if ((rc = dalloc(s, (void **)&s->outer, (size_t)items_per_box(s->g) * sizeof(uint2))) != MB_OK)
+      return cleanup(rc);
   }
   for (int c = 0; c < 3; c++) {
     if ((rc = dalloc(s, (void **)&s->v[c], ne * sizeof(double))) != MB_OK) return cleanup(rc);
@@ -493,7 +500,7 @@ int mb_sim_destroy(mb_sim *s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   drop_graph(s);
   if (s->ens) mb_ensemble_destroy(s->ens);
-  void *ptrs[] = {s->code, s->df, s->rho, s->id, s->epart, s->eout, s->stage, s->bad, s->irho, s->idf, s->itype,
+  void *ptrs[] = {s->code, s->df, s->rho, s->outer, s->id, s->epart, s->eout, s->stage, s->bad, s->irho, s->idf, s->itype,
                   s->iid, s->flag_list, s->flag_count, s->d_nitl, s->d_cand, s->d_cand_n, s->d_conv_counters};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -623,6 +630,7 @@ int mb_sim_upload(mb_sim *s, const mb_atom_element *box_atoms, const mb_atom_ele
   s->step = 0;
   s->n_e = 0;
   s->e_steps.clear();
+  s->outer_ok = false;
   MB_TRY(ensure_stage(s, (size_t)s->n_box));
   MB_CUDA(cudaMemcpyAsync(s->stage, box_atoms, (size_t)s->n_box * sizeof(mb_atom_element), cudaMemcpyHostToDevice,
                           s->stream));
@@ -808,9 +816,9 @@ static int step_host_whole(mb_sim *s, mb_atom_element *box_atoms, mb_atom_elemen
   const DevPot &P = pot_dev(s->pot);
   const int it = s->n_itl > 0;
   if (it) MB_TRY(launch_itl_mark64(s->g, L, I, s->stream));
-  MB_TRY(launch_rho64(s->g, s->st, P, L, sp.rc2, nullptr, 0, it, s->stream));
+  MB_TRY(launch_rho64(s->g, s->st, P, L, sp.rc2, nullptr, 0, it, s->stream, 0, -1, s->outer));
   if (it) MB_TRY(launch_itl_rho64(s->g, s->st, P, L, I, sp.rc2, nullptr, 0, s->stream));
-  MB_TRY(launch_force64(s->g, s->st, P, L, sp, nullptr, 0, it, s->stream));
+  MB_TRY(launch_force64(s->g, s->st, P, L, sp, nullptr, 0, it, s->stream, 0, -1, s->outer));
   if (it) MB_TRY(launch_itl_force64(s->g, s->st, P, L, I, sp, nullptr, 0, s->stream));
   MB_TRY(launch_pack_box_ids(s->g, s->stage, L, L.px, L.py, L.pz, sp.h, 0, s->id, s->stream));
   MB_CUDA(cudaMemcpyAsync(box_atoms, s->stage, (size_t)s->n_box * sizeof(mb_atom_element), cudaMemcpyDeviceToHost,
@@ -869,12 +877,12 @@ static int step_host_slabs(mb_sim *s, mb_atom_element *box_atoms, mb_atom_elemen
     return MB_OK;
   };
   auto rho = [&](int k) -> int {
-    MB_TRY(launch_rho64(g, s->st, P, L, sp.rc2, nullptr, 0, it, cs, zb[k], zb[k + 1]));
+    MB_TRY(launch_rho64(g, s->st, P, L, sp.rc2, nullptr, 0, it, cs, zb[k], zb[k + 1], s->outer));
     if (it) MB_TRY(launch_itl_rho64(g, s->st, P, L, I, sp.rc2, nullptr, 0, cs, zb[k], zb[k + 1]));
     return MB_OK;
   };
   auto force = [&](int k) -> int {
-    MB_TRY(launch_force64(g, s->st, P, L, sp, nullptr, 0, it, cs, zb[k], zb[k + 1]));
+    MB_TRY(launch_force64(g, s->st, P, L, sp, nullptr, 0, it, cs, zb[k], zb[k + 1], s->outer));
     if (it) MB_TRY(launch_itl_force64(g, s->st, P, L, I, sp, nullptr, 0, cs, zb[k], zb[k + 1]));
     MB_TRY(launch_pack_box_ids(g, s->stage, L, L.px, L.py, L.pz, sp.h, 0, s->id, cs, zb[k], zb[k + 1]));
     MB_CUDA(cudaEventRecord(s->ev_out[k], cs));
@@ -1005,6 +1013,7 @@ static int halo(mb_sim *s, int what, int pack, int side, void *buf, double z_shi
   if (!s || s->ens) return fail(MB_ERR_ARG, "bad arguments");
   if (!s->slab) return fail(MB_ERR_STATE, "halo layers belong to z-slab runs (mb_sim_create_slab)");
   double *c0 = what == 1 ? s->pos[s->cur][0] : s->df, *c1 = s->pos[s->cur][1], *c2 = s->pos[s->cur][2];
+  if (!pack && what != 2) s->outer_ok = false; // new ghost positions or codes: the masks are stale
   MB_TRY(launch_halo(s->g, what, pack, side, c0, c1, c2, s->code, buf, z_shift, s->stream));
   MB_CUDA(cudaStreamSynchronize(s->stream));
   return MB_OK;
@@ -1029,12 +1038,15 @@ int mb_sim_slab_phase(mb_sim *s, int32_t phase, int32_t energy) {
   double *ep = energy ? s->epart : nullptr;
   if (phase == 0) {
     if (energy) MB_CUDA(cudaMemsetAsync(s->epart, 0, sizeof(double) * energy_partials_needed(), s->stream));
-    MB_TRY(launch_rho64(s->g, s->st, P, L, s->cfg.cutoff * s->cfg.cutoff, ep, energy, 0, s->stream));
+    MB_TRY(launch_rho64(s->g, s->st, P, L, s->cfg.cutoff * s->cfg.cutoff, ep, energy, 0, s->stream, 0, -1,
+                        s->outer));
+    s->outer_ok = true;
     return MB_OK;
   }
   // forces at pos[cur], closing kick of the previous step (once primed), drift to pos[cur ^ 1]
   const StepParams sp = sim_params(s, s->primed ? 1 : 0, 1);
-  MB_TRY(launch_force64(s->g, s->st, P, L, sp, ep, energy, 0, s->stream));
+  MB_TRY(launch_force64(s->g, s->st, P, L, sp, ep, energy, 0, s->stream, 0, -1, s->outer_ok ? s->outer : nullptr));
+  s->outer_ok = false;
   const long long n = s->primed ? s->step + 1 : 0;
   s->step = n;
   if (energy) {
