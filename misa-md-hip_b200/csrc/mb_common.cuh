@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include <string>
 #include <vector>
@@ -197,6 +198,13 @@ int launch_force64(const Geom &g, const StencilSet &st, const DevPot &pot, const
                    const uint2 *outer = nullptr);
 // Work items (32-site row chunks) of the whole box: the length of the outer masks.
 inline long long items_per_box(const Geom &g) { return (long long)((g.bcx + 31) / 32) * g.by * 2 * g.bz; }
+// Outer-entry masks on (default), or off when MB_OUTER_MASKS=0 (the force passes then walk
+// every outer entry: the same results, kept for checking that); read when a sim is
+// created or an ensemble's walk is rebuilt.
+inline bool outer_masks_on() {
+  const char *v = getenv("MB_OUTER_MASKS");
+  return !(v && v[0] == '0');
+}
 int launch_itl_mark64(const Geom &g, const Lattice64 &L, const Itl64 &I, cudaStream_t s);
 // Flags the sites of layers [z0, z1) near an interstitial, without clearing or
 // resetting the list first.

@@ -194,6 +194,7 @@ struct mb_ensemble {
   int split = 0; // kernels in use: 0 persistent, 1 split with the brick walk, 2 split with the linear walk
   unsigned *d_item_first = nullptr; // linear walk: first item of each lattice
   double *d_epart_items = nullptr;  // split: energy partials per walk item
+  uint2 *d_outer_items = nullptr;   // split: outer-entry masks per walk item
   size_t cap_items = 0;
   int *d_icell = nullptr; // interstitial cell lists of every lattice (rebuilt each step)
   size_t cap_icell = 0;
@@ -543,13 +544,18 @@ static int rebuild(mb_ensemble *e) {
     W.n_items = (unsigned)n_items;
     if (n_items > e->cap_items) {
       const size_t C = std::max<size_t>((size_t)n_items, 2 * e->cap_items);
+      const size_t per = 2 * sizeof(double) + sizeof(uint2);
       if (e->d_epart_items) {
         cudaFree(e->d_epart_items);
-        e->device_bytes -= e->cap_items * 2 * sizeof(double);
-        e->fixed_bytes -= e->cap_items * 2 * sizeof(double);
+        cudaFree(e->d_outer_items);
+        e->device_bytes -= e->cap_items * per;
+        e->fixed_bytes -= e->cap_items * per;
       }
       e->d_epart_items = nullptr;
+      e->d_outer_items = nullptr;
+      e->cap_items = 0;
       MB_TRY(edalloc(e, (void **)&e->d_epart_items, C * 2 * sizeof(double)));
+      MB_TRY(edalloc(e, (void **)&e->d_outer_items, C * sizeof(uint2)));
       e->cap_items = C;
     }
     MB_CUDA(cudaMemcpyAsync(e->d_item_first, first.data(), sizeof(unsigned) * (nl + 1), cudaMemcpyHostToDevice,
@@ -557,6 +563,7 @@ static int rebuild(mb_ensemble *e) {
     MB_CUDA(cudaStreamSynchronize(e->stream));
     W.item_first = e->d_item_first;
     P.epart = e->d_epart_items;
+    P.outer = outer_masks_on() ? e->d_outer_items : nullptr;
   }
   e->dirty = false;
   return MB_OK;
@@ -898,7 +905,7 @@ int mb_ensemble_destroy(mb_ensemble *e) {
   for (auto &L : e->slots) free_slot(e, L);
   void *ptrs[] = {e->d_lats, e->d_tile_lat, e->d_tile_idx, e->d_tile_first, e->d_itl_lats, e->d_tmaps,
                   e->d_epart, e->d_eout, e->d_eitl, e->d_bar, e->d_err, e->d_bad, e->d_item_first,
-                  e->d_epart_items, e->d_icell};
+                  e->d_epart_items, e->d_outer_items, e->d_icell};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &ev : e->ev)

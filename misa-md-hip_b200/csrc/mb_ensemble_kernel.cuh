@@ -101,6 +101,8 @@ struct EnsParams {
   unsigned bar_spins; // polls a grid barrier makes before it gives up (ENS_BAR_SPINS by default)
   int *err;
   double *epart; // [tile][2]
+  uint2 *outer;  // split kernels: per walk item, the branch-walked built-in stencil entries some site
+                 // has inside the cutoff (written by the density pass, read by the force pass)
   const int *itl_lats;
   int n_itl_lats;
   int energy;

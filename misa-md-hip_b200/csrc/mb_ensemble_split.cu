@@ -197,9 +197,17 @@ __device__ __forceinline__ void mx_unpack(unsigned p, int &s, int &cx, int &y, i
   s = (int)(p >> 31);
 }
 
+// Margin (A^2) of the outer-entry masks over the pair test num < w: a pair the force
+// pass finds inside the cutoff is in the mask whatever the FMA contraction of either
+// pass.
+#define MX_MASK_MARGIN 1e-3f
+
+// near: bit k - 64 set when branch-walked built-in entry k (shells 7 and 8) is inside
+// the cutoff (plus MX_MASK_MARGIN) for this site.
 template <bool ENERGY, int FIXED>
 __device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStencil &S, const LatDesc &d,
-                                              const float2 *s_f, float ma0, long long i, unsigned pos) {
+                                              const float2 *s_f, float ma0, long long i, unsigned pos,
+                                              unsigned long long &near) {
   const int s = (int)(pos >> 31);
   const int code = d.code[i];
   if (code < 0) return 0.0;
@@ -221,6 +229,7 @@ __device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStenci
       float2 exy;
       float ez, q;
       const float num = mxc_num<k>(ma0, u, nb, exy, ez);
+      near |= (unsigned long long)(num < Q.w[HStore<k>::sh] + MX_MASK_MARGIN) << (k - nbf);
       if (num < Q.w[HStore<k>::sh]) {
         const int m = mxc_index<k, 0>(Q, num, q);
         const float2 t = s_f[m];
@@ -267,10 +276,13 @@ __device__ __forceinline__ double mx_rho_site(const EnsParams &P, const MxStenci
 
 // Force + velocity-Verlet of one site; adds pair energy and kinetic energy.  Pair terms
 // are added two at a time before one compensated add.
+// outer: the branch-walked built-in entries (bit k - 64) that some site of this item has
+// inside the cutoff at these positions (the density pass's masks); the others are not
+// loaded.
 template <bool ENERGY, int FIXED>
 __device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStencil &S, const LatDesc &d,
                                               const float2 *s_ab, float ma0, long long i, unsigned pos,
-                                              double &e_pair, double &e_kin) {
+                                              unsigned long long outer, double &e_pair, double &e_kin) {
   const int s = (int)(pos >> 31);
   const int code = d.code[i];
   if (code < 0) return;
@@ -304,15 +316,17 @@ __device__ __forceinline__ void mx_force_site(const EnsParams &P, const MxStenci
     });
     static_for<nbf, kBcc.start[FIXED]>([&](auto kc) {
       constexpr int k = decltype(kc)::value;
-      const float4 nb = mxc_load<k>(b);
-      float2 exy;
-      float ez;
-      const float num = mxc_num<k>(ma0, u, nb, exy, ez);
-      if (num < Q.w[HStore<k>::sh]) {
-        float2 d0;
-        float z0, e0 = 0.f;
-        const float f0 = mxc_force<k, ENERGY>(Q, ma0, b, u, s_ab, ptab, d0, z0, e0);
-        add1(d0, z0, f0, e0);
+      if ((outer >> (k - nbf)) & 1ull) {
+        const float4 nb = mxc_load<k>(b);
+        float2 exy;
+        float ez;
+        const float num = mxc_num<k>(ma0, u, nb, exy, ez);
+        if (num < Q.w[HStore<k>::sh]) {
+          float2 d0;
+          float z0, e0 = 0.f;
+          const float f0 = mxc_force<k, ENERGY>(Q, ma0, b, u, s_ab, ptab, d0, z0, e0);
+          add1(d0, z0, f0, e0);
+        }
       }
     });
   } else {
@@ -403,7 +417,13 @@ __global__ void __launch_bounds__(MX_RHO_THREADS, 1)
     const bool ok = mx_locate<WALK>(P, S.walk, lat, item, lane, at, s, cx, y, z, i);
     const LatDesc &d = P.lats[at.l];
     double e = 0.0;
-    if (ok && lat_active(d)) e = mx_rho_site<ENERGY, FIXED>(P, S, d, s_f, ma0, i, mx_pack(s, cx, y, z));
+    unsigned long long near = 0;
+    if (ok && lat_active(d)) e = mx_rho_site<ENERGY, FIXED>(P, S, d, s_f, ma0, i, mx_pack(s, cx, y, z), near);
+    if (FIXED && P.outer) {
+      const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)near);
+      const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(near >> 32));
+      if (lane == 0) P.outer[item] = make_uint2(lo, hi);
+    }
     if (ENERGY) {
       e = warp_sum(e);
       if (lane == 0) P.epart[2 * (size_t)item] = e;
@@ -433,7 +453,13 @@ __global__ void __launch_bounds__(MX_FORCE_THREADS, 1)
     const bool ok = mx_locate<WALK>(P, S.walk, lat, item, lane, at, s, cx, y, z, i);
     const LatDesc &d = P.lats[at.l];
     double ep = 0.0, ek = 0.0;
-    if (ok && lat_active(d)) mx_force_site<ENERGY, FIXED>(P, S, d, s_ab, ma0, i, mx_pack(s, cx, y, z), ep, ek);
+    unsigned long long outer = ~0ull;
+    if (FIXED && P.outer) {
+      const uint2 m2 = P.outer[item];
+      outer = (unsigned long long)m2.x | ((unsigned long long)m2.y << 32);
+    }
+    if (ok && lat_active(d))
+      mx_force_site<ENERGY, FIXED>(P, S, d, s_ab, ma0, i, mx_pack(s, cx, y, z), outer, ep, ek);
     if (ENERGY) {
       ep = warp_sum(ep);
       ek = warp_sum(ek);

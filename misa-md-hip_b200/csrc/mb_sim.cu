@@ -443,7 +443,8 @@ static int create_sim(const mb_sim_config *cfg, const mb_eam_tables *pot, int z_
   if (fp64) {
     if ((rc = dalloc(s, (void **)&s->df, ne * sizeof(double))) != MB_OK) return cleanup(rc);
     if ((rc = dalloc(s, (void **)&s->rho, ne * sizeof(double))) != MB_OK) return cleanup(rc);
-    if ((rc = dalloc(s, (void **)&s->outer, (size_t)items_per_box(s->g) * sizeof(uint2))) != MB_OK)
+    if (outer_masks_on() &&
+        (rc = dalloc(s, (void **)&s->outer, (size_t)items_per_box(s->g) * sizeof(uint2))) != MB_OK)
       return cleanup(rc);
   }
   for (int c = 0; c < 3; c++) {

@@ -66,3 +66,49 @@ def test_masked_outer_walk_equals_the_full_walk_bitwise():
     for k in ("x", "v", "f", "rho", "df"):
         assert np.array_equal(masked[k], full[k]), k
     assert np.array_equal(e_masked, e_full)
+
+
+@pytest.fixture
+def masks_off(monkeypatch):
+    def off():
+        monkeypatch.setenv("MB_OUTER_MASKS", "0")
+    return off
+
+
+def _sim_run(sc, precision, nsteps):
+    with mb.Sim(sc.cells, sc.tables, lattice_const=A0, mass=MASS, dt=1.0, cutoff=sc.cutoff,
+                stencil_skin=sc.skin, precision=precision, max_interstitials=max(1, sc.itl.shape[0])) as sim:
+        sim.upload(sc.box, sc.itl if sc.itl.shape[0] else None)
+        sim.run(nsteps)
+        return sim.download()
+
+
+@pytest.mark.parametrize("precision", [mb.MB_PREC_FP64, mb.MB_PREC_MIXED])
+def test_device_resident_steps_with_and_without_masks_are_bitwise_equal(precision, masks_off):
+    # 40 cells along x: the mixed path takes its brick walk; interstitials flag sites
+    sc = make(cells=(40, 12, 10), temperature=900.0, vacancy=0.01, n_itl=3, seed=29, jitter=0.15)
+    b1, i1 = _sim_run(sc, precision, 5)
+    masks_off()
+    b2, i2 = _sim_run(sc, precision, 5)
+    for k in ("x", "v", "f"):
+        assert np.array_equal(b1[k], b2[k]), k
+        assert np.array_equal(i1[k], i2[k]), k
+
+
+def test_batched_small_lattices_with_and_without_masks_are_bitwise_equal(masks_off):
+    # lattices narrower than 32 cells: the linear walk over every lattice's items
+    scs = [make(cells=c, temperature=900.0, vacancy=0.01, seed=40 + k, jitter=0.15)
+           for k, c in enumerate([(8, 9, 10), (12, 8, 8), (16, 10, 6)])]
+    kw = dict(lattice_const=A0, mass=MASS, dt=1.0, cutoff=scs[0].cutoff, stencil_skin=scs[0].skin)
+
+    def run():
+        with mb.Ensemble(scs[0].tables, **kw) as ens:
+            slots = [ens.add(sc.cells, sc.box, steps=0) for sc in scs]
+            ens.run(5)
+            return [ens.download(s)[0] for s in slots]
+
+    a = run()
+    masks_off()
+    b = run()
+    for x, y in zip(a, b):
+        assert np.array_equal(x["x"], y["x"]) and np.array_equal(x["f"], y["f"])
