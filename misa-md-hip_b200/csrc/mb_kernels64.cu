@@ -354,10 +354,20 @@ __global__ void __launch_bounds__(MB_FORCE_THREADS, 1)
       }
       if (k < st.n_near) force_term<ENERGY, true>(a, L, s_f1, i + off[k++], xi, yi, zi, dfi, fx, fy, fz, ep);
       if (n_outer <= 64) {
-        // set bits in ascending k, the order of the full walk
-        for (unsigned long long m = outer; m; m &= m - 1) {
-          const int kk = st.n_near + __ffsll((long long)m) - 1;
-          force_term<ENERGY, false>(a, L, s_f1, i + off[kk], xi, yi, zi, dfi, gx, gy, gz, eq);
+        // set bits in ascending k, the order of the full walk, two per trip so that two
+        // neighbour rows are in flight
+        unsigned long long m = outer;
+        while (m) {
+          const int k1 = st.n_near + __ffsll((long long)m) - 1;
+          m &= m - 1;
+          if (m) {
+            const int k2 = st.n_near + __ffsll((long long)m) - 1;
+            m &= m - 1;
+            force_term<ENERGY, false>(a, L, s_f1, i + off[k1], xi, yi, zi, dfi, gx, gy, gz, eq);
+            force_term<ENERGY, false>(a, L, s_f1, i + off[k2], xi, yi, zi, dfi, gx, gy, gz, eq);
+          } else {
+            force_term<ENERGY, false>(a, L, s_f1, i + off[k1], xi, yi, zi, dfi, gx, gy, gz, eq);
+          }
         }
       } else {
 #pragma unroll 2
