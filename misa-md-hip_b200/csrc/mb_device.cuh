@@ -179,6 +179,44 @@ __device__ __forceinline__ bool window_site(const Geom &g, const Window &w, int 
   return true;
 }
 
+// The reach test of candidate c alone (the same arithmetic as window_site /
+// window_site_rel, so the same candidates pass).
+__device__ __forceinline__ bool window_in_reach(const Window &w, int c, double qx, double qy, double qz, double a0,
+                                                double R) {
+  const int ix = c % w.nx;
+  const int rest = c / w.nx;
+  const int iy = rest % w.ny;
+  const int iz = rest / w.ny;
+  const int gx = w.gx0 + ix, gy = w.gy0 + iy, gz = w.gz0 + iz;
+  const double h = 0.5 * (double)(gx & 1);
+  const double ox = 0.5 * a0 * gx - qx, oy = a0 * (gy + h) - qy, oz = a0 * (gz + h) - qz;
+  return ox * ox + oy * oy + oz * oz < R * R;
+}
+
+// In-reach candidates of a window, listed by one warp in candidate order: list[k] for
+// k < the returned count (list: this warp's cap entries of shared memory).  The reach
+// test is cheap arithmetic and about 1 candidate in 8 passes (a sphere in its bounding
+// box of sites), so the walk that follows loads only real sites, several per lane at
+// once, instead of one dependent load chain per round of 32 candidates.  Returns -1
+// when more than cap candidates pass (the caller then walks every candidate).
+__device__ __forceinline__ int window_compact(const Window &w, double qx, double qy, double qz, double a0, double R,
+                                              int *list, int cap) {
+  const int lane = threadIdx.x & 31;
+  const int ncand = w.nx * w.ny * w.nz;
+  int n = 0;
+  for (int base = 0; base < ncand; base += 32) {
+    const int c = base + lane;
+    const bool in = c < ncand && window_in_reach(w, c, qx, qy, qz, a0, R);
+    const unsigned m = __ballot_sync(0xffffffffu, in);
+    const int k = n + __popc(m & ((1u << lane) - 1u));
+    if (in && k < cap) list[k] = c;
+    n += __popc(m);
+  }
+  __syncwarp();
+  return n <= cap ? n : -1;
+}
+#define MB_WIN_LIST 256 // compacted window entries per warp
+
 // Same candidate walk, returning the ideal image position relative to the query point
 // (ox, oy, oz) instead of the periodic shift.
 __device__ __forceinline__ bool window_site_rel(const Geom &g, const Window &w, int c, double qx, double qy,

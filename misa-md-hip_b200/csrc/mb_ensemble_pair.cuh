@@ -129,15 +129,19 @@ __device__ __forceinline__ void itl_clear_flags(const LatDesc &d) {
   if (blockIdx.x == 0 && threadIdx.x == 0) d.flag_count[cur] = 0;
 }
 
-// Warp `w` of the grid flags the lattice sites within reach of interstitial w.
-__device__ __forceinline__ void itl_mark_one(const EnsParams &P, const LatDesc &d, int it) {
+// Warp `w` of the grid flags the lattice sites within reach of interstitial w.  With
+// `list` (this warp's MB_WIN_LIST entries of shared memory) the in-reach candidates are
+// listed first and the lanes then flag only those.
+__device__ __forceinline__ void itl_mark_one(const EnsParams &P, const LatDesc &d, int it, int *list = nullptr) {
   const Geom g = lat_geom(d);
   const int lane = threadIdx.x & 31;
   const int cur = d.cur;
   const double qx = d.ipx[cur][it], qy = d.ipy[cur][it], qz = d.ipz[cur][it];
   const Window w = make_window(qx, qy, qz, P.a0, P.reach);
-  const int ncand = w.nx * w.ny * w.nz;
-  for (int c = lane; c < ncand; c += 32) {
+  const int nlist = list ? window_compact(w, qx, qy, qz, P.a0, P.reach, list, MB_WIN_LIST) : -1;
+  const int ncand = nlist >= 0 ? nlist : w.nx * w.ny * w.nz;
+  for (int k = lane; k < ncand; k += 32) {
+    const int c = nlist >= 0 ? list[k] : k;
     long long idx;
     double sx, sy, sz;
     if (!window_site(g, w, c, qx, qy, qz, P.a0, P.reach, idx, sx, sy, sz)) continue;
@@ -195,13 +199,148 @@ __device__ __forceinline__ void itl_pairs(const LatDesc &d, const Geom &g, int c
   }
 }
 
+// Last part of an item, on one lane, from its summed pairs: df (density pass), or force,
+// velocity-Verlet, drift and ghost images (force pass), of a flagged site (i at s, cx, y,
+// z) or of interstitial it.
+template <bool FORCE, bool ENERGY>
+__device__ __forceinline__ void itl_finish(const EnsParams &P, const LatDesc &d, const Geom &g, bool is_site,
+                                           long long i, int s, int cx, int y, int z, int it, int ti, double xi,
+                                           double yi, double zi, double rho, double fx, double fy, double fz,
+                                           double ep) {
+  const int cur = d.cur;
+  if (!FORCE) {
+    const double df = dF64(P.P, ti, rho);
+    if (is_site) {
+      float4 *uw = d.u4[cur];
+      reinterpret_cast<float *>(uw + i)[3] = (float)df;
+      d.rho[i] = (float)rho;
+      for_images(g, s, cx, y, z,
+                 [&](long long idx, double, double, double) { reinterpret_cast<float *>(uw + idx)[3] = (float)df; });
+    } else {
+      d.irho[it] = rho;
+      d.idf[it] = df;
+    }
+    if (ENERGY) atomicAdd(&d.e_itl[0], F64(P.P, ti, rho));
+    return;
+  }
+  double vx, vy, vz;
+  if (is_site) {
+    d.fx[i] = (float)fx;
+    d.fy[i] = (float)fy;
+    d.fz[i] = (float)fz;
+    vx = d.vx[i];
+    vy = d.vy[i];
+    vz = d.vz[i];
+  } else {
+    d.ifx[it] = fx;
+    d.ify[it] = fy;
+    d.ifz[it] = fz;
+    vx = d.ivx[it];
+    vy = d.ivy[it];
+    vz = d.ivz[it];
+  }
+  if (d.primed) {
+    vx += P.h * fx;
+    vy += P.h * fy;
+    vz += P.h * fz;
+  }
+  if (ENERGY) {
+    atomicAdd(&d.e_itl[0], ep);
+    atomicAdd(&d.e_itl[1], 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E);
+  }
+  vx += P.h * fx;
+  vy += P.h * fy;
+  vz += P.h * fz;
+  if (is_site) {
+    d.vx[i] = vx;
+    d.vy[i] = vy;
+    d.vz[i] = vz;
+    const double nx = d.ux[i] + P.dt * vx, ny = d.uy[i] + P.dt * vy, nz = d.uz[i] + P.dt * vz;
+    d.ux[i] = nx;
+    d.uy[i] = ny;
+    d.uz[i] = nz;
+    const float4 nu = make_float4((float)nx, (float)ny, (float)nz, 0.f);
+    float4 *un = d.u4[cur ^ 1];
+    un[i] = nu;
+    ens_conv_check(P, d, s, cx, y, z, nx, ny, nz);
+    for_images(g, s, cx, y, z, [&](long long idx, double, double, double) { un[idx] = nu; });
+  } else {
+    d.ivx[it] = vx;
+    d.ivy[it] = vy;
+    d.ivz[it] = vz;
+    d.ipx[cur ^ 1][it] = xi + P.dt * vx;
+    d.ipy[cur ^ 1][it] = yi + P.dt * vy;
+    d.ipz[cur ^ 1][it] = zi + P.dt * vz;
+  }
+}
+
+// Sum over the 8 lanes of a group (lanes 8g .. 8g + 7), in a fixed order.
+__device__ __forceinline__ double group8_sum(double v) {
+  v += __shfl_xor_sync(0xffffffffu, v, 4);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  return v;
+}
+
+// Pairs of interstitial it (position xi, yi, zi) with the lattice sites of its window,
+// one warp, handed to pair (which sums them per lane).  With `list` (this warp's MB_WIN_LIST entries of shared
+// memory) the in-reach sites are listed first and each lane then loads up to four of
+// them at once; without it (or when more than MB_WIN_LIST sites are in reach) every
+// candidate of the window is visited in rounds of 32.
+template <class Pair>
+__device__ __forceinline__ void itl_window_pairs(const EnsParams &P, const LatDesc &d, const Geom &g,
+                                                 const float4 *u4, double xi, double yi, double zi, int *list,
+                                                 bool with_df, Pair pair) {
+  const int lane = threadIdx.x & 31;
+  const Window win = make_window(xi, yi, zi, P.a0, P.reach);
+  const int n = list ? window_compact(win, xi, yi, zi, P.a0, P.reach, list, MB_WIN_LIST) : -1;
+  if (n >= 0) {
+    for (int k0 = 0; k0 < n; k0 += 128) {
+      long long j[4];
+      double ox[4], oy[4], oz[4];
+      bool ok[4];
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        const int k = k0 + 32 * t + lane;
+        j[t] = 0;
+        ox[t] = oy[t] = oz[t] = 0.0;
+        ok[t] = k < n && window_site_rel(g, win, list[k], xi, yi, zi, P.a0, P.reach, j[t], ox[t], oy[t], oz[t]);
+      }
+      int cj[4];
+      float4 uj[4];
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        cj[t] = ok[t] ? (int)d.code[j[t]] : -1;
+        uj[t] = ok[t] ? u4[j[t]] : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int t = 0; t < 4; t++)
+        if (cj[t] >= 0)
+          pair(-(ox[t] + (double)uj[t].x), -(oy[t] + (double)uj[t].y), -(oz[t] + (double)uj[t].z), cj[t] & 0x3F,
+               with_df ? (double)uj[t].w : 0.0);
+    }
+    return;
+  }
+  const int ncand = win.nx * win.ny * win.nz;
+  for (int c = lane; c < ncand; c += 32) {
+    long long j;
+    double ox, oy, oz;
+    if (!window_site_rel(g, win, c, xi, yi, zi, P.a0, P.reach, j, ox, oy, oz)) continue;
+    const int cj = d.code[j];
+    if (cj < 0) continue;
+    const float4 uj = u4[j];
+    pair(-(ox + (double)uj.x), -(oy + (double)uj.y), -(oz + (double)uj.z), cj & 0x3F, with_df ? (double)uj.w : 0.0);
+  }
+}
+
 // Work of one warp on item w of lattice d: a flagged site (w < nflag) or an
 // interstitial.  FORCE = false: density pass; true: force + integration pass.  A
 // flagged site's lattice-pair part comes from the lattice kernels (rho / f of the site);
 // its interstitial pairs, df, integration and ghost images are done here.  An
 // interstitial's pairs (lattice window and other interstitials) are all done here, FP64.
+// `list`: see itl_window_pairs.
 template <bool FORCE, bool ENERGY, bool CELLS>
-__device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag) {
+__device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag, int *list = nullptr) {
   const int lane = threadIdx.x & 31;
   const Geom g = lat_geom(d);
   const int cur = d.cur;
@@ -259,105 +398,133 @@ __device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag)
       }
     }
   } else {
-    const Window win = make_window(xi, yi, zi, P.a0, P.reach);
-    const int ncand = win.nx * win.ny * win.nz;
-    for (int c = lane; c < ncand; c += 32) {
-      long long j;
-      double ox, oy, oz;
-      if (!window_site_rel(g, win, c, xi, yi, zi, P.a0, P.reach, j, ox, oy, oz)) continue;
-      const int cj = d.code[j];
-      if (cj < 0) continue;
-      const float4 uj = u4[j];
-      pair(-(ox + (double)uj.x), -(oy + (double)uj.y), -(oz + (double)uj.z), cj & 0x3F, FORCE ? (double)uj.w : 0.0);
-    }
+    itl_window_pairs(P, d, g, u4, xi, yi, zi, list, FORCE, pair);
   }
   itl_pairs<CELLS>(d, g, cur, xi, yi, zi, is_site ? -1 : it, lane, pair, FORCE);
   if (!FORCE) {
     acc0 = warp_sum(acc0);
-    if (lane == 0) {
-      const double df = dF64(P.P, ti, acc0);
-      if (is_site) {
-        float4 *uw = d.u4[cur];
-        reinterpret_cast<float *>(uw + i)[3] = (float)df;
-        d.rho[i] = (float)acc0;
-        for_images(g, s, cx, y, z,
-                   [&](long long idx, double, double, double) { reinterpret_cast<float *>(uw + idx)[3] = (float)df; });
-      } else {
-        d.irho[it] = acc0;
-        d.idf[it] = df;
-      }
-      if (ENERGY) atomicAdd(&d.e_itl[0], F64(P.P, ti, acc0));
-    }
-    return;
-  }
-  fx = warp_sum(fx);
-  fy = warp_sum(fy);
-  fz = warp_sum(fz);
-  if (ENERGY) ep = warp_sum(ep);
-  if (lane != 0) return;
-  double vx, vy, vz;
-  if (is_site) {
-    d.fx[i] = (float)fx;
-    d.fy[i] = (float)fy;
-    d.fz[i] = (float)fz;
-    vx = d.vx[i];
-    vy = d.vy[i];
-    vz = d.vz[i];
   } else {
-    d.ifx[it] = fx;
-    d.ify[it] = fy;
-    d.ifz[it] = fz;
-    vx = d.ivx[it];
-    vy = d.ivy[it];
-    vz = d.ivz[it];
+    fx = warp_sum(fx);
+    fy = warp_sum(fy);
+    fz = warp_sum(fz);
+    if (ENERGY) ep = warp_sum(ep);
   }
-  if (d.primed) {
-    vx += P.h * fx;
-    vy += P.h * fy;
-    vz += P.h * fz;
-  }
-  if (ENERGY) {
-    atomicAdd(&d.e_itl[0], ep);
-    atomicAdd(&d.e_itl[1], 0.5 * P.mass * (vx * vx + vy * vy + vz * vz) * MB_MVV2E);
-  }
-  vx += P.h * fx;
-  vy += P.h * fy;
-  vz += P.h * fz;
-  if (is_site) {
-    d.vx[i] = vx;
-    d.vy[i] = vy;
-    d.vz[i] = vz;
-    const double nx = d.ux[i] + P.dt * vx, ny = d.uy[i] + P.dt * vy, nz = d.uz[i] + P.dt * vz;
-    d.ux[i] = nx;
-    d.uy[i] = ny;
-    d.uz[i] = nz;
-    const float4 nu = make_float4((float)nx, (float)ny, (float)nz, 0.f);
-    float4 *un = d.u4[cur ^ 1];
-    un[i] = nu;
-    ens_conv_check(P, d, s, cx, y, z, nx, ny, nz);
-    for_images(g, s, cx, y, z, [&](long long idx, double, double, double) { un[idx] = nu; });
-  } else {
-    d.ivx[it] = vx;
-    d.ivy[it] = vy;
-    d.ivz[it] = vz;
-    d.ipx[cur ^ 1][it] = xi + P.dt * vx;
-    d.ipy[cur ^ 1][it] = yi + P.dt * vy;
-    d.ipz[cur ^ 1][it] = zi + P.dt * vz;
-  }
+  if (lane == 0) itl_finish<FORCE, ENERGY>(P, d, g, is_site, i, s, cx, y, z, it, ti, xi, yi, zi, acc0, fx, fy, fz, ep);
 }
 
-// CELLS: the split kernels' per-step interstitial cell list applies (the persistent
-// kernel walks whole lists).
+// Flagged lattice site w of lattice d, worked by the 8-lane group of this lane (a warp
+// works four sites at once; every lane of the warp takes part in the group sums, with a
+// site or not): the lattice kernels summed its lattice pairs (FP32, compensated) into
+// rho / f, the group adds its interstitial pairs in FP64 (lane l of the group walks cells
+// l, l + 8, l + 16, l + 24 of the 27 around the site in the split kernels' cell list, or
+// list entries l, l + 8, ... without one) and its first lane finishes the site.  A
+// flagged site's item is a chain of dependent loads with little work, so four of them
+// per warp keep four chains in flight.
+template <bool FORCE, bool ENERGY>
+__device__ void itl_site_group(const EnsParams &P, const LatDesc &d, int w, bool valid) {
+  const int l8 = threadIdx.x & 7;
+  const Geom g = lat_geom(d);
+  const int cur = d.cur;
+  long long i = 0;
+  int s = 0, cx = 0, y = 0, z = 0, ti = 0;
+  double xi = 0.0, yi = 0.0, zi = 0.0, dfi = 0.0;
+  double acc0 = 0.0, fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
+  auto pair = [&](double dx, double dy, double dz, int tj, double dfj) {
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 >= P.rc2) return;
+    const double rinv = rsqrt(d2);
+    const double r = d2 * rinv;
+    if (!FORCE) {
+      acc0 += rho_of_r(P.P, tj, r);
+    } else {
+      double ph = 0.0;
+      const double psip = pair_psip(P.P, ti, tj, r, dfi, dfj, ENERGY ? &ph : nullptr);
+      const double fpair = -psip * rinv;
+      fx += dx * fpair;
+      fy += dy * fpair;
+      fz += dz * fpair;
+      if (ENERGY) ep += 0.5 * ph;
+    }
+  };
+  if (valid) {
+    i = d.flag_list[w];
+    decode_ext(g, i, s, cx, y, z);
+    ti = d.code[i] & 0x3F;
+    double X, Y, Z;
+    ideal_pos(s, cx, y, z, P.a0, X, Y, Z);
+    xi = X + d.ux[i];
+    yi = Y + d.uy[i];
+    zi = Z + d.uz[i];
+    if (FORCE) dfi = (double)d.u4[cur][i].w;
+    if (l8 == 0) {
+      if (FORCE) {
+        fx = (double)d.fx[i];
+        fy = (double)d.fy[i];
+        fz = (double)d.fz[i];
+      } else {
+        acc0 = (double)d.rho[i];
+      }
+    }
+    if (d.icount && d.iflag[0]) {
+      int qx, qy, qz;
+      itl_cell3(d, xi, yi, zi, qx, qy, qz);
+      for (int cc = l8; cc < 27; cc += 8) {
+        const int ox = cc % 3 - 1, oy = (cc / 3) % 3 - 1, oz = cc / 9 - 1;
+        const int ccx = (qx + ox + d.icn[0]) % d.icn[0], ccy = (qy + oy + d.icn[1]) % d.icn[1],
+                  ccz = (qz + oz + d.icn[2]) % d.icn[2];
+        const int c = (ccz * d.icn[1] + ccy) * d.icn[0] + ccx;
+        const int n = d.icount[c], s0 = d.istart[c];
+        for (int jj = s0; jj < s0 + n; jj++) {
+          const int K = d.iitem[jj];
+          pair(min_image(xi - d.ipx[cur][K], g.Lx, g.iLx), min_image(yi - d.ipy[cur][K], g.Ly, g.iLy),
+               min_image(zi - d.ipz[cur][K], g.Lz, g.iLz), d.itype[K], FORCE ? d.idf[K] : 0.0);
+        }
+      }
+    } else {
+      for (int K = l8; K < d.n_itl; K += 8)
+        pair(min_image(xi - d.ipx[cur][K], g.Lx, g.iLx), min_image(yi - d.ipy[cur][K], g.Ly, g.iLy),
+             min_image(zi - d.ipz[cur][K], g.Lz, g.iLz), d.itype[K], FORCE ? d.idf[K] : 0.0);
+    }
+  }
+  if (!FORCE) {
+    acc0 = group8_sum(acc0);
+  } else {
+    fx = group8_sum(fx);
+    fy = group8_sum(fy);
+    fz = group8_sum(fz);
+    if (ENERGY) ep = group8_sum(ep);
+  }
+  if (valid && l8 == 0)
+    itl_finish<FORCE, ENERGY>(P, d, g, true, i, s, cx, y, z, 0, ti, xi, yi, zi, acc0, fx, fy, fz, ep);
+}
+
+// Items of every lattice that holds interstitials.  Split kernels (CELLS: their per-step
+// interstitial cell list applies; `list`: this warp's window list): the interstitials
+// first, one warp each, so that their window walks (the longest items) start at once,
+// then the flagged sites four to a warp.  Persistent kernel: one item per warp, whole
+// interstitial lists.
 template <bool FORCE, bool ENERGY, bool CELLS = false>
-__device__ void itl_items(const EnsParams &P) {
+__device__ void itl_items(const EnsParams &P, int *list = nullptr) {
   const int warps = gridDim.x * (blockDim.x >> 5);
   const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   for (int q = 0; q < P.n_itl_lats; q++) {
     const LatDesc &d = P.lats[P.itl_lats[q]];
     if (!lat_active(d)) continue;
     const int nflag = min(d.flag_count[d.cur], d.cap_flag);
-    const int n = nflag + d.n_itl;
-    for (int w = gw; w < n; w += warps) itl_item<FORCE, ENERGY, CELLS>(P, d, w, nflag);
+    if (CELLS) {
+      const int n = d.n_itl + (nflag + 3) / 4;
+      for (int w = gw; w < n; w += warps) {
+        if (w < d.n_itl) {
+          itl_item<FORCE, ENERGY, true>(P, d, nflag + w, nflag, list);
+        } else {
+          const int f = 4 * (w - d.n_itl) + (int)((threadIdx.x & 31) >> 3);
+          itl_site_group<FORCE, ENERGY>(P, d, f, f < nflag);
+        }
+      }
+    } else {
+      const int n = nflag + d.n_itl;
+      for (int w = gw; w < n; w += warps) itl_item<FORCE, ENERGY, false>(P, d, w, nflag);
+    }
   }
 }
 

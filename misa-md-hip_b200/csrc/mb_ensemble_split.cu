@@ -531,19 +531,24 @@ __global__ void __launch_bounds__(MX_BIN_THREADS, 1) k_mx_itl_bin(const __grid_c
   }
 }
 
-__global__ void k_mx_itl_mark(const __grid_constant__ EnsParams P) {
+// The interstitial kernels run MX_ITL_THREADS threads per block; each warp keeps its list
+// of in-reach window sites (window_compact) in shared memory.
+#define MX_ITL_THREADS 256
+__global__ void __launch_bounds__(MX_ITL_THREADS) k_mx_itl_mark(const __grid_constant__ EnsParams P) {
+  __shared__ int s_list[MX_ITL_THREADS / 32][MB_WIN_LIST];
   const int warps = gridDim.x * (blockDim.x >> 5);
   const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   for (int q = 0; q < P.n_itl_lats; q++) {
     const LatDesc &d = P.lats[P.itl_lats[q]];
     if (!lat_active(d)) continue;
-    for (int it = gw; it < d.n_itl; it += warps) itl_mark_one(P, d, it);
+    for (int it = gw; it < d.n_itl; it += warps) itl_mark_one(P, d, it, s_list[threadIdx.x >> 5]);
   }
 }
 
 template <bool FORCE, bool ENERGY>
-__global__ void k_mx_itl_items(const __grid_constant__ EnsParams P) {
-  itl_items<FORCE, ENERGY, true>(P);
+__global__ void __launch_bounds__(MX_ITL_THREADS, 2) k_mx_itl_items(const __grid_constant__ EnsParams P) {
+  __shared__ int s_list[MX_ITL_THREADS / 32][MB_WIN_LIST];
+  itl_items<FORCE, ENERGY, true>(P, s_list[threadIdx.x >> 5]);
 }
 
 // Lattice <-> interstitial bookkeeping after the drift, one CTA per lattice that can
@@ -833,25 +838,25 @@ int mx_launch_step(const EnsParams &P, const MxStencil &S, int lat, int energy, 
   if (P.n_itl_lats > 0) {
     k_mx_itl_clear<<<itl_grid, 256, 0, s>>>(P);
     k_mx_itl_bin<<<P.n_itl_lats, MX_BIN_THREADS, 0, s>>>(P);
-    k_mx_itl_mark<<<itl_grid, 256, 0, s>>>(P);
+    k_mx_itl_mark<<<itl_grid, MX_ITL_THREADS, 0, s>>>(P);
   }
   if (ev) MB_CUDA(cudaEventRecord(ev[0], s));
   mx_passes(P, S, lat, energy, s, 0, rho_smem);
   if (ev) MB_CUDA(cudaEventRecord(ev[1], s));
   if (P.n_itl_lats > 0) {
     if (energy)
-      k_mx_itl_items<false, true><<<itl_grid, 256, 0, s>>>(P);
+      k_mx_itl_items<false, true><<<itl_grid, MX_ITL_THREADS, 0, s>>>(P);
     else
-      k_mx_itl_items<false, false><<<itl_grid, 256, 0, s>>>(P);
+      k_mx_itl_items<false, false><<<itl_grid, MX_ITL_THREADS, 0, s>>>(P);
   }
   if (ev) MB_CUDA(cudaEventRecord(ev[2], s));
   mx_passes(P, S, lat, energy, s, 1, force_smem);
   if (ev) MB_CUDA(cudaEventRecord(ev[3], s));
   if (P.n_itl_lats > 0) {
     if (energy)
-      k_mx_itl_items<true, true><<<itl_grid, 256, 0, s>>>(P);
+      k_mx_itl_items<true, true><<<itl_grid, MX_ITL_THREADS, 0, s>>>(P);
     else
-      k_mx_itl_items<true, false><<<itl_grid, 256, 0, s>>>(P);
+      k_mx_itl_items<true, false><<<itl_grid, MX_ITL_THREADS, 0, s>>>(P);
     if (P.conv2 > 0.0) k_mx_convert<<<P.n_itl_lats, MX_CONV_THREADS, 0, s>>>(P);
   }
   if (energy) {

@@ -615,15 +615,22 @@ __global__ void k_itl_clear(const Lattice64 L, const Itl64 I) {
 
 // ... then one warp per interstitial flags the sites within reach (the count was
 // reset in between); only sites in box layers [z0, z1) when that is not the whole box.
-__global__ void k_itl_mark(const Geom g, const Lattice64 L, const Itl64 I, int z0, int z1) {
+// The in-reach sites of the window are listed first (window_compact), so the lanes then
+// flag only those, several at once.
+__global__ void __launch_bounds__(MB_ITL_THREADS)
+    k_itl_mark(const Geom g, const Lattice64 L, const Itl64 I, int z0, int z1) {
+  __shared__ int s_list[MB_ITL_THREADS / 32][MB_WIN_LIST];
   const bool all_z = z0 <= 0 && z1 >= g.bz;
   const int lane = threadIdx.x & 31;
   const int it = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-  if (it >= itl_n(I)) return;
+  if (it >= itl_n(I)) return; // the same for the whole warp
   const double qx = I.px[it], qy = I.py[it], qz = I.pz[it];
   const Window w = make_window(qx, qy, qz, I.a0, I.reach);
-  const int ncand = w.nx * w.ny * w.nz;
-  for (int c = lane; c < ncand; c += 32) {
+  int *list = s_list[threadIdx.x >> 5];
+  const int nlist = window_compact(w, qx, qy, qz, I.a0, I.reach, list, MB_WIN_LIST);
+  const int ncand = nlist >= 0 ? nlist : w.nx * w.ny * w.nz;
+  for (int k = lane; k < ncand; k += 32) {
+    const int c = nlist >= 0 ? list[k] : k;
     long long idx;
     double sx, sy, sz;
     if (!window_site(g, w, c, qx, qy, qz, I.a0, I.reach, idx, sx, sy, sz)) continue;
@@ -647,6 +654,58 @@ __global__ void k_itl_mark(const Geom g, const Lattice64 L, const Itl64 I, int z
   }
 }
 
+// Lattice sites of the window of interstitial q, one warp: pair(dx, dy, dz, type, df)
+// for every occupied site in reach, d = q - (x_j + its periodic image shift), df only with
+// DF.  The in-reach sites are listed first (window_compact, list: this warp's shared
+// memory) and each lane then loads up to four of them at once: one round of dependent
+// loads instead of one per 32 candidates.
+template <bool DF, class Pair>
+__device__ __forceinline__ void window_pairs64(const Geom &g, const Lattice64 &L, const Itl64 &I, double qx,
+                                               double qy, double qz, int *list, Pair pair) {
+  const int lane = threadIdx.x & 31;
+  const Window win = make_window(qx, qy, qz, I.a0, I.reach);
+  const int n = window_compact(win, qx, qy, qz, I.a0, I.reach, list, MB_WIN_LIST);
+  if (n >= 0) {
+    for (int k0 = 0; k0 < n; k0 += 128) {
+      long long j[4];
+      double sx[4], sy[4], sz[4];
+      bool ok[4];
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        const int k = k0 + 32 * t + lane;
+        j[t] = 0;
+        sx[t] = sy[t] = sz[t] = 0.0;
+        ok[t] = k < n && window_site(g, win, list[k], qx, qy, qz, I.a0, I.reach, j[t], sx[t], sy[t], sz[t]);
+      }
+      int cj[4];
+      double xj[4], yj[4], zj[4], dj[4];
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        cj[t] = ok[t] ? (int)L.code[j[t]] : -1;
+        xj[t] = ok[t] ? L.px[j[t]] : 0.0;
+        yj[t] = ok[t] ? L.py[j[t]] : 0.0;
+        zj[t] = ok[t] ? L.pz[j[t]] : 0.0;
+        dj[t] = (DF && ok[t]) ? L.df[j[t]] : 0.0;
+      }
+#pragma unroll
+      for (int t = 0; t < 4; t++)
+        if (cj[t] >= 0) pair(qx - (xj[t] + sx[t]), qy - (yj[t] + sy[t]), qz - (zj[t] + sz[t]), cj[t] & 0x3F, dj[t]);
+    }
+    return;
+  }
+  const int ncand = win.nx * win.ny * win.nz;
+  for (int c = lane; c < ncand; c += 32) {
+    long long j;
+    double sx, sy, sz;
+    if (!window_site(g, win, c, qx, qy, qz, I.a0, I.reach, j, sx, sy, sz)) continue;
+    const int cj = L.code[j];
+    if (cj < 0) continue;
+    pair(qx - (L.px[j] + sx), qy - (L.py[j] + sy), qz - (L.pz[j] + sz), cj & 0x3F, DF ? L.df[j] : 0.0);
+  }
+}
+
+// Items of the interstitial passes: the interstitials first (w < n_itl), so that their
+// window walks (the longest items) start at once, then the flagged sites.
 template <bool ENERGY>
 __global__ void __launch_bounds__(MB_ITL_THREADS)
     k_itl_rho64(const __grid_constant__ StencilSet st, const Geom g, const DevPot P, const Lattice64 L, const Itl64 I,
@@ -657,10 +716,12 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
   const int n_itl = itl_n(I);
   const long long n_items = (long long)nflag + n_itl;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+  __shared__ int s_list[MB_ITL_THREADS / 32][MB_WIN_LIST];
+  int *list = s_list[threadIdx.x >> 5];
   double e_acc = 0.0;
   for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_items; w += wstride) {
-    if (w < nflag) {
-      const long long i = I.flag_list[w];
+    if (w >= n_itl) {
+      const long long i = I.flag_list[w - n_itl];
       int s, cx, y, z;
       decode_ext(g, i, s, cx, y, z);
       if (!all_z && (z < z0 || z >= z1)) continue;
@@ -688,25 +749,17 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
         if (ENERGY) e_acc += F64(P, ti, rho);
       }
     } else {
-      const int it = (int)(w - nflag);
+      const int it = (int)w;
       const double qx = I.px[it], qy = I.py[it], qz = I.pz[it];
       if (!all_z) {
         const int lz = z_layer(g, I.a0, qz);
         if (lz < z0 || lz >= z1) continue;
       }
-      const Window win = make_window(qx, qy, qz, I.a0, I.reach);
-      const int ncand = win.nx * win.ny * win.nz;
       double rho = 0.0;
-      for (int c = lane; c < ncand; c += 32) {
-        long long j;
-        double sx, sy, sz;
-        if (!window_site(g, win, c, qx, qy, qz, I.a0, I.reach, j, sx, sy, sz)) continue;
-        const int cj = L.code[j];
-        if (cj < 0) continue;
-        const double dx = qx - (L.px[j] + sx), dy = qy - (L.py[j] + sy), dz = qz - (L.pz[j] + sz);
+      window_pairs64<false>(g, L, I, qx, qy, qz, list, [&](double dx, double dy, double dz, int tj, double) {
         const double d2 = dx * dx + dy * dy + dz * dz;
-        if (d2 < rc2) rho += rho_of_r(P, cj & 0x3F, d2 * rsqrt(d2));
-      }
+        if (d2 < rc2) rho += rho_of_r(P, tj, d2 * rsqrt(d2));
+      });
       for (int K = lane; K < n_itl; K += 32) {
         if (K == it) continue;
         const double dx = min_image(qx - I.px[K], g.Lx, g.iLx), dy = min_image(qy - I.py[K], g.Ly, g.iLy),
@@ -739,14 +792,16 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
   const int n_itl = itl_n(I);
   const long long n_items = (long long)nflag + n_itl;
   const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+  __shared__ int s_list[MB_ITL_THREADS / 32][MB_WIN_LIST];
+  int *list = s_list[threadIdx.x >> 5];
   double ep_acc = 0.0, ek_acc = 0.0;
   for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n_items; w += wstride) {
-    const bool is_site = w < nflag;
+    const bool is_site = w >= n_itl;
     long long i = 0;
     int s = 0, cx = 0, y = 0, z = 0, it = 0, ti;
     double xi, yi, zi, dfi;
     if (is_site) {
-      i = I.flag_list[w];
+      i = I.flag_list[w - n_itl];
       decode_ext(g, i, s, cx, y, z);
       ti = L.code[i] & 0x3F;
       xi = L.px[i];
@@ -754,7 +809,7 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
       zi = L.pz[i];
       dfi = L.df[i];
     } else {
-      it = (int)(w - nflag);
+      it = (int)w;
       ti = I.type[it];
       xi = I.px[it];
       yi = I.py[it];
@@ -786,16 +841,7 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
         add_pair(xi - L.px[j], yi - L.py[j], zi - L.pz[j], cj & 0x3F, L.df[j]);
       }
     } else {
-      const Window win = make_window(xi, yi, zi, I.a0, I.reach);
-      const int ncand = win.nx * win.ny * win.nz;
-      for (int c = lane; c < ncand; c += 32) {
-        long long j;
-        double sx, sy, sz;
-        if (!window_site(g, win, c, xi, yi, zi, I.a0, I.reach, j, sx, sy, sz)) continue;
-        const int cj = L.code[j];
-        if (cj < 0) continue;
-        add_pair(xi - (L.px[j] + sx), yi - (L.py[j] + sy), zi - (L.pz[j] + sz), cj & 0x3F, L.df[j]);
-      }
+      window_pairs64<true>(g, L, I, xi, yi, zi, list, add_pair);
     }
     for (int K = lane; K < n_itl; K += 32) {
       if (!is_site && K == it) continue;
@@ -873,14 +919,16 @@ int launch_itl_mark64(const Geom &g, const Lattice64 &L, const Itl64 &I, cudaStr
   MB_CUDA(cudaGetLastError());
   MB_CUDA(cudaMemsetAsync(I.flag_count, 0, sizeof(int), s));
   const int nmax = I.nd ? I.cap : I.n;
-  if (nmax > 0) k_itl_mark<<<(nmax * 32 + 255) / 256, 256, 0, s>>>(g, L, I, 0, g.bz);
+  if (nmax > 0)
+    k_itl_mark<<<(nmax * 32 + MB_ITL_THREADS - 1) / MB_ITL_THREADS, MB_ITL_THREADS, 0, s>>>(g, L, I, 0, g.bz);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
 
 int launch_itl_mark_slab64(const Geom &g, const Lattice64 &L, const Itl64 &I, int z0, int z1, cudaStream_t s) {
   const int nmax = I.nd ? I.cap : I.n;
-  if (nmax > 0 && z0 < z1) k_itl_mark<<<(nmax * 32 + 255) / 256, 256, 0, s>>>(g, L, I, z0, z1);
+  if (nmax > 0 && z0 < z1)
+    k_itl_mark<<<(nmax * 32 + MB_ITL_THREADS - 1) / MB_ITL_THREADS, MB_ITL_THREADS, 0, s>>>(g, L, I, z0, z1);
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
