@@ -87,7 +87,11 @@ def test_budget_queues_and_faults_are_contained():
 @pytest.mark.gpu
 def test_large_admission_is_prepared_off_the_loop_thread():
     # small lattices run for many steps while a 2 M-atom request arrives; its lattice is
-    # built on a worker thread, so the loop thread only uploads it between chunks
+    # built on a worker thread, so the loop thread only uploads it between chunks.  Built
+    # on the loop thread instead, the admission would take the build time plus the upload.
+    warm = serve.Server(chunk=20)  # first use of the kernels and allocator in this process
+    warm.serve([serve.Request(60, 0.0, (10, 10, 10), 20, 300.0, 0.0, 3)], realtime=False)
+    warm.close()
     small = serve.poisson_stream(3, rate=1000.0, seed=21, atoms=(2e4, 5e4), steps=(40000, 40000))
     big = serve.Request(50, 0.05, serve.cells_for_atoms(2e6), 20, 600.0, 0.005, 77)
     probe = serve.Request(51, 0.0, big.cells, 20, 600.0, 0.005, 77)
@@ -99,7 +103,7 @@ def test_large_admission_is_prepared_off_the_loop_thread():
     srv.close()
     assert stats["completed"] == 4
     stall = dict(srv.admit_stall)[big.rid]
-    assert stall < 0.3 * t_build, (stall, t_build)
+    assert stall < 0.75 * t_build, (stall, t_build)
     assert big.admitted < max(r.finished for r in small)  # it joined while the others ran
 
 
