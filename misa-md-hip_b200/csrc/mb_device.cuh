@@ -217,6 +217,25 @@ __device__ __forceinline__ int window_compact(const Window &w, double qx, double
 }
 #define MB_WIN_LIST 256 // compacted window entries per warp
 
+// Appends this lane's entry (when `add`) to list[0 .. cap) with one atomicAdd on *count
+// per warp instead of one per lane (many lanes appending at once would serialise on the
+// counter); every lane of the warp must call it.  Entries past cap are dropped and
+// *overflow is set.  The order of entries within a call follows the lanes.
+__device__ __forceinline__ void warp_append(bool add, int value, int *count, int *list, int cap, int *overflow) {
+  const unsigned m = __ballot_sync(0xffffffffu, add);
+  if (!m) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  int first = 0;
+  if (lane == leader) first = atomicAdd(count, __popc(m));
+  first = __shfl_sync(0xffffffffu, first, leader);
+  if (!add) return;
+  const int slot = first + __popc(m & ((1u << lane) - 1u));
+  if (slot < cap)
+    list[slot] = value;
+  else
+    *overflow = 1;
+}
+
 // Same candidate walk, returning the ideal image position relative to the query point
 // (ox, oy, oz) instead of the periodic shift.
 __device__ __forceinline__ bool window_site_rel(const Geom &g, const Window &w, int c, double qx, double qy,

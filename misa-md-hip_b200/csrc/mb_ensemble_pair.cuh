@@ -140,23 +140,20 @@ __device__ __forceinline__ void itl_mark_one(const EnsParams &P, const LatDesc &
   const Window w = make_window(qx, qy, qz, P.a0, P.reach);
   const int nlist = list ? window_compact(w, qx, qy, qz, P.a0, P.reach, list, MB_WIN_LIST) : -1;
   const int ncand = nlist >= 0 ? nlist : w.nx * w.ny * w.nz;
-  for (int k = lane; k < ncand; k += 32) {
-    const int c = nlist >= 0 ? list[k] : k;
-    long long idx;
+  for (int base = 0; base < ncand; base += 32) { // whole warp per round (warp_append)
+    const int k = base + lane;
+    long long idx = 0;
+    bool fresh = false;
     double sx, sy, sz;
-    if (!window_site(g, w, c, qx, qy, qz, P.a0, P.reach, idx, sx, sy, sz)) continue;
-    if (d.code[idx] < 0) continue;
-    const uintptr_t addr = (uintptr_t)(d.code + idx);
-    unsigned int *word = (unsigned int *)(addr & ~(uintptr_t)3);
-    const unsigned int bit = (unsigned int)MB_FLAG_ITL << (8 * (addr & 3));
-    const unsigned int old = atomicOr(word, bit);
-    if (!(old & bit)) {
-      const int slot = atomicAdd(&d.flag_count[cur], 1);
-      if (slot < d.cap_flag)
-        d.flag_list[slot] = (int)idx;
-      else
-        d.flag_count[2] = 1; // overflow: reported by the host
+    if (k < ncand && window_site(g, w, nlist >= 0 ? list[k] : k, qx, qy, qz, P.a0, P.reach, idx, sx, sy, sz) &&
+        d.code[idx] >= 0) {
+      const uintptr_t addr = (uintptr_t)(d.code + idx);
+      unsigned int *word = (unsigned int *)(addr & ~(uintptr_t)3);
+      const unsigned int bit = (unsigned int)MB_FLAG_ITL << (8 * (addr & 3));
+      fresh = !(atomicOr(word, bit) & bit);
     }
+    // flag_count[2]: overflow, reported by the host
+    warp_append(fresh, (int)idx, &d.flag_count[cur], d.flag_list, d.cap_flag, &d.flag_count[2]);
   }
 }
 

@@ -629,28 +629,25 @@ __global__ void __launch_bounds__(MB_ITL_THREADS)
   int *list = s_list[threadIdx.x >> 5];
   const int nlist = window_compact(w, qx, qy, qz, I.a0, I.reach, list, MB_WIN_LIST);
   const int ncand = nlist >= 0 ? nlist : w.nx * w.ny * w.nz;
-  for (int k = lane; k < ncand; k += 32) {
-    const int c = nlist >= 0 ? list[k] : k;
-    long long idx;
+  for (int base = 0; base < ncand; base += 32) { // whole warp per round (warp_append)
+    const int k = base + lane;
+    long long idx = 0;
+    bool fresh = false;
     double sx, sy, sz;
-    if (!window_site(g, w, c, qx, qy, qz, I.a0, I.reach, idx, sx, sy, sz)) continue;
-    if (!all_z) {
+    bool site = k < ncand && window_site(g, w, nlist >= 0 ? list[k] : k, qx, qy, qz, I.a0, I.reach, idx, sx, sy, sz);
+    if (site && !all_z) {
       int ss, scx, sy_, sz_;
       decode_ext(g, idx, ss, scx, sy_, sz_);
-      if (sz_ < z0 || sz_ >= z1) continue;
+      site = sz_ >= z0 && sz_ < z1;
     }
-    if (L.code[idx] < 0) continue;
-    const uintptr_t addr = (uintptr_t)(L.code + idx);
-    unsigned int *word = (unsigned int *)(addr & ~(uintptr_t)3);
-    const unsigned int bit = (unsigned int)MB_FLAG_ITL << (8 * (addr & 3));
-    const unsigned int old = atomicOr(word, bit);
-    if (!(old & bit)) {
-      const int slot = atomicAdd(&I.flag_count[0], 1);
-      if (slot < I.cap_flag)
-        I.flag_list[slot] = (int)idx;
-      else
-        I.flag_count[1] = 1; // overflow: reported by the host
+    if (site && L.code[idx] >= 0) {
+      const uintptr_t addr = (uintptr_t)(L.code + idx);
+      unsigned int *word = (unsigned int *)(addr & ~(uintptr_t)3);
+      const unsigned int bit = (unsigned int)MB_FLAG_ITL << (8 * (addr & 3));
+      fresh = !(atomicOr(word, bit) & bit);
     }
+    // flag_count[1]: overflow, reported by the host
+    warp_append(fresh, (int)idx, &I.flag_count[0], I.flag_list, I.cap_flag, &I.flag_count[1]);
   }
 }
 
