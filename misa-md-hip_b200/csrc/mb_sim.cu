@@ -775,13 +775,17 @@ int mb_sim_kernel_times(mb_sim *s, float *rho_ms, float *force_ms) {
 // Box layers [zb[k], zb[k+1]) of the host-buffer step's z-slabs.  Each slab is at
 // least as thick as anything a site or an interstitial reaches (the stencil's ghost
 // layers; interstitial windows of cutoff + skin, flagged sites within them), so the
-// work on slab k reads only slabs k-1, k, k+1 (periodic in z).  Automatic: as many as
-// fit, with at least 4 MiB of records per slab (a slab's copy then outlasts the
+// work on slab k reads only slabs k-1, k, k+1 (periodic in z).  An interstitial in box
+// layer Z reaches sites of layers Z - ceil(R / a0) .. Z + ceil(R / a0) (sublattice-1
+// sites sit half a layer up), hence ceil(R / a0) + 1 layers with a layer to spare.
+// More slabs shorten the tail of the step (the periodic ring closes after the last
+// slab arrives: two density and four force slabs and their copies out).  Automatic: as
+// many as fit, with at least 4 MiB of records per slab (a slab's copy then outlasts the
 // launches of its passes).  Fewer than 4 slabs: one piece.
 static int slab_plan(const mb_sim *s, int *zb) {
   const int bz = s->g.bz;
   const double reach = s->cfg.cutoff + s->cfg.stencil_skin;
-  const int rz = std::max(s->g.gz, (int)ceil(reach / s->cfg.lattice_const) + 2);
+  const int rz = std::max(s->g.gz, (int)ceil(reach / s->cfg.lattice_const) + 1);
   const long long by_bytes = (long long)s->n_box * (long long)sizeof(mb_atom_element) / (4LL << 20);
   const int want = s->host_slabs > 0 ? s->host_slabs : (int)std::min<long long>(by_bytes, MB_SLAB_MAX);
   int n = std::min(std::min(want, bz / std::max(rz, 1)), MB_SLAB_MAX);

@@ -52,7 +52,7 @@ class Scenario:
 
 
 def make(cells=(5, 5, 5), temperature=600.0, vacancy=0.0, n_itl=0, seed=1, jitter=0.05, tables=None,
-         n_types=1) -> Scenario:
+         n_types=1, skin=SKIN) -> Scenario:
     tables = tables or (mb.potential.fe_analytic() if n_types == 1 else mb.potential.alloy_analytic(n_types))
     box = mb.lattice.bcc_box(cells, A0)
     rng = np.random.default_rng(seed + 100)
@@ -65,8 +65,8 @@ def make(cells=(5, 5, 5), temperature=600.0, vacancy=0.0, n_itl=0, seed=1, jitte
     mb.lattice.maxwell_boltzmann(box, itl, temperature, MASS, seed + 2)
     live = box["type"] >= 0
     box["x"][live] += rng.normal(0.0, jitter, size=(int(live.sum()), 3))
-    ghost = mb.lattice.ghost_for_reach(A0, RC + SKIN)
-    return Scenario(tuple(cells), box, itl, tables, ghost)
+    ghost = mb.lattice.ghost_for_reach(A0, RC + skin)
+    return Scenario(tuple(cells), box, itl, tables, ghost, skin=skin)
 
 
 def rel_err(a: np.ndarray, b: np.ndarray) -> float:

@@ -243,6 +243,27 @@ def _sim(sc, precision=mb.MB_PREC_FP64):
                   stencil_skin=sc.skin, precision=precision, max_interstitials=max(8, sc.itl.shape[0]))
 
 
+def test_wide_reach_interstitial_windows_match_oracle():
+    # cutoff + skin = 9.0 A: about 262 sites lie in reach of an interstitial, more than the
+    # per-warp list of in-reach window sites holds (256), so the interstitial passes walk
+    # every window candidate instead; the results are still the oracle's
+    sc = make(cells=(8, 8, 8), temperature=600.0, vacancy=0.01, n_itl=3, seed=53, skin=3.4)
+    nsteps = 5
+    bo, io, eo = _oracle_md(sc, nsteps)
+    with _sim(sc) as sim:
+        sim.upload(sc.box, sc.itl)
+        sim.run(nsteps, energy_every=1)
+        bg, ig = sim.download()
+        eg = sim.energies()
+    live = bo["type"] >= 0
+    n_atoms = int(live.sum()) + 3
+    assert np.max(np.abs(bg["x"][live] - bo["x"][live])) < 1e-10
+    assert rel_err(bg["f"][live], bo["f"][live]) < F_TOL
+    assert rel_err(ig["f"], io["f"]) < F_TOL
+    assert np.max(np.abs(ig["x"] - io["x"])) < 1e-10
+    assert np.max(np.abs(eg[:, 1:] - eo)) / n_atoms < E_TOL
+
+
 @pytest.mark.parametrize("n_itl,vac,n_types", [(0, 0.0, 1), (3, 0.01, 1), (2, 0.01, 3)])
 def test_device_md_matches_oracle(n_itl, vac, n_types):
     sc = make(cells=(6, 7, 8), temperature=600.0, vacancy=vac, n_itl=n_itl, seed=31, n_types=n_types)
@@ -359,8 +380,8 @@ def test_host_buffer_slabs_are_bitwise_one_piece(cells, n_itl):
             for _ in range(4):
                 sim.step_host(box, ig if n_itl else None)
         out[slabs] = (box, ig)
-    # as many as the reach allows: slabs of at least 5 layers
-    assert out[1, "n"] == 1 and out[32, "n"] == cells[2] // 5 and out[5, "n"] == 5 and out[4, "n"] == 4
+    # as many as the reach allows: slabs of at least ceil((cutoff + skin) / a0) + 1 = 4 layers
+    assert out[1, "n"] == 1 and out[32, "n"] == cells[2] // 4 and out[5, "n"] == 5 and out[4, "n"] == 4
     for slabs in (32, 5, 4):
         for a, b in zip(out[1], out[slabs]):
             assert a.tobytes() == b.tobytes(), slabs
