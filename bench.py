@@ -689,8 +689,10 @@ def serve_measure(mb, n_requests: int, max_seconds: float = 600.0, clocks_device
             "latency_p50_s": stats["latency_p50_s"], "latency_p99_s": stats["latency_p99_s"],
             "makespan_s": stats["makespan_s"], "admit_stall_s": stats["admit_stall_s"],
             "gpu_launches": stats["launches"], "clocks": clk, "dtype": "f32 pairs + two-sum, f64 state",
+            "admission": {"order": srv.order, "batch_atoms": srv.batch_atoms},
             "workload": "Poisson 50 req/s (seed 13), atoms log-uniform [1e3, 2e6], steps uniform [100, 5000], "
-                        "300-1200 K, 0-1% vacancies, 160 GB HBM budget, continuous batching"}
+                        "300-1200 K, 0-1% vacancies, 160 GB HBM budget, continuous batching, shortest remaining "
+                        "work admitted first under a batch target of sites in flight"}
 
 
 def run_serve(args, mb, world, rank, local, pg) -> None:
@@ -704,8 +706,9 @@ def run_serve(args, mb, world, rank, local, pg) -> None:
             "config": {"workload": "serve_poisson50_seed13", "requests": args.requests,
                        "completed": sv["completed"], "rejected": sv["rejected"]},
             "latency_p50_s": sv["latency_p50_s"], "latency_p99_s": sv["latency_p99_s"],
-            "makespan_s": sv["makespan_s"], "admit_stall_s": sv["admit_stall_s"], "gpu_launches": sv["gpu_launches"],
-            "clocks": sv["clocks"], "cpu_baseline": None, "e2e": None}), flush=True)
+            "makespan_s": sv["makespan_s"], "admit_stall_s": sv["admit_stall_s"], "admission": sv["admission"],
+            "gpu_launches": sv["gpu_launches"], "clocks": sv["clocks"], "cpu_baseline": None, "e2e": None}),
+              flush=True)
 
 
 def run_decomp(args, mb, world, rank, local, pg) -> None:

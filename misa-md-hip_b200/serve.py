@@ -15,6 +15,17 @@ loop thread only uploads a prepared lattice, so a large arrival does not hold up
 launches of the others.  The time the loop thread spends admitting requests between
 chunks is recorded (``admit_stall_s``).
 
+Admission order: by default the queued request with the least remaining work (sites x
+steps) goes first, requests resumed from a checkpoint ahead of all, and new lattices
+join only while the atoms in flight stay under a batch target (``batch_atoms``; 4 M by
+default, enough to fill the GPU; a request is always admitted when nothing runs).  With
+every request in one batch each step costs the whole batch's time, so even the shortest
+request waits as long as a step of everything; shortest-first under a target lets short
+requests finish within a few seconds while the batch still saturates the device (the same
+work, so about the same makespan and throughput).  ``order="fifo"`` and
+``batch_atoms=0`` give first-come, first-served admission of everything that fits the
+budget.
+
 Host-side failure handling: malformed requests are rejected at submission; a
 request larger than the whole budget is rejected instead of queued forever; a
 request can be cancelled while queued or in flight (its slot is freed, the other
@@ -103,6 +114,18 @@ def build_lattice(req: Request) -> np.ndarray:
     return box
 
 
+def lattice_sites(req: Request) -> int:
+    """Sites of a request's lattice (2 per BCC cell; its atoms, up to the vacancies)."""
+    return 2 * int(req.cells[0]) * int(req.cells[1]) * int(req.cells[2])
+
+
+def admission_key(req: Request) -> tuple:
+    """Sort key of the shortest-work-first queue: requests resumed from a checkpoint
+    first, then the least remaining work (sites x steps left), then arrival."""
+    resumed = 0 if req.snapshot is not None else 1
+    return (resumed, lattice_sites(req) * (req.steps - req.steps_before), req.arrival, req.rid)
+
+
 def validate_request(req: Request, budget: int) -> str:
     """Why a request cannot be served at all ("" when it can)."""
     if len(req.cells) != 3 or min(req.cells) < 6:
@@ -119,9 +142,16 @@ def validate_request(req: Request, budget: int) -> str:
 class Server:
     def __init__(self, tables: potential.EamTables | None = None, hbm_budget_bytes: int = 160 << 30,
                  chunk: int = 50, energy_every: int = 0, keep_results: bool = False, prep_workers: int = 2,
-                 prep_ahead: int = 4):
+                 prep_ahead: int = 4, order: str = "shortest", batch_atoms: float = 4e6):
         """prep_workers threads build the lattices of up to prep_ahead queued requests
-        ahead of their admission (0 workers: built on the loop thread at admission)."""
+        ahead of their admission (0 workers: built on the loop thread at admission).
+        order: "shortest" (least remaining work first) or "fifo"; batch_atoms: sites in
+        flight beyond which queued requests wait for running ones to finish (0: no
+        target, only the HBM budget)."""
+        if order not in ("shortest", "fifo"):
+            raise ValueError("order must be 'shortest' or 'fifo'")
+        self.order = order
+        self.batch_atoms = float(batch_atoms)
         self.tables = tables or potential.fe_analytic()
         self.budget = int(hbm_budget_bytes)
         self.ens = Ensemble(self.tables, lattice_const=A0, mass=MASS, hbm_budget_bytes=self.budget)
@@ -156,8 +186,16 @@ class Server:
             return False
         req.status = "queued"
         self.queue.append(req)
+        self._order_queue()
         self._prefetch()
         return True
+
+    def _order_queue(self) -> None:
+        if self.order == "shortest":
+            self.queue.sort(key=admission_key)
+
+    def running_sites(self) -> int:
+        return sum(lattice_sites(r) for r in self.running.values())
 
     def _prefetch(self) -> None:
         if self.pool is None:
@@ -184,6 +222,7 @@ class Server:
         req.snapshot, req.steps_before = box, done
         req.status = "queued"
         self.queue.insert(0, req)
+        self._order_queue()  # resumed requests stay at the head
 
     def cancel(self, req: Request) -> None:
         if req.status == "queued":
@@ -197,10 +236,13 @@ class Server:
         req.status = "cancelled"
 
     def _admit(self) -> None:
-        # first come, first served: a head request whose lattice is still being built
-        # waits (the running lattices keep advancing) unless nothing else runs
+        # in queue order (see _order_queue): a head request whose lattice is still being
+        # built waits (the running lattices keep advancing) unless nothing else runs
         while self.queue:
             req = self.queue[0]
+            if self.running and self.batch_atoms > 0 and \
+                    self.running_sites() + lattice_sites(req) > self.batch_atoms:
+                return  # the batch is full: wait for a running lattice to finish
             t_in = time.perf_counter()
             fut = self.prepared.get(req.rid)
             if req.snapshot is not None:

@@ -32,6 +32,18 @@ def test_request_validation_without_a_device():
     assert "budget" in serve.validate_request(serve.Request(4, 0.0, (200, 200, 200), 5, 300.0, 0.0, 1), budget)
 
 
+def test_shortest_work_first_order_without_a_device():
+    a = serve.Request(0, 0.0, (10, 10, 10), 1000, 300.0, 0.0, 1)  # 2,000 sites x 1,000 steps
+    b = serve.Request(1, 0.1, (10, 10, 10), 100, 300.0, 0.0, 1)  # less work, arrived later
+    c = serve.Request(2, 0.2, (40, 40, 40), 100, 300.0, 0.0, 1)  # 128,000 sites x 100 steps
+    d = serve.Request(3, 0.3, (20, 20, 20), 5000, 300.0, 0.0, 1)
+    d.snapshot, d.steps_before = np.zeros(1), 4000  # resumed from a checkpoint: first
+    assert [r.rid for r in sorted([a, b, c, d], key=serve.admission_key)] == [3, 1, 0, 2]
+    assert serve.lattice_sites(c) == 128000
+    with pytest.raises(ValueError):
+        serve.Server.__init__(object.__new__(serve.Server), order="random")
+
+
 def _small_stream(n, seed=5):
     return serve.poisson_stream(n, rate=200.0, seed=seed, atoms=(1e3, 2e4), steps=(10, 40))
 
@@ -106,6 +118,28 @@ def test_large_admission_is_prepared_off_the_loop_thread(monkeypatch):
     assert built_on[big.rid] != threading.get_ident()  # not on the loop thread
     assert big.rid in dict(srv.admit_stall)
     assert big.admitted < max(r.finished for r in small)  # it joined while the others ran
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", ["shortest", "fifo"])
+def test_admission_order_under_a_batch_target(order):
+    # three requests at once, a batch target of one lattice: shortest-first runs the two
+    # short requests before the long one, first-come-first-served the long one first
+    long_ = serve.Request(0, 0.0, (12, 12, 12), 400, 300.0, 0.0, 1)
+    short = [serve.Request(k, 0.0, (10, 10, 10), 40, 300.0, 0.0, k) for k in (1, 2)]
+    srv = serve.Server(chunk=10, order=order, batch_atoms=serve.lattice_sites(long_))
+    peak = []
+    stats = srv.serve([long_] + short, realtime=False, on_tick=lambda s: peak.append(len(s.running)))
+    srv.close()
+    assert stats["completed"] == 3 and max(peak) == 1
+    first = short[0].finished < short[1].finished < long_.finished
+    assert first if order == "shortest" else long_.finished < short[0].finished
+    everything = serve.Server(chunk=10, batch_atoms=0)  # no target: all three at once
+    peak = []
+    everything.serve([serve.Request(k, 0.0, (10, 10, 10), 40, 300.0, 0.0, k) for k in range(3)], realtime=False,
+                     on_tick=lambda s: peak.append(len(s.running)))
+    everything.close()
+    assert max(peak) == 3
 
 
 @pytest.mark.gpu
