@@ -242,7 +242,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
   return ok != 0;
 }
 
-// 5-D tiled TMA load (no multicast): box {4, TX+4, TY+4, TZ+4, 2} of float32.
+// 5-D tiled TMA load into this CTA's own shared memory from this GPU's memory: box
+// {4, TX+4, TY+4, TZ+4, 2} of float32.
 __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3, int c4,
                                             uint64_t *bar) {
   asm volatile(
