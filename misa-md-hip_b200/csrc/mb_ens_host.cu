@@ -531,6 +531,20 @@ static int rebuild(mb_ensemble *e) {
     std::vector<unsigned> first(nl + 1, 0);
     unsigned long long n_items = 0;
     if (W.linear) {
+      // brick order for lattices with large planes (MxWalk); the environment variable
+      // MB_MX_LBRICK = "chunks,zcells,min_plane_sites" overrides it, for tuning ("0,0,0":
+      // every lattice plane by plane)
+      W.lcb = MX_LCB;
+      W.lbz = MX_LBZ;
+      W.lmin = MX_LMIN;
+      if (const char *v = getenv("MB_MX_LBRICK")) {
+        unsigned a = 0, b = 0, m = 0;
+        if (sscanf(v, "%u,%u,%u", &a, &b, &m) == 3 && a <= 64 && b <= 64) {
+          W.lcb = (a && b) ? a : 0;
+          W.lbz = (a && b) ? b : 0;
+          W.lmin = m;
+        }
+      }
       for (int c = 0; c < nl; c++) {
         const LatDesc &d = descs[c];
         first[c] = (unsigned)n_items;

@@ -136,15 +136,24 @@ struct MxEntry {
 // walks one contiguous range of the concatenated items.
 #define MX_BY 8
 #define MX_BZ 8
+#define MX_LCB 8      // linear walk, large lattices: bricks of 8 chunks ...
+#define MX_LBZ 8      // ... by 8 z cells ...
+#define MX_LMIN 4096  // ... for planes of at least 64 x 64 sites
 struct MxWalk {
   int linear;                // 0: bricks of lattice `lat`; 1: linear items over every lattice
   unsigned chunks, m_chunks; // x chunks per row and floor((2^32 - 1) / chunks)
   unsigned by, bz, bitems;   // brick rows, planes and items (2 by bz; MX_BY, MX_BZ unless overridden)
   unsigned nyb, m_nyb;       // y bricks
   unsigned n_units;          // bricks
-  // linear walk: item = 32 consecutive sites of one (z, sublattice) plane of a lattice,
-  // planes ordered z-major; lattice l owns items [item_first[l], item_first[l + 1])
+  // linear walk: item = 32 consecutive sites (a chunk) of one (z, sublattice) plane of a
+  // lattice; lattice l owns items [item_first[l], item_first[l + 1]).  A lattice whose
+  // (z, sublattice) planes hold at least lmin sites orders its items by bricks of lbz z
+  // cells (both sublattices) by lcb chunks: z block, then chunk block, then plane, then
+  // chunk, so that a block's warps share neighbour planes in L1 (10 planes of such a
+  // lattice exceed it).  Smaller lattices go plane by plane, which measured faster for
+  // them (lcb == 0: every lattice plane by plane).
   const unsigned *item_first;
+  unsigned lcb, lbz, lmin;
   unsigned n_items; // every walk: items (energy partials)
   int n_lats;
 };

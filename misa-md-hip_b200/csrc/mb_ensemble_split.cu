@@ -142,7 +142,22 @@ __device__ __forceinline__ bool mx_locate(const EnsParams &P, const MxWalk &W, i
     }
     const LatDesc &d = P.lats[at.l];
     const unsigned plane_sites = (unsigned)(d.bcx * d.by), cpp = (plane_sites + 31u) / 32u;
-    const unsigned j = item - at.lo, plane = j / cpp, b = (j - plane * cpp) * 32u + (unsigned)lane;
+    const unsigned j = item - at.lo;
+    unsigned plane, chunk;
+    if (W.lcb && plane_sites >= W.lmin) {
+      // brick order (see MxWalk); the last z block and chunk block of a lattice are
+      // shorter, so every item holds sites
+      const unsigned per_zb = cpp * 2u * W.lbz, zb = j / per_zb, j1 = j - zb * per_zb;
+      const unsigned nzp = 2u * min(W.lbz, (unsigned)d.bz - zb * W.lbz);
+      const unsigned per_cb = W.lcb * nzp, cb = j1 / per_cb, j2 = j1 - cb * per_cb;
+      const unsigned ncb = min(W.lcb, cpp - cb * W.lcb), p = j2 / ncb;
+      plane = zb * 2u * W.lbz + p;
+      chunk = cb * W.lcb + (j2 - p * ncb);
+    } else {
+      plane = j / cpp;
+      chunk = j - plane * cpp;
+    }
+    const unsigned b = chunk * 32u + (unsigned)lane;
     if (b >= plane_sites) return false;
     s = (int)(plane & 1u);
     z = (int)(plane >> 1);

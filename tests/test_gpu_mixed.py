@@ -199,6 +199,31 @@ def test_batched_equals_alone(mode):
             assert ens.status(s)[0] == 25
 
 
+def test_batched_equals_alone_with_large_planes():
+    # lattices with planes of >= 64 x 64 sites are walked by bricks inside a batch (z blocks
+    # of 8 cells by 8 chunks; these two end in shorter blocks), small ones plane by plane,
+    # and a lattice alone by the single-lattice bricks: the same positions and forces
+    specs = [((64, 66, 6), 2, 0.005), ((70, 65, 9), 0, 0.01), ((8, 9, 10), 1, 0.0)]
+    scs = [make(cells=c, temperature=700.0 + 100 * k, vacancy=v, n_itl=n, seed=120 + k)
+           for k, (c, n, v) in enumerate(specs)]
+    alone = []
+    for sc in scs:
+        with _ens(sc) as ens:
+            s = ens.add(sc.cells, sc.box, sc.itl if sc.itl.shape[0] else None, steps=20)
+            ens.advance(100, energy_every=5)
+            alone.append((*ens.download(s), ens.energies(s)))
+    with _ens(scs[0]) as ens:
+        slots = [ens.add(sc.cells, sc.box, sc.itl if sc.itl.shape[0] else None, steps=20) for sc in scs]
+        ens.advance(100, energy_every=5)
+        for k, s in enumerate(slots):
+            (b, i), e = ens.download(s), ens.energies(s)
+            ab, ai, ae = alone[k]
+            assert np.array_equal(b["x"], ab["x"]), k
+            assert np.array_equal(b["f"], ab["f"]), k
+            assert np.array_equal(i["x"], ai["x"]), k
+            np.testing.assert_allclose(e[:, 1:], ae[:, 1:], rtol=1e-12)
+
+
 def test_uneven_step_targets_and_slot_reuse():
     sc = make(cells=(8, 8, 8), temperature=600.0, seed=91)
     with _ens(sc) as ens:
