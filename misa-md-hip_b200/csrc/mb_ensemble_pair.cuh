@@ -196,6 +196,30 @@ __device__ __forceinline__ void itl_pairs(const LatDesc &d, const Geom &g, int c
   }
 }
 
+// One FP64 pair of an interstitial item (atom of type ti, df dfi; partner of type tj, df
+// dfj at pair vector d = own - partner): its density term into rho, or its force and pair
+// energy into f and ep.  Pairs at or beyond the cutoff add nothing.
+template <bool FORCE, bool ENERGY>
+__device__ __forceinline__ void itl_pair(const EnsParams &P, int ti, double dfi, double dx, double dy, double dz,
+                                         int tj, double dfj, double &rho, double &fx, double &fy, double &fz,
+                                         double &ep) {
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  if (d2 >= P.rc2) return;
+  const double rinv = rsqrt(d2);
+  const double r = d2 * rinv;
+  if (!FORCE) {
+    rho += rho_of_r(P.P, tj, r);
+  } else {
+    double ph = 0.0;
+    const double psip = pair_psip(P.P, ti, tj, r, dfi, dfj, ENERGY ? &ph : nullptr);
+    const double fpair = -psip * rinv;
+    fx += dx * fpair;
+    fy += dy * fpair;
+    fz += dz * fpair;
+    if (ENERGY) ep += 0.5 * ph;
+  }
+}
+
 // Last part of an item, on one lane, from its summed pairs: df (density pass), or force,
 // velocity-Verlet, drift and ghost images (force pass), of a flagged site (i at s, cx, y,
 // z) or of interstitial it.
@@ -366,21 +390,7 @@ __device__ void itl_item(const EnsParams &P, const LatDesc &d, int w, int nflag,
   }
   double acc0 = 0.0, fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
   auto pair = [&](double dx, double dy, double dz, int tj, double dfj) {
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    if (d2 >= P.rc2) return;
-    const double rinv = rsqrt(d2);
-    const double r = d2 * rinv;
-    if (!FORCE) {
-      acc0 += rho_of_r(P.P, tj, r);
-    } else {
-      double ph = 0.0;
-      const double psip = pair_psip(P.P, ti, tj, r, dfi, dfj, ENERGY ? &ph : nullptr);
-      const double fpair = -psip * rinv;
-      fx += dx * fpair;
-      fy += dy * fpair;
-      fz += dz * fpair;
-      if (ENERGY) ep += 0.5 * ph;
-    }
+    itl_pair<FORCE, ENERGY>(P, ti, dfi, dx, dy, dz, tj, dfj, acc0, fx, fy, fz, ep);
   };
   if (is_site) {
     // the lattice kernels summed this site's lattice pairs (FP32, compensated) into
@@ -427,21 +437,7 @@ __device__ void itl_site_group(const EnsParams &P, const LatDesc &d, int w, bool
   double xi = 0.0, yi = 0.0, zi = 0.0, dfi = 0.0;
   double acc0 = 0.0, fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
   auto pair = [&](double dx, double dy, double dz, int tj, double dfj) {
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    if (d2 >= P.rc2) return;
-    const double rinv = rsqrt(d2);
-    const double r = d2 * rinv;
-    if (!FORCE) {
-      acc0 += rho_of_r(P.P, tj, r);
-    } else {
-      double ph = 0.0;
-      const double psip = pair_psip(P.P, ti, tj, r, dfi, dfj, ENERGY ? &ph : nullptr);
-      const double fpair = -psip * rinv;
-      fx += dx * fpair;
-      fy += dy * fpair;
-      fz += dz * fpair;
-      if (ENERGY) ep += 0.5 * ph;
-    }
+    itl_pair<FORCE, ENERGY>(P, ti, dfi, dx, dy, dz, tj, dfj, acc0, fx, fy, fz, ep);
   };
   if (valid) {
     i = d.flag_list[w];
