@@ -4,7 +4,7 @@
 // and two TMA tile buffers resident, which caps it at 16 warps per SM.  Here the
 // density pass and the force + velocity-Verlet pass are separate kernels, each holding
 // only its own squared-distance table in shared memory and reading neighbour rows
-// through L1, so each runs with 24-32 warps per SM.  Pair terms are FP32 (linear
+// through L1, so each runs with 28-32 warps per SM.  Pair terms are FP32 (linear
 // interpolation in s = r^2 of tables built from the FP64 spline, index from the small
 // quantity r^2 - R^2) with two-sum accumulation; state and integration stay FP64.
 // The kernels of one step (interstitial phases included) are captured into one CUDA
@@ -22,7 +22,9 @@ namespace mb {
 #define MX_RHO_THREADS 1024
 #endif
 #ifndef MX_FORCE_THREADS
-#define MX_FORCE_THREADS 768
+#define MX_FORCE_THREADS 896 // 28 warps per SM at 72 registers; measured against 768 (80 registers,
+                             // no spills) and 1024 (64, more spills): force pass 0.170 / 0.165 /
+                             // 0.171 ns per atom on 128^3 cells
 #endif
 #define MX_SMEM_MAX (220 * 1024)
 
