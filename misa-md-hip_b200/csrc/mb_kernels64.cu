@@ -54,8 +54,12 @@ __device__ __forceinline__ void conv_check(const Geom &g, const StepParams &sp, 
 
 
 #define MB_EPART_CAP 4096 // CTA partial sums per energy region
+#ifndef MB_RHO_THREADS
 #define MB_RHO_THREADS 1024  // 52 registers: a full SM of warps
+#endif
+#ifndef MB_FORCE_THREADS
 #define MB_FORCE_THREADS 768 // up to 85 registers
+#endif
 #define MB_ITL_THREADS 256
 
 int energy_partials_needed() { return 8 * MB_EPART_CAP; }
