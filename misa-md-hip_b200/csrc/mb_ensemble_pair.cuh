@@ -1,6 +1,6 @@
 // Per-pair FP32 arithmetic and interstitial items of the mixed-precision step,
-// shared by the persistent tile kernel (mb_ensemble.cu) and the split kernels of
-// single large lattices (mb_ensemble_split.cu).
+// shared by the persistent tile kernel (mb_ensemble.cu) and the split kernels
+// (mb_ensemble_split.cu, one lattice or many).
 #pragma once
 
 #include "mb_ensemble_kernel.cuh"
@@ -129,7 +129,7 @@ __device__ __forceinline__ void itl_clear_flags(const LatDesc &d) {
   if (blockIdx.x == 0 && threadIdx.x == 0) d.flag_count[cur] = 0;
 }
 
-// Warp `w` of the grid flags the lattice sites within reach of interstitial w.  With
+// One warp flags the lattice sites within reach of interstitial `it`.  With
 // `list` (this warp's MB_WIN_LIST entries of shared memory) the in-reach candidates are
 // listed first and the lanes then flag only those.
 __device__ __forceinline__ void itl_mark_one(const EnsParams &P, const LatDesc &d, int it, int *list = nullptr) {
